@@ -1,0 +1,56 @@
+"""Builds librtfmm_b200.so in place with nvcc for sm_100a.
+
+    python exafmm-rd_b200/build.py
+
+The library holds the host set-up (C++/OpenMP), the CUDA kernels and the C
+ABI declared in include/rtfmm_b200.h.  It is written next to this file so
+that it travels with the source tree.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "librtfmm_b200.so")
+SOURCES = ["rtfmm_plan.cpp", "rtfmm_kernels.cu", "rtfmm_capi.cu"]
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
+         "-Xcompiler", "-fPIC,-fopenmp,-O3", "--expt-relaxed-constexpr"]
+
+
+def _stale():
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)]
+    deps.append(os.path.join(ROOT, "include", "rtfmm_b200.h"))
+    deps.append(os.path.abspath(__file__))
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(force=False, verbose=False):
+    if not force and not _stale():
+        return LIB
+    objs = []
+    odir = os.path.join(HERE, "_build")
+    os.makedirs(odir, exist_ok=True)
+    for src in SOURCES:
+        obj = os.path.join(odir, src + ".o")
+        cmd = [NVCC] + FLAGS + ["-I", os.path.join(ROOT, "include"), "-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+        objs.append(obj)
+    tmp = LIB + ".tmp"
+    cmd = [NVCC] + FLAGS + ["-shared", "-o", tmp] + objs + ["-lgomp"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)

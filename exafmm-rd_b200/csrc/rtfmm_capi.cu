@@ -1,0 +1,995 @@
+// C ABI of the B200 FMM evaluation pass: handle, device buffers and the
+// orchestration of one pass across two CUDA streams.
+//
+//   stream s0 (far field):  P2M -> M2M levels -> FFT-M2L (up, Hadamard, down)
+//                           -> L2L levels -> L2P            ... then post
+//   stream s1 (near field): P2P, concurrently with the far field
+//
+// This is LaplaceFMM::solve (3dpp/src/fmm.cpp:13-81) split at its hot block.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/rtfmm_b200.h"
+#include "rtfmm_kernels.cuh"
+#include "rtfmm_plan.h"
+
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
+using namespace rtfmm_b200;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CK(call)                                                                              \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess)                                                                    \
+      return fail(e_ == cudaErrorMemoryAllocation ? RTFMM_ENOMEM : RTFMM_ECUDA,               \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                        \
+  } while (0)
+
+enum Stage { ST_PREP = 0, ST_P2M, ST_M2M, ST_UP, ST_HAD, ST_DOWN, ST_L2L, ST_L2P, ST_P2P, ST_POST, ST_N };
+
+struct ApplyCall {
+  int groups, S, rows_max;
+  size_t inrow_off, outrow_off, scale_off, goff_off;  // offsets into the index / scale pools
+  int bsel;        // which operator stack
+  int a_is_leafvec, c_is_leafvec;  // A / C on the leaf scratch instead of the cell arrays
+  int beta;
+  bool has_scale;
+};
+
+enum BSel { B_P2M = 0, B_L2P, B_M2MT, B_M2M, B_IMGSUMT, B_IMG13, B_NUM };
+
+}  // namespace
+
+struct rtfmm_fmm {
+  Args args;
+  Plan plan;
+  Operators ops;
+  bool ops_valid = false;
+  bool setup_done = false;
+  bool device_ready = false;
+  bool pass_done = false;
+  std::vector<double> x_in;  // input-order positions of the set-up bodies
+  std::vector<double> q_in;
+
+  // host plan tables
+  std::vector<LeafInfo> leaves;
+  std::vector<int> body_leaf;
+  std::vector<P2PItem> items;
+  std::vector<int> list_off;
+  std::vector<P2PSrc32> list32;
+  std::vector<P2PSrc64> list64;
+  std::vector<int> idx_pool;
+  std::vector<double> scale_pool;
+  std::vector<ApplyCall> p2m_call, m2m_calls, l2l_calls, l2p_call;
+  std::vector<int> up8_items, down8_items, up27_items, down27_items;
+  std::vector<int> tsrc8, tsrc27;
+  std::vector<double> tscale8, tscale27;
+  int nS8 = 0, nT8 = 0, nS27 = 0, nT27 = 0;
+
+  // device
+  int dev = -1;
+  cudaStream_t s0 = nullptr, s1 = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_near0 = nullptr, ev_near = nullptr, ev_stop = nullptr;
+  cudaEvent_t ev_st[ST_N] = {};
+  std::vector<void*> allocs;
+  double4* d_body64 = nullptr;
+  float4* d_body32 = nullptr;
+  int* d_body_leaf = nullptr;
+  int64_t* d_perm = nullptr;
+  double *d_xin = nullptr, *d_qin = nullptr;
+  LeafInfo* d_leaves = nullptr;
+  double *d_qeq = nullptr, *d_pchk = nullptr, *d_leafvec = nullptr;
+  double *d_far_phi = nullptr, *d_far_grad = nullptr, *d_near_phi = nullptr, *d_near_grad = nullptr;
+  double *d_out_phi = nullptr, *d_out_grad = nullptr;
+  P2PItem* d_items = nullptr;
+  int* d_list_off = nullptr;
+  P2PSrc32* d_list32 = nullptr;
+  P2PSrc64* d_list64 = nullptr;
+  double *d_surf_unit = nullptr, *d_twiddle = nullptr;
+  int* d_surf_ijk = nullptr;
+  double* d_B[B_NUM] = {};
+  int* d_idx_pool = nullptr;
+  double* d_scale_pool = nullptr;
+  void *d_G8 = nullptr, *d_Q8 = nullptr, *d_Pk8 = nullptr;
+  double *d_G27 = nullptr, *d_Q27 = nullptr, *d_Pk27 = nullptr;
+  int *d_up8 = nullptr, *d_down8 = nullptr, *d_up27 = nullptr, *d_down27 = nullptr;
+  int *d_tsrc8 = nullptr, *d_tsrc27 = nullptr;
+  double *d_tscale8 = nullptr, *d_tscale27 = nullptr;
+  double* d_dip = nullptr;
+  void* d_flush = nullptr;
+  size_t flush_bytes = 0;
+  float stage_ms[ST_N] = {};
+  int64_t launches = 0;
+};
+
+namespace {
+
+template <typename T>
+int dalloc(rtfmm_fmm* f, T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, sizeof(T) * count);
+  if (e != cudaSuccess)
+    return fail(RTFMM_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  f->allocs.push_back(q);
+  *p = reinterpret_cast<T*>(q);
+  return RTFMM_OK;
+}
+
+template <typename T>
+int dupload(rtfmm_fmm* f, T** p, const std::vector<T>& h) {
+  int rc = dalloc(f, p, h.size());
+  if (rc) return rc;
+  if (!h.empty()) CK(cudaMemcpy(*p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+  return RTFMM_OK;
+}
+
+void free_device(rtfmm_fmm* f) {
+  if (f->dev >= 0) cudaSetDevice(f->dev);
+  for (void* p : f->allocs) cudaFree(p);
+  f->allocs.clear();
+  if (f->s0) cudaStreamDestroy(f->s0);
+  if (f->s1) cudaStreamDestroy(f->s1);
+  f->s0 = f->s1 = nullptr;
+  cudaEvent_t* evs[] = {&f->ev_start, &f->ev_near0, &f->ev_near, &f->ev_stop};
+  for (auto e : evs)
+    if (*e) {
+      cudaEventDestroy(*e);
+      *e = nullptr;
+    }
+  for (int k = 0; k < ST_N; ++k)
+    if (f->ev_st[k]) {
+      cudaEventDestroy(f->ev_st[k]);
+      f->ev_st[k] = nullptr;
+    }
+  f->device_ready = false;
+}
+
+bool finite_all(const double* a, int64_t n) {
+  for (int64_t i = 0; i < n; ++i)
+    if (!std::isfinite(a[i])) return false;
+  return true;
+}
+
+// Host tables for the device pass, derived from the plan.
+void build_tables(rtfmm_fmm* f) {
+  Plan& p = f->plan;
+  const Operators& o = f->ops;
+  const int ns = o.ns;
+  std::vector<int> leaf_of_cell(p.cells.size(), -1);
+  f->leaves.clear();
+  for (int c = 0; c < p.ntree; ++c) {
+    const Cell& cl = p.cells[c];
+    if (cl.cnum != 0) continue;
+    LeafInfo L;
+    L.cx = cl.x[0];
+    L.cy = cl.x[1];
+    L.cz = cl.x[2];
+    L.r = cl.r;
+    L.scale = std::pow(0.5, cl.depth);
+    L.cell = c;
+    L.boff = cl.boff;
+    L.bnum = cl.bnum;
+    leaf_of_cell[c] = (int)f->leaves.size();
+    f->leaves.push_back(L);
+  }
+  f->body_leaf.assign(p.n, 0);
+  for (int l = 0; l < (int)f->leaves.size(); ++l)
+    for (int b = 0; b < f->leaves[l].bnum; ++b) f->body_leaf[f->leaves[l].boff + b] = l;
+
+  // P2P lists in CSR by target leaf; work items of 32 targets
+  f->list_off.assign(f->leaves.size() + 1, 0);
+  f->list32.clear();
+  f->list64.clear();
+  f->items.clear();
+  for (int l = 0; l < (int)f->leaves.size(); ++l) {
+    f->list_off[l] = (int)f->list32.size();
+    const int c = f->leaves[l].cell;
+    auto it = p.p2p.find(c);
+    if (it != p.p2p.end()) {
+      for (const P2PEntry& e : it->second) {
+        const int sl = leaf_of_cell[e.src];
+        const Cell& S = p.cells[e.src];
+        const Cell& T = p.cells[c];
+        P2PSrc32 a;
+        a.dx = (float)(S.x[0] + e.off[0] - T.x[0]);
+        a.dy = (float)(S.x[1] + e.off[1] - T.x[1]);
+        a.dz = (float)(S.x[2] + e.off[2] - T.x[2]);
+        a.leaf = sl;
+        a.self = (e.src == c && e.off[0] == 0 && e.off[1] == 0 && e.off[2] == 0) ? 1 : 0;
+        a.pad[0] = a.pad[1] = a.pad[2] = 0;
+        f->list32.push_back(a);
+        P2PSrc64 b;
+        b.ox = e.off[0];
+        b.oy = e.off[1];
+        b.oz = e.off[2];
+        b.leaf = sl;
+        b.self = a.self;
+        f->list64.push_back(b);
+      }
+    }
+    for (int t0 = 0; t0 < f->leaves[l].bnum; t0 += 32) f->items.push_back({l, t0});
+  }
+  f->list_off[f->leaves.size()] = (int)f->list32.size();
+
+  // batched operator applications
+  f->idx_pool.clear();
+  f->scale_pool.clear();
+  auto add_call = [&](std::vector<ApplyCall>& dst, int S, const std::vector<std::vector<int>>& in_by_group,
+                      const std::vector<std::vector<int>>& out_by_group, const std::vector<double>* scale,
+                      int bsel, int a_leaf, int c_leaf, int beta) {
+    ApplyCall ac;
+    ac.groups = (int)out_by_group.size();
+    ac.S = S;
+    ac.rows_max = 0;
+    ac.bsel = bsel;
+    ac.a_is_leafvec = a_leaf;
+    ac.c_is_leafvec = c_leaf;
+    ac.beta = beta;
+    ac.has_scale = scale != nullptr;
+    ac.goff_off = f->idx_pool.size();
+    int acc = 0;
+    for (auto& g : out_by_group) {
+      f->idx_pool.push_back(acc);
+      acc += (int)g.size();
+      ac.rows_max = std::max(ac.rows_max, (int)g.size());
+    }
+    f->idx_pool.push_back(acc);
+    ac.inrow_off = f->idx_pool.size();
+    for (auto& g : in_by_group) f->idx_pool.insert(f->idx_pool.end(), g.begin(), g.end());
+    ac.outrow_off = f->idx_pool.size();
+    for (auto& g : out_by_group) f->idx_pool.insert(f->idx_pool.end(), g.begin(), g.end());
+    ac.scale_off = f->scale_pool.size();
+    if (scale) f->scale_pool.insert(f->scale_pool.end(), scale->begin(), scale->end());
+    if (acc > 0) dst.push_back(ac);
+  };
+  f->p2m_call.clear();
+  f->m2m_calls.clear();
+  f->l2l_calls.clear();
+  f->l2p_call.clear();
+  {
+    std::vector<int> in, out;
+    std::vector<double> sc;
+    for (int l = 0; l < (int)f->leaves.size(); ++l) {
+      in.push_back(l);
+      out.push_back(f->leaves[l].cell);
+      sc.push_back(f->leaves[l].scale);
+    }
+    add_call(f->p2m_call, 1, {in}, {out}, &sc, B_P2M, 1, 0, 0);
+    std::vector<int> in2, out2;
+    for (int l = 0; l < (int)f->leaves.size(); ++l) {
+      in2.push_back(f->leaves[l].cell);
+      out2.push_back(l);
+    }
+    add_call(f->l2p_call, 1, {in2}, {out2}, &sc, B_L2P, 0, 1, 0);
+  }
+  // M2M bottom-up (fmm.cpp:111-150): depth = dmax .. dmin+1
+  for (int depth = p.dmax; depth > p.dmin; --depth) {
+    std::vector<int> in, out;
+    for (int c = 0; c < (int)p.cells.size(); ++c) {
+      const Cell& cl = p.cells[c];
+      if (cl.depth != depth || cl.cnum == 0) continue;
+      out.push_back(c);
+      if (depth >= 0) {
+        int slot[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
+        for (int k = 0; k < cl.cnum; ++k) slot[p.cells[cl.coff + k].octant] = cl.coff + k;
+        in.insert(in.end(), slot, slot + 8);
+      } else {
+        in.push_back(cl.coff);
+      }
+    }
+    if (out.empty()) continue;
+    if (depth >= 0)
+      add_call(f->m2m_calls, 8, {in}, {out}, nullptr, B_M2MT, 0, 0, 0);
+    else
+      add_call(f->m2m_calls, 1, {in}, {out}, nullptr, B_IMGSUMT, 0, 0, 0);
+  }
+  // L2L top-down (fmm.cpp:195-229): depth = dmin .. dmax-1
+  for (int depth = p.dmin; depth < p.dmax; ++depth) {
+    std::vector<std::vector<int>> in(8), out(8);
+    std::vector<int> in1, out1;
+    for (int c = 0; c < (int)p.cells.size(); ++c) {
+      const Cell& cl = p.cells[c];
+      if (cl.depth != depth || cl.cnum == 0) continue;
+      if (depth >= 0) {
+        for (int k = 0; k < cl.cnum; ++k) {
+          const int ch = cl.coff + k;
+          in[p.cells[ch].octant].push_back(c);
+          out[p.cells[ch].octant].push_back(ch);
+        }
+      } else {
+        in1.push_back(c);
+        out1.push_back(cl.coff);
+      }
+    }
+    if (depth >= 0) {
+      bool any = false;
+      for (auto& g : out) any |= !g.empty();
+      if (any) add_call(f->l2l_calls, 1, in, out, nullptr, B_M2M, 0, 0, 1);
+    } else if (!out1.empty()) {
+      add_call(f->l2l_calls, 1, {in1}, {out1}, nullptr, B_IMG13, 0, 0, 1);
+    }
+  }
+
+  // FFT-M2L lists (m2l_fft_precompute_t, kernel.cpp:1153-1245)
+  std::map<int, int> s8, s27;
+  std::vector<int> t8cells, t27cells;
+  for (auto& kv : p.m2l) {
+    bool single = false, normal = false;
+    for (const M2LEntry& e : kv.second) (e.single ? single : normal) = true;
+    if (normal) t8cells.push_back(kv.first);
+    if (single) t27cells.push_back(kv.first);
+    for (const M2LEntry& e : kv.second) (e.single ? s27 : s8)[e.src] = 0;
+  }
+  int k = 0;
+  for (auto& kv : s8) kv.second = k++;
+  k = 0;
+  for (auto& kv : s27) kv.second = k++;
+  f->nS8 = (int)s8.size();
+  f->nS27 = (int)s27.size();
+  f->nT8 = (int)t8cells.size();
+  f->nT27 = (int)t27cells.size();
+  auto child_slot = [&](int ch) { return p.cells[ch].octant == 13 ? 0 : p.cells[ch].octant; };
+  f->up8_items.clear();
+  f->up27_items.clear();
+  for (auto& kv : s8) {
+    int slot[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
+    const Cell& cl = p.cells[kv.first];
+    for (int c = 0; c < cl.cnum; ++c) slot[child_slot(cl.coff + c)] = cl.coff + c;
+    for (int sl = 0; sl < 8; ++sl) {
+      f->up8_items.push_back(kv.second);
+      f->up8_items.push_back(sl);
+      f->up8_items.push_back(slot[sl]);
+    }
+  }
+  for (auto& kv : s27) {
+    const Cell& cl = p.cells[kv.first];
+    f->up27_items.push_back(kv.second);
+    f->up27_items.push_back(0);
+    f->up27_items.push_back(cl.coff);
+  }
+  auto direction = [&](int t, const M2LEntry& e) {
+    const Cell& T = p.cells[t];
+    const Cell& S = p.cells[e.src];
+    int v[3];
+    for (int q = 0; q < 3; ++q) v[q] = (int)std::lround((S.x[q] + e.off[q] - T.x[q]) / (T.r * 2));
+    int d = (v[2] + 1) * 9 + (v[1] + 1) * 3 + (v[0] + 1);
+    return d > 13 ? d - 1 : d;
+  };
+  const double N3 = (double)o.N * o.N * o.N;
+  auto fill_targets = [&](const std::vector<int>& tcells, bool single, std::map<int, int>& smap,
+                          std::vector<int>& tsrc, std::vector<double>& tscale, std::vector<int>& down) {
+    tsrc.assign(tcells.size() * 26, -1);
+    tscale.assign(tcells.size(), 0.0);
+    down.clear();
+    for (int ti = 0; ti < (int)tcells.size(); ++ti) {
+      const int t = tcells[ti];
+      for (const M2LEntry& e : p.m2l[t]) {
+        if ((e.single != 0) != single) continue;
+        tsrc[ti * 26 + direction(t, e)] = smap[e.src];
+      }
+      const Cell& T = p.cells[t];
+      tscale[ti] = std::pow(T.depth >= -1 ? 2.0 : 3.0, T.depth + 1) / N3;
+      for (int c = 0; c < T.cnum; ++c) {
+        down.push_back(ti);
+        down.push_back(child_slot(T.coff + c));
+        down.push_back(T.coff + c);
+      }
+    }
+  };
+  fill_targets(t8cells, false, s8, f->tsrc8, f->tscale8, f->down8_items);
+  fill_targets(t27cells, true, s27, f->tsrc27, f->tscale27, f->down27_items);
+  (void)ns;
+}
+
+int ensure_device(rtfmm_fmm* f) {
+  if (f->dev != f->args.device || !f->s0) {
+    free_device(f);
+    CK(cudaSetDevice(f->args.device));
+    f->dev = f->args.device;
+    CK(cudaStreamCreateWithFlags(&f->s0, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&f->s1, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&f->ev_start));
+    CK(cudaEventCreate(&f->ev_near0));
+    CK(cudaEventCreate(&f->ev_near));
+    CK(cudaEventCreate(&f->ev_stop));
+    for (int k = 0; k < ST_N; ++k) CK(cudaEventCreate(&f->ev_st[k]));
+  } else {
+    CK(cudaSetDevice(f->dev));
+  }
+  return RTFMM_OK;
+}
+
+// Upload the plan (everything but the per-pass body values) to the device.
+int upload_plan(rtfmm_fmm* f) {
+  int rc = ensure_device(f);
+  if (rc) return rc;
+  // drop buffers of a previous plan, keep streams/events
+  CK(cudaDeviceSynchronize());
+  for (void* p : f->allocs) cudaFree(p);
+  f->allocs.clear();
+  Plan& p = f->plan;
+  const Operators& o = f->ops;
+  const int64_t n = p.n;
+  const int ns = o.ns, Nf = o.Nf;
+  const size_t ncell = p.cells.size(), nleaf = f->leaves.size();
+  const bool mixed = f->args.precision == RTFMM_FP32_MIXED;
+#define RC(x)          \
+  do {                 \
+    int r_ = (x);      \
+    if (r_) return r_; \
+  } while (0)
+  RC(dalloc(f, &f->d_body64, n));
+  RC(dalloc(f, &f->d_body32, n));
+  RC(dupload(f, &f->d_body_leaf, f->body_leaf));
+  RC(dupload(f, &f->d_perm, p.perm));
+  RC(dalloc(f, &f->d_xin, 3 * n));
+  RC(dalloc(f, &f->d_qin, n));
+  RC(dupload(f, &f->d_leaves, f->leaves));
+  RC(dalloc(f, &f->d_qeq, ncell * ns));
+  RC(dalloc(f, &f->d_pchk, ncell * ns));
+  RC(dalloc(f, &f->d_leafvec, nleaf * ns));
+  RC(dalloc(f, &f->d_far_phi, n));
+  RC(dalloc(f, &f->d_far_grad, 3 * n));
+  RC(dalloc(f, &f->d_near_phi, n));
+  RC(dalloc(f, &f->d_near_grad, 3 * n));
+  RC(dalloc(f, &f->d_out_phi, n));
+  RC(dalloc(f, &f->d_out_grad, 3 * n));
+  RC(dupload(f, &f->d_items, f->items));
+  RC(dupload(f, &f->d_list_off, f->list_off));
+  RC(dupload(f, &f->d_list32, f->list32));
+  RC(dupload(f, &f->d_list64, f->list64));
+  RC(dupload(f, &f->d_surf_unit, o.surf_unit));
+  RC(dupload(f, &f->d_surf_ijk, o.surf_ijk));
+  std::vector<double> tw(2 * o.N);
+  for (int m = 0; m < o.N; ++m) {
+    tw[2 * m] = std::cos(2.0 * M_PI * m / o.N);
+    tw[2 * m + 1] = -std::sin(2.0 * M_PI * m / o.N);
+  }
+  RC(dupload(f, &f->d_twiddle, tw));
+  // operator stacks in the [s][j][n] layout of k_apply_f64
+  const size_t nn = (size_t)ns * ns;
+  std::vector<double> b;
+  b = o.pinv_down;  // P2M: B[j][n] = pinv_up[n][j]
+  RC(dupload(f, &f->d_B[B_P2M], b));
+  b = o.pinv_up;    // L2P: B[j][n] = pinv_down[n][j]
+  RC(dupload(f, &f->d_B[B_L2P], b));
+  b.assign(8 * nn, 0.0);
+  for (int oc = 0; oc < 8; ++oc)
+    for (int j = 0; j < ns; ++j)
+      for (int i = 0; i < ns; ++i) b[oc * nn + (size_t)j * ns + i] = o.m2m[oc][(size_t)i * ns + j];
+  RC(dupload(f, &f->d_B[B_M2MT], b));
+  b.assign(8 * nn, 0.0);
+  for (int oc = 0; oc < 8; ++oc) std::memcpy(&b[oc * nn], o.m2m[oc].data(), sizeof(double) * nn);
+  RC(dupload(f, &f->d_B[B_M2M], b));
+  b.assign(nn, 0.0);
+  for (int j = 0; j < ns; ++j)
+    for (int i = 0; i < ns; ++i) b[(size_t)j * ns + i] = o.m2m_img_sum[(size_t)i * ns + j];
+  RC(dupload(f, &f->d_B[B_IMGSUMT], b));
+  b.assign(nn, 0.0);
+  for (int j = 0; j < ns; ++j)
+    for (int i = 0; i < ns; ++i) b[(size_t)j * ns + i] = o.l2l_img[(size_t)i * ns + j];
+  RC(dupload(f, &f->d_B[B_IMG13], b));
+  RC(dupload(f, &f->d_idx_pool, f->idx_pool));
+  RC(dupload(f, &f->d_scale_pool, f->scale_pool));
+  // M2L
+  if (mixed) {
+    std::vector<float> g(o.cc8.size());
+    for (size_t i = 0; i < g.size(); ++i) g[i] = (float)o.cc8[i];
+    float* gp;
+    RC(dupload(f, &gp, g));
+    f->d_G8 = gp;
+    float *qp, *pp;
+    RC(dalloc(f, &qp, (size_t)f->nS8 * 8 * Nf * 2));
+    RC(dalloc(f, &pp, (size_t)f->nT8 * 8 * Nf * 2));
+    f->d_Q8 = qp;
+    f->d_Pk8 = pp;
+  } else {
+    double* gp;
+    RC(dupload(f, &gp, o.cc8));
+    f->d_G8 = gp;
+    double *qp, *pp;
+    RC(dalloc(f, &qp, (size_t)f->nS8 * 8 * Nf * 2));
+    RC(dalloc(f, &pp, (size_t)f->nT8 * 8 * Nf * 2));
+    f->d_Q8 = qp;
+    f->d_Pk8 = pp;
+  }
+  RC(dupload(f, &f->d_G27, o.cc27sum));
+  RC(dalloc(f, &f->d_Q27, (size_t)f->nS27 * 8 * Nf * 2));
+  RC(dalloc(f, &f->d_Pk27, (size_t)f->nT27 * 8 * Nf * 2));
+  RC(dupload(f, &f->d_up8, f->up8_items));
+  RC(dupload(f, &f->d_down8, f->down8_items));
+  RC(dupload(f, &f->d_up27, f->up27_items));
+  RC(dupload(f, &f->d_down27, f->down27_items));
+  RC(dupload(f, &f->d_tsrc8, f->tsrc8));
+  RC(dupload(f, &f->d_tsrc27, f->tsrc27));
+  RC(dupload(f, &f->d_tscale8, f->tscale8));
+  RC(dupload(f, &f->d_tscale27, f->tscale27));
+  RC(dalloc(f, &f->d_dip, 3 * 256 + 3));
+#undef RC
+  f->device_ready = true;
+  return RTFMM_OK;
+}
+
+int run_apply(rtfmm_fmm* f, const ApplyCall& c) {
+  ApplyBatch b;
+  b.A = c.a_is_leafvec ? f->d_leafvec : (c.bsel == B_L2P || c.bsel == B_M2M || c.bsel == B_IMG13 ? f->d_pchk : f->d_qeq);
+  b.C = c.c_is_leafvec ? f->d_leafvec : (c.bsel == B_M2M || c.bsel == B_IMG13 ? f->d_pchk : f->d_qeq);
+  b.inrow = f->d_idx_pool + c.inrow_off;
+  b.outrow = f->d_idx_pool + c.outrow_off;
+  b.group_off = f->d_idx_pool + c.goff_off;
+  b.scale = c.has_scale ? f->d_scale_pool + c.scale_off : nullptr;
+  b.B = f->d_B[c.bsel];
+  b.groups = c.groups;
+  b.S = c.S;
+  b.ns = f->ops.ns;
+  b.beta = c.beta;
+  b.max_rows = c.rows_max;
+  CK(launch_apply(b, f->s0));
+  f->launches++;
+  return RTFMM_OK;
+}
+
+// One evaluation pass on the device-resident bodies (d_body64).
+int enqueue_pass(rtfmm_fmm* f) {
+  const Plan& p = f->plan;
+  const Operators& o = f->ops;
+  const int n = (int)p.n, ns = o.ns, Nf = o.Nf, P = o.P;
+  const int nleaf = (int)f->leaves.size();
+  const bool mixed = f->args.precision == RTFMM_FP32_MIXED;
+  const unsigned stages = f->args.stages ? f->args.stages : RTFMM_STAGE_ALL;
+  const bool near = stages & RTFMM_STAGE_NEAR, far = stages & RTFMM_STAGE_FAR;
+  cudaStream_t s0 = f->s0, s1 = f->s1;
+  f->launches = 0;
+  CK(cudaEventRecord(f->ev_start, s0));
+  if (near) {
+    CK(cudaStreamWaitEvent(s1, f->ev_start, 0));
+    CK(cudaEventRecord(f->ev_near0, s1));
+    if (mixed) {
+      CK(launch_prep32(f->d_body64, f->d_body_leaf, f->d_leaves, f->d_body32, n, s1));
+      CK(launch_p2p32(f->d_body32, f->d_leaves, f->d_items, (int)f->items.size(), f->d_list_off, f->d_list32,
+                      f->d_near_phi, f->d_near_grad, s1));
+      f->launches += 2;
+    } else {
+      CK(launch_p2p64(f->d_body64, f->d_leaves, f->d_items, (int)f->items.size(), f->d_list_off, f->d_list64,
+                      f->d_near_phi, f->d_near_grad, s1));
+      f->launches += 1;
+    }
+    CK(cudaEventRecord(f->ev_near, s1));
+  }
+  CK(cudaEventRecord(f->ev_st[ST_PREP], s0));
+  if (far) {
+    CK(cudaMemsetAsync(f->d_pchk, 0, sizeof(double) * p.cells.size() * ns, s0));
+    CK(launch_p2m_check(f->d_body64, f->d_leaves, nleaf, f->d_surf_unit, ns, f->d_leafvec, s0));
+    f->launches++;
+    for (auto& c : f->p2m_call) {
+      int rc = run_apply(f, c);
+      if (rc) return rc;
+    }
+    CK(cudaEventRecord(f->ev_st[ST_P2M], s0));
+    for (auto& c : f->m2m_calls) {
+      int rc = run_apply(f, c);
+      if (rc) return rc;
+    }
+    CK(cudaEventRecord(f->ev_st[ST_M2M], s0));
+    const int nup8 = (int)f->up8_items.size() / 3, nup27 = (int)f->up27_items.size() / 3;
+    const int ndn8 = (int)f->down8_items.size() / 3, ndn27 = (int)f->down27_items.size() / 3;
+    if (mixed) {
+      CK(launch_m2l_up<float>(f->d_qeq, f->d_up8, nup8, f->d_surf_ijk, f->d_twiddle, P, ns, (float*)f->d_Q8, s0));
+    } else {
+      CK(launch_m2l_up<double>(f->d_qeq, f->d_up8, nup8, f->d_surf_ijk, f->d_twiddle, P, ns, (double*)f->d_Q8,
+                               s0));
+    }
+    CK(launch_m2l_up<double>(f->d_qeq, f->d_up27, nup27, f->d_surf_ijk, f->d_twiddle, P, ns, f->d_Q27, s0));
+    f->launches += (nup8 > 0) + (nup27 > 0);
+    CK(cudaEventRecord(f->ev_st[ST_UP], s0));
+    if (mixed) {
+      CK(launch_m2l_hadamard8<float>((const float*)f->d_Q8, (const float*)f->d_G8, f->d_tsrc8, f->nT8, Nf,
+                                     (float*)f->d_Pk8, s0));
+    } else {
+      CK(launch_m2l_hadamard8<double>((const double*)f->d_Q8, (const double*)f->d_G8, f->d_tsrc8, f->nT8, Nf,
+                                      (double*)f->d_Pk8, s0));
+    }
+    CK(launch_m2l_hadamard27(f->d_Q27, f->d_G27, f->d_tsrc27, f->nT27, Nf, f->d_Pk27, s0));
+    f->launches += (f->nT8 > 0) + (f->nT27 > 0);
+    CK(cudaEventRecord(f->ev_st[ST_HAD], s0));
+    if (mixed) {
+      CK(launch_m2l_down<float>((const float*)f->d_Pk8, f->d_down8, f->d_tscale8, ndn8, f->d_surf_ijk,
+                                f->d_twiddle, P, ns, f->d_pchk, s0));
+    } else {
+      CK(launch_m2l_down<double>((const double*)f->d_Pk8, f->d_down8, f->d_tscale8, ndn8, f->d_surf_ijk,
+                                 f->d_twiddle, P, ns, f->d_pchk, s0));
+    }
+    CK(launch_m2l_down<double>(f->d_Pk27, f->d_down27, f->d_tscale27, ndn27, f->d_surf_ijk, f->d_twiddle, P, ns,
+                               f->d_pchk, s0));
+    f->launches += (ndn8 > 0) + (ndn27 > 0);
+    CK(cudaEventRecord(f->ev_st[ST_DOWN], s0));
+    for (auto& c : f->l2l_calls) {
+      int rc = run_apply(f, c);
+      if (rc) return rc;
+    }
+    CK(cudaEventRecord(f->ev_st[ST_L2L], s0));
+    for (auto& c : f->l2p_call) {
+      int rc = run_apply(f, c);
+      if (rc) return rc;
+    }
+    CK(launch_l2p_eval(f->d_body64, f->d_leaves, nleaf, f->d_surf_unit, ns, f->d_leafvec, f->d_far_phi,
+                       f->d_far_grad, s0));
+    f->launches++;
+    CK(cudaEventRecord(f->ev_st[ST_L2P], s0));
+  } else {
+    for (int k = ST_P2M; k <= ST_L2P; ++k) CK(cudaEventRecord(f->ev_st[k], s0));
+  }
+  if (near) CK(cudaStreamWaitEvent(s0, f->ev_near, 0));
+  CK(cudaEventRecord(f->ev_st[ST_P2P], s0));
+  const Args& a = f->args;
+  if (a.dipole_correction) {
+    CK(launch_dipole(f->d_body64, n, f->d_dip, s0));
+    f->launches += 2;
+  }
+  const double coef = 4 * M_PI / (3 * a.cycle * a.cycle * a.cycle);
+  CK(launch_post(far ? f->d_far_phi : nullptr, f->d_far_grad, near ? f->d_near_phi : nullptr, f->d_near_grad,
+                 f->d_body64, f->d_perm, n, f->d_dip, coef, a.dipole_correction,
+                 a.divide_4pi ? 1.0 / (4 * M_PI) : 1.0, f->d_out_phi, f->d_out_grad, s0));
+  f->launches++;
+  CK(cudaEventRecord(f->ev_st[ST_POST], s0));
+  CK(cudaEventRecord(f->ev_stop, s0));
+  return RTFMM_OK;
+}
+
+int collect_times(rtfmm_fmm* f, float* total) {
+  CK(cudaEventSynchronize(f->ev_stop));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, f->ev_start, f->ev_stop));
+  if (total) *total = ms;
+  cudaEvent_t prev = f->ev_start;
+  for (int k = 0; k < ST_N; ++k) {
+    float t = 0;
+    if (k == ST_P2P) {
+      const unsigned stages = f->args.stages ? f->args.stages : RTFMM_STAGE_ALL;
+      if (stages & RTFMM_STAGE_NEAR) CK(cudaEventElapsedTime(&t, f->ev_near0, f->ev_near));
+      f->stage_ms[k] = t;
+      prev = f->ev_st[k];
+      continue;
+    }
+    CK(cudaEventElapsedTime(&t, prev, f->ev_st[k]));
+    f->stage_ms[k] = t;
+    prev = f->ev_st[k];
+  }
+  return RTFMM_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+void rtfmm_b200_default_args(rtfmm_args* a) {
+  if (!a) return;
+  a->P = 4;
+  a->ncrit = 16;
+  a->images = 0;
+  a->cycle = 2 * M_PI;
+  a->x[0] = a->x[1] = a->x[2] = 0.0;
+  a->dipole_correction = 1;
+  a->divide_4pi = 0;
+  a->precision = RTFMM_FP64;
+  a->stages = RTFMM_STAGE_ALL;
+  a->device = 0;
+}
+
+int rtfmm_b200_create(const rtfmm_args* a, rtfmm_fmm** out) {
+  if (!a || !out) return fail(RTFMM_EINVAL, "null argument");
+  *out = nullptr;
+  if (a->P < 2 || a->P > 16) return fail(RTFMM_EINVAL, "P must be in [2, 16]");
+  if (a->ncrit < 1) return fail(RTFMM_EINVAL, "ncrit must be >= 1");
+  if (a->images < 0 || a->images > 20) return fail(RTFMM_EINVAL, "images must be in [0, 20]");
+  if (!(a->cycle > 0) || !std::isfinite(a->cycle)) return fail(RTFMM_EINVAL, "cycle must be positive and finite");
+  if (a->precision != RTFMM_FP64 && a->precision != RTFMM_FP32_MIXED)
+    return fail(RTFMM_EINVAL, "unknown precision");
+  if (a->stages & ~RTFMM_STAGE_ALL) return fail(RTFMM_EINVAL, "unknown stage bits");
+  for (int k = 0; k < 3; ++k)
+    if (!std::isfinite(a->x[k])) return fail(RTFMM_EINVAL, "centre must be finite");
+  rtfmm_fmm* f = new (std::nothrow) rtfmm_fmm();
+  if (!f) return fail(RTFMM_ENOMEM, "host allocation failed");
+  f->args.P = a->P;
+  f->args.ncrit = a->ncrit;
+  f->args.images = a->images;
+  f->args.cycle = a->cycle;
+  f->args.x = {a->x[0], a->x[1], a->x[2]};
+  f->args.dipole_correction = a->dipole_correction;
+  f->args.divide_4pi = a->divide_4pi;
+  f->args.precision = a->precision;
+  f->args.stages = a->stages ? a->stages : RTFMM_STAGE_ALL;
+  f->args.device = a->device;
+  *out = f;
+  return RTFMM_OK;
+}
+
+int rtfmm_b200_destroy(rtfmm_fmm* f) {
+  if (!f) return RTFMM_OK;
+  free_device(f);
+  delete f;
+  return RTFMM_OK;
+}
+
+int rtfmm_b200_setup(rtfmm_fmm* f, int64_t n, const double* x, const double* q) {
+  if (!f) return fail(RTFMM_EINVAL, "null handle");
+  if (n < 0 || n > (int64_t)1 << 30) return fail(RTFMM_EINVAL, "n out of range");
+  if (n > 0 && (!x || !q)) return fail(RTFMM_EINVAL, "null body arrays");
+  if (!finite_all(x, 3 * n) || !finite_all(q, n)) return fail(RTFMM_EINVAL, "non-finite body position or charge");
+  try {
+    f->setup_done = false;
+    f->pass_done = false;
+    f->plan = Plan();
+    f->plan.args = f->args;
+    f->plan.n = n;
+    f->x_in.assign(x, x + 3 * n);
+    f->q_in.assign(q, q + n);
+    std::string err = build_tree(f->plan, x, q);
+    if (!err.empty()) return fail(RTFMM_EINVAL, err);
+    traverse(f->plan);
+    if (!f->ops_valid || f->ops.P != f->args.P || f->ops.images != f->args.images ||
+        f->ops.r0 != f->plan.r0) {
+      build_operators(f->ops, f->args.P, f->plan.r0, f->args.images);
+      f->ops_valid = true;
+    }
+    build_tables(f);
+  } catch (const std::bad_alloc&) {
+    return fail(RTFMM_ENOMEM, "host allocation failed during set-up");
+  } catch (const std::exception& e) {
+    return fail(RTFMM_EINVAL, std::string("set-up failed: ") + e.what());
+  }
+  f->setup_done = true;
+  f->device_ready = false;
+  return RTFMM_OK;
+}
+
+int rtfmm_b200_upload(rtfmm_fmm* f) {
+  if (!f) return fail(RTFMM_EINVAL, "null handle");
+  if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");
+  if (!f->device_ready) {
+    int rc = upload_plan(f);
+    if (rc) return rc;
+  }
+  CK(cudaSetDevice(f->dev));
+  if (f->plan.n > 0) {
+    std::vector<double4> b(f->plan.n);
+    for (int64_t i = 0; i < f->plan.n; ++i)
+      b[i] = make_double4(f->plan.x[3 * i], f->plan.x[3 * i + 1], f->plan.x[3 * i + 2], f->plan.q[i]);
+    CK(cudaMemcpy(f->d_body64, b.data(), sizeof(double4) * b.size(), cudaMemcpyHostToDevice));
+  }
+  return RTFMM_OK;
+}
+
+int rtfmm_b200_evaluate_device(rtfmm_fmm* f, float* ms) {
+  if (!f) return fail(RTFMM_EINVAL, "null handle");
+  if (!f->setup_done || !f->device_ready) return fail(RTFMM_ESTATE, "upload has not run");
+  CK(cudaSetDevice(f->dev));
+  if (f->plan.n == 0) {
+    if (ms) *ms = 0;
+    return RTFMM_OK;
+  }
+  int rc = enqueue_pass(f);
+  if (rc) return rc;
+  float t = 0;
+  rc = collect_times(f, &t);
+  if (rc) return rc;
+  CK(cudaGetLastError());
+  if (ms) *ms = t;
+  f->pass_done = true;
+  return RTFMM_OK;
+}
+
+int rtfmm_b200_download(rtfmm_fmm* f, double* phi, double* grad) {
+  if (!f) return fail(RTFMM_EINVAL, "null handle");
+  if (!f->pass_done) return fail(RTFMM_ESTATE, "no pass has run");
+  if (f->plan.n == 0) return RTFMM_OK;
+  CK(cudaSetDevice(f->dev));
+  if (phi) CK(cudaMemcpyAsync(phi, f->d_out_phi, sizeof(double) * f->plan.n, cudaMemcpyDeviceToHost, f->s0));
+  if (grad) CK(cudaMemcpyAsync(grad, f->d_out_grad, sizeof(double) * 3 * f->plan.n, cudaMemcpyDeviceToHost, f->s0));
+  CK(cudaStreamSynchronize(f->s0));
+  return RTFMM_OK;
+}
+
+int rtfmm_b200_evaluate(rtfmm_fmm* f, const double* q, double* phi, double* grad) {
+  if (!f) return fail(RTFMM_EINVAL, "null handle");
+  if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");
+  const int64_t n = f->plan.n;
+  if (n == 0) return RTFMM_OK;
+  if (q && !finite_all(q, n)) return fail(RTFMM_EINVAL, "non-finite charge");
+  if (!f->device_ready) {
+    int rc = upload_plan(f);
+    if (rc) return rc;
+  }
+  CK(cudaSetDevice(f->dev));
+  // host -> device (input order), then gather into tree order on the device
+  CK(cudaMemcpyAsync(f->d_xin, f->x_in.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice, f->s0));
+  CK(cudaMemcpyAsync(f->d_qin, q ? q : f->q_in.data(), sizeof(double) * n, cudaMemcpyHostToDevice, f->s0));
+  CK(launch_gather_bodies(f->d_xin, f->d_qin, f->d_perm, (int)n, f->d_body64, f->s0));
+  int rc = enqueue_pass(f);
+  if (rc) return rc;
+  f->launches++;
+  if (phi) CK(cudaMemcpyAsync(phi, f->d_out_phi, sizeof(double) * n, cudaMemcpyDeviceToHost, f->s0));
+  if (grad) CK(cudaMemcpyAsync(grad, f->d_out_grad, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, f->s0));
+  CK(cudaStreamSynchronize(f->s0));
+  CK(cudaGetLastError());
+  rc = collect_times(f, nullptr);
+  if (rc) return rc;
+  f->pass_done = true;
+  return RTFMM_OK;
+}
+
+int rtfmm_b200_solve(rtfmm_fmm* f, int64_t n, const double* x, const double* q, double* phi, double* grad) {
+  int rc = rtfmm_b200_setup(f, n, x, q);
+  if (rc) return rc;
+  return rtfmm_b200_evaluate(f, q, phi, grad);
+}
+
+int rtfmm_b200_adjoint(rtfmm_fmm* f, const double* w, double* dLdq, double* dLdx) {
+  (void)w;
+  (void)dLdq;
+  (void)dLdx;
+  if (!f) return fail(RTFMM_EINVAL, "null handle");
+  return fail(RTFMM_ENOTSUP, "adjoint not built yet");
+}
+
+int rtfmm_b200_stage_times(rtfmm_fmm* f, double* ms, int cap) {
+  if (!f) return fail(RTFMM_EINVAL, "null handle");
+  for (int k = 0; k < ST_N && k < cap; ++k) ms[k] = f->stage_ms[k];
+  return ST_N;
+}
+
+int rtfmm_b200_launch_count(rtfmm_fmm* f, int64_t* launches) {
+  if (!f || !launches) return fail(RTFMM_EINVAL, "null argument");
+  *launches = f->launches;
+  return RTFMM_OK;
+}
+
+int rtfmm_b200_flush_l2(rtfmm_fmm* f) {
+  if (!f) return fail(RTFMM_EINVAL, "null handle");
+  if (!f->s0) return fail(RTFMM_ESTATE, "no device state");
+  CK(cudaSetDevice(f->dev));
+  if (!f->d_flush) {
+    f->flush_bytes = (size_t)256 << 20;
+    CK(cudaMalloc(&f->d_flush, f->flush_bytes));
+    f->allocs.push_back(f->d_flush);
+  }
+  CK(cudaMemsetAsync(f->d_flush, f->launches & 0xff, f->flush_bytes, f->s0));
+  CK(cudaStreamSynchronize(f->s0));
+  return RTFMM_OK;
+}
+
+int rtfmm_b200_info(rtfmm_fmm* f, int64_t* info, int cap) {
+  if (!f || !info) return fail(RTFMM_EINVAL, "null argument");
+  if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");
+  int64_t v[8] = {(int64_t)f->plan.cells.size(), (int64_t)f->leaves.size(), f->plan.dmin, f->plan.dmax,
+                  f->plan.n_p2p, (int64_t)f->plan.m2l.size(), f->plan.n_m2l, f->ops.ns};
+  for (int k = 0; k < 8 && k < cap; ++k) info[k] = v[k];
+  return 8;
+}
+
+int rtfmm_b200_get_cells(rtfmm_fmm* f, int32_t* ints, double* reals) {
+  if (!f) return fail(RTFMM_EINVAL, "null handle");
+  if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");
+  for (size_t c = 0; c < f->plan.cells.size(); ++c) {
+    const Cell& cl = f->plan.cells[c];
+    if (ints) {
+      int32_t* o = ints + 7 * c;
+      o[0] = cl.octant;
+      o[1] = cl.depth;
+      o[2] = cl.coff;
+      o[3] = cl.cnum;
+      o[4] = cl.boff;
+      o[5] = cl.bnum;
+      o[6] = 0;
+    }
+    if (reals) {
+      double* o = reals + 4 * c;
+      o[0] = cl.r;
+      o[1] = cl.x[0];
+      o[2] = cl.x[1];
+      o[3] = cl.x[2];
+    }
+  }
+  return RTFMM_OK;
+}
+
+int rtfmm_b200_get_perm(rtfmm_fmm* f, int64_t* perm) {
+  if (!f || !perm) return fail(RTFMM_EINVAL, "null argument");
+  if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");
+  std::memcpy(perm, f->plan.perm.data(), sizeof(int64_t) * f->plan.perm.size());
+  return RTFMM_OK;
+}
+
+int rtfmm_b200_get_p2p(rtfmm_fmm* f, int32_t* ints, double* off) {
+  if (!f) return fail(RTFMM_EINVAL, "null handle");
+  if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");
+  size_t e = 0;
+  for (auto& kv : f->plan.p2p)
+    for (const P2PEntry& s : kv.second) {
+      if (ints) {
+        ints[2 * e] = kv.first;
+        ints[2 * e + 1] = s.src;
+      }
+      if (off)
+        for (int k = 0; k < 3; ++k) off[3 * e + k] = s.off[k];
+      ++e;
+    }
+  return RTFMM_OK;
+}
+
+int rtfmm_b200_get_m2l(rtfmm_fmm* f, int32_t* ints, double* off) {
+  if (!f) return fail(RTFMM_EINVAL, "null handle");
+  if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");
+  size_t e = 0;
+  for (auto& kv : f->plan.m2l)
+    for (const M2LEntry& s : kv.second) {
+      if (ints) {
+        ints[3 * e] = kv.first;
+        ints[3 * e + 1] = s.src;
+        ints[3 * e + 2] = s.single;
+      }
+      if (off)
+        for (int k = 0; k < 3; ++k) off[3 * e + k] = s.off[k];
+      ++e;
+    }
+  return RTFMM_OK;
+}
+
+int rtfmm_b200_get_cell_vectors(rtfmm_fmm* f, int which, double* out) {
+  if (!f || !out) return fail(RTFMM_EINVAL, "null argument");
+  if (!f->pass_done) return fail(RTFMM_ESTATE, "no pass has run");
+  if (which != 0 && which != 1) return fail(RTFMM_EINVAL, "which must be 0 or 1");
+  CK(cudaSetDevice(f->dev));
+  CK(cudaMemcpy(out, which == 0 ? f->d_qeq : f->d_pchk, sizeof(double) * f->plan.cells.size() * f->ops.ns,
+                cudaMemcpyDeviceToHost));
+  return RTFMM_OK;
+}
+
+int rtfmm_b200_get_operator(rtfmm_fmm* f, int which, double* out, int64_t cap) {
+  if (!f || !out) return fail(RTFMM_EINVAL, "null argument");
+  if (!f->ops_valid) return fail(RTFMM_ESTATE, "setup has not run");
+  const Operators& o = f->ops;
+  const size_t nn = (size_t)o.ns * o.ns;
+  std::vector<double> v;
+  if (which == 0) {
+    v = o.pinv_up;
+  } else if (which == 1) {
+    v.resize(8 * nn);
+    for (int k = 0; k < 8; ++k) std::memcpy(&v[k * nn], o.m2m[k].data(), sizeof(double) * nn);
+  } else if (which == 2) {
+    v = o.m2m_img_sum;
+  } else if (which == 3) {
+    v = o.cc8;
+  } else {
+    return fail(RTFMM_EINVAL, "unknown operator");
+  }
+  if ((int64_t)v.size() > cap) return fail(RTFMM_EINVAL, "output buffer too small");
+  std::memcpy(out, v.data(), sizeof(double) * v.size());
+  return RTFMM_OK;
+}
+
+const char* rtfmm_b200_last_error(void) { return g_err.c_str(); }
+
+const char* rtfmm_b200_version(void) { return "rtfmm_b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

@@ -1,0 +1,824 @@
+// Device kernels of the periodic KIFMM evaluation pass for sm_100a.
+//
+// Stage map (reference function -> kernel here):
+//   p2p_1toN_256          (3dpp/src/kernel.cpp:258-311)   k_p2p32 / k_p2p64
+//   p2m_precompute        (kernel.cpp:332-371)            k_p2m_check + k_apply_f64
+//   m2m_precompute / img  (kernel.cpp:395-404, 434-442)   k_apply_f64 per level
+//   m2l_fft_precompute_t  (kernel.cpp:1140-1397)          k_m2l_up, k_m2l_hadamard8,
+//     hadamard_8x8 / 1x27 (kernel.cpp:1012-1138)          k_m2l_hadamard27, k_m2l_down
+//   l2l_precompute / img  (kernel.cpp:1419-1435)          k_apply_f64 per level
+//   l2p_precompute        (kernel.cpp:1458-1511)          k_apply_f64 + k_l2p_eval
+//   dipole_correction, scale_bodies, sort_bodies_by_idx
+//                         (kernel.cpp:1580-1596, body.cpp:88-96,177-190)  k_dipole_*, k_post
+//
+// Every index a kernel forms is checked against the extent of the buffer it
+// addresses; no kernel waits on another block.
+#include "rtfmm_kernels.cuh"
+
+#include <cuda_runtime.h>
+
+namespace rtfmm_b200 {
+
+// ---------------------------------------------------------------------------
+// small helpers
+// ---------------------------------------------------------------------------
+template <typename T> struct Cplx;
+template <> struct Cplx<float> { using type = float2; };
+template <> struct Cplx<double> { using type = double2; };
+
+__device__ __forceinline__ float rsqrt_approx(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// ---------------------------------------------------------------------------
+// body preparation
+// ---------------------------------------------------------------------------
+__global__ void k_gather_bodies(const double* __restrict__ x_in, const double* __restrict__ q_in,
+                                const int64_t* __restrict__ perm, int n, double4* __restrict__ body64) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int64_t k = perm[i];
+  body64[i] = make_double4(x_in[3 * k], x_in[3 * k + 1], x_in[3 * k + 2], q_in[k]);
+}
+
+// FP32 leaf-relative positions: (x - c_leaf, q) so that P2P differences stay
+// accurate in single precision.
+__global__ void k_prep32(const double4* __restrict__ body64, const int* __restrict__ body_leaf,
+                         const LeafInfo* __restrict__ leaves, float4* __restrict__ body32, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double4 b = body64[i];
+  const LeafInfo L = leaves[body_leaf[i]];
+  body32[i] = make_float4((float)(b.x - L.cx), (float)(b.y - L.cy), (float)(b.z - L.cz), (float)b.w);
+}
+
+// ---------------------------------------------------------------------------
+// P2P: one warp per (target leaf, 32 targets); sources staged 32 at a time in
+// a per-warp shared-memory slot and read as broadcasts.  FP32 partial sums
+// per source leaf are accumulated into FP64.
+// ---------------------------------------------------------------------------
+constexpr int kP2PWarps = 4;
+
+template <bool MASK>
+__device__ __forceinline__ void p2p32_tile(const float4* __restrict__ s, int cnt, float px, float py,
+                                           float pz, float& p, float& fx, float& fy, float& fz) {
+#pragma unroll 8
+  for (int k = 0; k < cnt; ++k) {
+    const float4 b = s[k];
+    const float dx = px - b.x, dy = py - b.y, dz = pz - b.z;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    float ir = rsqrt_approx(r2);
+    if (MASK) ir = r2 > 0.f ? ir : 0.f;
+    const float qir = b.w * ir;
+    p += qir;
+    const float q3 = qir * ir * ir;
+    fx = fmaf(q3, dx, fx);
+    fy = fmaf(q3, dy, fy);
+    fz = fmaf(q3, dz, fz);
+  }
+}
+
+__global__ void __launch_bounds__(32 * kP2PWarps)
+    k_p2p32(const float4* __restrict__ body32, const LeafInfo* __restrict__ leaves,
+            const P2PItem* __restrict__ items, int nitems, const int* __restrict__ list_off,
+            const P2PSrc32* __restrict__ list, double* __restrict__ phi, double* __restrict__ grad) {
+  __shared__ float4 sbuf[kP2PWarps][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int item = blockIdx.x * kP2PWarps + warp;
+  if (item >= nitems) return;  // warp-uniform
+  const P2PItem it = items[item];
+  const LeafInfo T = leaves[it.leaf];
+  const int t = it.t0 + lane;
+  const bool active = t < T.bnum;
+  const float4 xt = active ? body32[T.boff + t] : make_float4(0.f, 0.f, 0.f, 0.f);
+  double P = 0.0, Gx = 0.0, Gy = 0.0, Gz = 0.0;
+  const int e1 = list_off[it.leaf + 1];
+  for (int e = list_off[it.leaf]; e < e1; ++e) {
+    const P2PSrc32 src = list[e];
+    const LeafInfo S = leaves[src.leaf];
+    const float px = xt.x - src.dx, py = xt.y - src.dy, pz = xt.z - src.dz;
+    float p = 0.f, fx = 0.f, fy = 0.f, fz = 0.f;
+    for (int c0 = 0; c0 < S.bnum; c0 += 32) {
+      const int cnt = min(32, S.bnum - c0);
+      __syncwarp();
+      if (lane < cnt) sbuf[warp][lane] = body32[S.boff + c0 + lane];
+      __syncwarp();
+      if (src.self)
+        p2p32_tile<true>(sbuf[warp], cnt, px, py, pz, p, fx, fy, fz);
+      else
+        p2p32_tile<false>(sbuf[warp], cnt, px, py, pz, p, fx, fy, fz);
+    }
+    P += (double)p;
+    Gx += (double)fx;
+    Gy += (double)fy;
+    Gz += (double)fz;
+  }
+  if (active) {
+    const int b = T.boff + t;
+    phi[b] = P;
+    grad[3 * b + 0] = -Gx;
+    grad[3 * b + 1] = -Gy;
+    grad[3 * b + 2] = -Gz;
+  }
+}
+
+__global__ void __launch_bounds__(32 * kP2PWarps)
+    k_p2p64(const double4* __restrict__ body64, const LeafInfo* __restrict__ leaves,
+            const P2PItem* __restrict__ items, int nitems, const int* __restrict__ list_off,
+            const P2PSrc64* __restrict__ list, double* __restrict__ phi, double* __restrict__ grad) {
+  __shared__ double4 sbuf[kP2PWarps][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int item = blockIdx.x * kP2PWarps + warp;
+  if (item >= nitems) return;
+  const P2PItem it = items[item];
+  const LeafInfo T = leaves[it.leaf];
+  const int t = it.t0 + lane;
+  const bool active = t < T.bnum;
+  const double4 xt = active ? body64[T.boff + t] : make_double4(0, 0, 0, 0);
+  double P = 0.0, Gx = 0.0, Gy = 0.0, Gz = 0.0;
+  const int e1 = list_off[it.leaf + 1];
+  for (int e = list_off[it.leaf]; e < e1; ++e) {
+    const P2PSrc64 src = list[e];
+    const LeafInfo S = leaves[src.leaf];
+    for (int c0 = 0; c0 < S.bnum; c0 += 32) {
+      const int cnt = min(32, S.bnum - c0);
+      __syncwarp();
+      if (lane < cnt) sbuf[warp][lane] = body64[S.boff + c0 + lane];
+      __syncwarp();
+#pragma unroll 4
+      for (int k = 0; k < cnt; ++k) {
+        const double4 b = sbuf[warp][k];
+        // dx = x_t - (x_s + offset), as p2p_1toN_256 forms it (kernel.cpp:283-290)
+        const double dx = xt.x - (b.x + src.ox), dy = xt.y - (b.y + src.oy), dz = xt.z - (b.z + src.oz);
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        const double ir = r2 > 0.0 ? rsqrt(r2) : 0.0;
+        const double qir = b.w * ir;
+        P += qir;
+        const double q3 = qir * ir * ir;
+        Gx += q3 * dx;
+        Gy += q3 * dy;
+        Gz += q3 * dz;
+      }
+    }
+  }
+  if (active) {
+    const int b = T.boff + t;
+    phi[b] = P;
+    grad[3 * b + 0] = -Gx;
+    grad[3 * b + 1] = -Gy;
+    grad[3 * b + 2] = -Gz;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// P2M: check-surface potential of each leaf's bodies (FP64).  Surface points
+// are unit * (2.95 r) + centre (kernel.cpp:336).
+// ---------------------------------------------------------------------------
+constexpr int kSurfThreads = 128;
+constexpr int kSurfPer = 4;
+
+__global__ void __launch_bounds__(kSurfThreads)
+    k_p2m_check(const double4* __restrict__ body64, const LeafInfo* __restrict__ leaves,
+                const double* __restrict__ surf_unit, int ns, double* __restrict__ out) {
+  __shared__ double4 sb[kSurfThreads];
+  const LeafInfo L = leaves[blockIdx.x];
+  const double R = L.r * 2.95;
+  const int tid = threadIdx.x;
+  for (int i0 = 0; i0 < ns; i0 += kSurfThreads * kSurfPer) {
+    double yx[kSurfPer], yy[kSurfPer], yz[kSurfPer], acc[kSurfPer];
+#pragma unroll
+    for (int k = 0; k < kSurfPer; ++k) {
+      const int i = i0 + tid + k * kSurfThreads;
+      const int ii = i < ns ? i : 0;
+      yx[k] = surf_unit[3 * ii + 0] * R + L.cx;
+      yy[k] = surf_unit[3 * ii + 1] * R + L.cy;
+      yz[k] = surf_unit[3 * ii + 2] * R + L.cz;
+      acc[k] = 0.0;
+    }
+    for (int b0 = 0; b0 < L.bnum; b0 += kSurfThreads) {
+      const int cnt = min(kSurfThreads, L.bnum - b0);
+      __syncthreads();
+      if (tid < cnt) sb[tid] = body64[L.boff + b0 + tid];
+      __syncthreads();
+      for (int j = 0; j < cnt; ++j) {
+        const double4 b = sb[j];
+#pragma unroll
+        for (int k = 0; k < kSurfPer; ++k) {
+          const double dx = yx[k] - b.x, dy = yy[k] - b.y, dz = yz[k] - b.z;
+          const double r2 = dx * dx + dy * dy + dz * dz;
+          const double ir = r2 > 0.0 ? rsqrt(r2) : 0.0;
+          acc[k] += b.w * ir;
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kSurfPer; ++k) {
+      const int i = i0 + tid + k * kSurfThreads;
+      if (i < ns) out[(size_t)blockIdx.x * ns + i] = acc[k];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// L2P: potential and gradient at each leaf's bodies from the downward
+// equivalent density on the 2.95 r surface (kernel.cpp:1461, 1469-1510), FP64.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kSurfThreads)
+    k_l2p_eval(const double4* __restrict__ body64, const LeafInfo* __restrict__ leaves,
+               const double* __restrict__ surf_unit, int ns, const double* __restrict__ q_down,
+               double* __restrict__ phi, double* __restrict__ grad) {
+  extern __shared__ double4 sy[];  // ns entries
+  const LeafInfo L = leaves[blockIdx.x];
+  const double R = L.r * 2.95;
+  for (int i = threadIdx.x; i < ns; i += blockDim.x)
+    sy[i] = make_double4(surf_unit[3 * i] * R + L.cx, surf_unit[3 * i + 1] * R + L.cy,
+                         surf_unit[3 * i + 2] * R + L.cz, q_down[(size_t)blockIdx.x * ns + i]);
+  __syncthreads();
+  for (int t = threadIdx.x; t < L.bnum; t += blockDim.x) {
+    const double4 x = body64[L.boff + t];
+    double p = 0, gx = 0, gy = 0, gz = 0;
+    for (int i = 0; i < ns; ++i) {
+      const double4 y = sy[i];
+      const double dx = x.x - y.x, dy = x.y - y.y, dz = x.z - y.z;
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      const double ir = r2 > 0.0 ? rsqrt(r2) : 0.0;
+      const double qir = y.w * ir;
+      p += qir;
+      const double q3 = qir * ir * ir;
+      gx += q3 * dx;
+      gy += q3 * dy;
+      gz += q3 * dz;
+    }
+    const int b = L.boff + t;
+    phi[b] = p;
+    grad[3 * b + 0] = -gx;
+    grad[3 * b + 1] = -gy;
+    grad[3 * b + 2] = -gz;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Batched FP64 operator application:
+//   C[outrow[r]][n] = beta*C + scale[r] * sum_s sum_j A[inrow[r*S+s]][j] B[g][s][j][n]
+// 64x64 output tiles, 16-deep K steps, 4x4 outputs per thread.
+// ---------------------------------------------------------------------------
+constexpr int kTM = 64, kTN = 64, kTK = 16;
+
+__global__ void __launch_bounds__(256) k_apply_f64(ApplyBatch b) {
+  __shared__ double As[kTK][kTM + 1];
+  __shared__ double Bs[kTK][kTN];
+  __shared__ int rsrc[kTM];
+  const int g = blockIdx.z;
+  const int rbeg = b.group_off[g], rend = b.group_off[g + 1];
+  const int r0 = rbeg + blockIdx.y * kTM;
+  const int c0 = blockIdx.x * kTN;
+  if (r0 >= rend) return;  // block-uniform
+  const int ns = b.ns;
+  const double* Bg = b.B + (size_t)g * b.S * ns * ns;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  double acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+  for (int s = 0; s < b.S; ++s) {
+    __syncthreads();
+    if (tid < kTM) {
+      const int row = r0 + tid;
+      rsrc[tid] = row < rend ? b.inrow[(size_t)row * b.S + s] : -1;
+    }
+    __syncthreads();
+    for (int j0 = 0; j0 < ns; j0 += kTK) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int e = tid + 256 * u;
+        const int r = e >> 4, k = e & 15;
+        const int src = rsrc[r];
+        const int j = j0 + k;
+        As[k][r] = (src >= 0 && j < ns) ? b.A[(size_t)src * ns + j] : 0.0;
+        const int kk = e >> 6, c = e & 63;
+        const int jj = j0 + kk, n = c0 + c;
+        Bs[kk][c] = (jj < ns && n < ns) ? Bg[((size_t)s * ns + jj) * ns + n] : 0.0;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < kTK; ++k) {
+        double a[4], bb[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = As[k][ty + 16 * i];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) bb[j] = Bs[k][tx + 16 * j];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], bb[j], acc[i][j]);
+      }
+      __syncthreads();
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int row = r0 + ty + 16 * i;
+    if (row >= rend) continue;
+    const int o = b.outrow[row];
+    const double sc = b.scale ? b.scale[row] : 1.0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int n = c0 + tx + 16 * j;
+      if (n >= ns) continue;
+      double* cp = b.C + (size_t)o * ns + n;
+      *cp = b.beta ? *cp + sc * acc[i][j] : sc * acc[i][j];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FFT-M2L.  Grids are N = 2P-1 points per edge, stored [z][y][x]; spectra are
+// the r2c half-spectrum [kz][ky][kx], kx < P.  The twiddle table holds
+// w^m = exp(-2 pi i m / N) for m < N.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void cmad(T& re, T& im, T ar, T ai, T br, T bi) {
+  re = fma(ar, br, re);
+  re = fma(-ai, bi, re);
+  im = fma(ar, bi, im);
+  im = fma(ai, br, im);
+}
+
+// up: one block per (source parent, child slot): scatter the child's
+// equivalent density onto the [0,P)^3 corner of the grid
+// (surf_conv_idx_map_up, kernel.cpp:1246-1252, 1304-1315) and take its
+// forward DFT separably (x, then y, then z), writing Q[src][slot][f].
+template <typename T>
+__global__ void __launch_bounds__(256)
+    k_m2l_up(const double* __restrict__ q_equiv, const int* __restrict__ items,
+             const int* __restrict__ surf_ijk, const double* __restrict__ twiddle, int P, int ns,
+             T* __restrict__ Q) {
+  extern __shared__ unsigned char smem_raw[];
+  T* sm = reinterpret_cast<T*>(smem_raw);
+  const int N = 2 * P - 1;
+  const int P3 = P * P * P, Nf = N * N * P;
+  T* cube = sm;                    // P^3
+  T* A = cube + P3;                // P^3 complex: [z][y][kx]
+  T* Bm = A + 2 * P3;              // P*N*P complex: [z][ky][kx]
+  T* w = Bm + 2 * P * N * P;       // N complex
+  const int src = items[3 * blockIdx.x], slot = items[3 * blockIdx.x + 1], child = items[3 * blockIdx.x + 2];
+  T* out = Q + ((size_t)src * 8 + slot) * Nf * 2;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  if (child < 0) {
+    for (int f = tid; f < 2 * Nf; f += nt) out[f] = T(0);
+    return;
+  }
+  for (int m = tid; m < 2 * N; m += nt) w[m] = (T)twiddle[m];
+  for (int e = tid; e < P3; e += nt) cube[e] = T(0);
+  __syncthreads();
+  for (int i = tid; i < ns; i += nt) {
+    const int x = surf_ijk[3 * i], y = surf_ijk[3 * i + 1], z = surf_ijk[3 * i + 2];
+    cube[(z * P + y) * P + x] = (T)q_equiv[(size_t)child * ns + i];
+  }
+  __syncthreads();
+  for (int e = tid; e < P3; e += nt) {
+    const int z = e / (P * P), y = (e / P) % P, kx = e % P;
+    T re = 0, im = 0;
+    const T* row = cube + (z * P + y) * P;
+    for (int x = 0; x < P; ++x) {
+      const int m = (kx * x) % N;
+      re = fma(row[x], w[2 * m], re);
+      im = fma(row[x], w[2 * m + 1], im);
+    }
+    A[2 * e] = re;
+    A[2 * e + 1] = im;
+  }
+  __syncthreads();
+  for (int e = tid; e < P * N * P; e += nt) {
+    const int z = e / (N * P), ky = (e / P) % N, kx = e % P;
+    T re = 0, im = 0;
+    for (int y = 0; y < P; ++y) {
+      const int m = (ky * y) % N;
+      const int a = (z * P + y) * P + kx;
+      cmad(re, im, A[2 * a], A[2 * a + 1], w[2 * m], w[2 * m + 1]);
+    }
+    Bm[2 * e] = re;
+    Bm[2 * e + 1] = im;
+  }
+  __syncthreads();
+  for (int f = tid; f < Nf; f += nt) {
+    const int kz = f / (N * P), ky = (f / P) % N, kx = f % P;
+    T re = 0, im = 0;
+    for (int z = 0; z < P; ++z) {
+      const int m = (kz * z) % N;
+      const int b = (z * N + ky) * P + kx;
+      cmad(re, im, Bm[2 * b], Bm[2 * b + 1], w[2 * m], w[2 * m + 1]);
+    }
+    out[2 * f] = re;
+    out[2 * f + 1] = im;
+  }
+}
+
+// Hadamard 8x8 (hadamard_8x8 + c2c_8x8x2_avx, kernel.cpp:1012-1082, c2c.h:201-296):
+//   Pk[t][itar][f] = sum_d sum_isrc G[d][isrc][itar][f] * Q[src(t,d)][isrc][f]
+// Block = 32 frequencies x 8 warps; each warp owns 2 targets.  For each of
+// the 26 directions the block stages G_d for its 32 frequencies in shared
+// memory.  FP32 partial sums per direction are accumulated into FP64.
+constexpr int kHadWarps = 8, kHadTPW = 2, kHadTargets = kHadWarps * kHadTPW;
+
+template <typename T>
+__global__ void __launch_bounds__(32 * kHadWarps)
+    k_m2l_hadamard8(const T* __restrict__ Q, const T* __restrict__ G, const int* __restrict__ tsrc,
+                    int ntar, int Nf, T* __restrict__ Pk) {
+  using C2 = typename Cplx<T>::type;
+  __shared__ C2 Gs[64][32];
+  const int lane = threadIdx.x, warp = threadIdx.y;
+  const int tid = warp * 32 + lane;
+  const int f0 = blockIdx.y * 32;
+  const int f = f0 + lane;
+  int tt[kHadTPW];
+  bool tv[kHadTPW];
+#pragma unroll
+  for (int j = 0; j < kHadTPW; ++j) {
+    tt[j] = blockIdx.x * kHadTargets + warp * kHadTPW + j;
+    tv[j] = tt[j] < ntar;
+  }
+  double acc[kHadTPW][8][2];
+#pragma unroll
+  for (int j = 0; j < kHadTPW; ++j)
+#pragma unroll
+    for (int i = 0; i < 8; ++i) acc[j][i][0] = acc[j][i][1] = 0.0;
+  const C2* G2 = reinterpret_cast<const C2*>(G);
+  const C2* Q2 = reinterpret_cast<const C2*>(Q);
+  for (int d = 0; d < 26; ++d) {
+    int s[kHadTPW];
+    int any = 0;
+#pragma unroll
+    for (int j = 0; j < kHadTPW; ++j) {
+      s[j] = tv[j] ? tsrc[tt[j] * 26 + d] : -1;
+      any |= (s[j] >= 0);
+    }
+    if (!__syncthreads_or(any)) continue;
+    for (int e = tid; e < 64 * 32; e += 32 * kHadWarps) {
+      const int pair = e >> 5, fl = e & 31;
+      const int ff = f0 + fl;
+      C2 v;
+      v.x = T(0);
+      v.y = T(0);
+      if (ff < Nf) v = G2[((size_t)d * 64 + pair) * Nf + ff];
+      Gs[pair][fl] = v;
+    }
+    __syncthreads();
+    if (any && f < Nf) {
+      T pr[kHadTPW][8], pi[kHadTPW][8];
+#pragma unroll
+      for (int j = 0; j < kHadTPW; ++j)
+#pragma unroll
+        for (int i = 0; i < 8; ++i) pr[j][i] = pi[j][i] = T(0);
+#pragma unroll
+      for (int isrc = 0; isrc < 8; ++isrc) {
+        C2 q[kHadTPW];
+#pragma unroll
+        for (int j = 0; j < kHadTPW; ++j) {
+          q[j].x = T(0);
+          q[j].y = T(0);
+          if (s[j] >= 0) q[j] = Q2[((size_t)s[j] * 8 + isrc) * Nf + f];
+        }
+#pragma unroll
+        for (int itar = 0; itar < 8; ++itar) {
+          const C2 gv = Gs[isrc * 8 + itar][lane];
+#pragma unroll
+          for (int j = 0; j < kHadTPW; ++j) cmad(pr[j][itar], pi[j][itar], gv.x, gv.y, q[j].x, q[j].y);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kHadTPW; ++j)
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          acc[j][i][0] += (double)pr[j][i];
+          acc[j][i][1] += (double)pi[j][i];
+        }
+    }
+    __syncthreads();
+  }
+  if (f < Nf) {
+    C2* P2 = reinterpret_cast<C2*>(Pk);
+#pragma unroll
+    for (int j = 0; j < kHadTPW; ++j) {
+      if (!tv[j]) continue;
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        C2 v;
+        v.x = (T)acc[j][i][0];
+        v.y = (T)acc[j][i][1];
+        P2[((size_t)tt[j] * 8 + i) * Nf + f] = v;
+      }
+    }
+  }
+}
+
+// Hadamard 1x27 (hadamard_1x27 + c2c_1x27x1_AVX, kernel.cpp:1084-1138) for the
+// image levels, FP64; the 27 image spectra of a direction are pre-summed.
+__global__ void k_m2l_hadamard27(const double* __restrict__ Q, const double* __restrict__ G27,
+                                 const int* __restrict__ tsrc, int ntar, int Nf, double* __restrict__ Pk) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = blockIdx.y;
+  if (f >= Nf || t >= ntar) return;
+  double re = 0, im = 0;
+  for (int d = 0; d < 26; ++d) {
+    const int s = tsrc[t * 26 + d];
+    if (s < 0) continue;
+    const double gr = G27[((size_t)d * Nf + f) * 2], gi = G27[((size_t)d * Nf + f) * 2 + 1];
+    const size_t qo = (((size_t)s * 8 + 0) * Nf + f) * 2;
+    cmad(re, im, gr, gi, Q[qo], Q[qo + 1]);
+  }
+  const size_t po = (((size_t)t * 8 + 0) * Nf + f) * 2;
+  Pk[po] = re;
+  Pk[po + 1] = im;
+}
+
+// down: one block per (target parent, child): inverse DFT of Pk[t][slot]
+// evaluated only at the child's check-surface points, which sit at
+// [P-1, 2P-2]^3 of the grid (surf_conv_idx_map_down, kernel.cpp:1253-1259);
+// then p_check[child] += value * scale / N^3 (kernel.cpp:1369-1382).
+template <typename T>
+__global__ void __launch_bounds__(256)
+    k_m2l_down(const T* __restrict__ Pk, const int* __restrict__ items, const double* __restrict__ tscale,
+               const int* __restrict__ surf_ijk, const double* __restrict__ twiddle, int P, int ns,
+               double* __restrict__ p_check) {
+  extern __shared__ unsigned char smem_raw[];
+  T* sm = reinterpret_cast<T*>(smem_raw);
+  const int N = 2 * P - 1;
+  const int P3 = P * P * P, Nf = N * N * P;
+  T* X = sm;                        // Nf complex
+  T* Y1 = X + 2 * Nf;               // P*N*P complex: [zo][ky][kx]
+  T* Y2 = Y1 + 2 * P * N * P;       // P^3 complex: [zo][yo][kx]
+  T* w = Y2 + 2 * P3;               // N complex
+  const int tar = items[3 * blockIdx.x], slot = items[3 * blockIdx.x + 1], child = items[3 * blockIdx.x + 2];
+  const T* in = Pk + ((size_t)tar * 8 + slot) * Nf * 2;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int m = tid; m < 2 * N; m += nt) w[m] = (T)twiddle[m];
+  for (int e = tid; e < 2 * Nf; e += nt) X[e] = in[e];
+  __syncthreads();
+  for (int e = tid; e < P * N * P; e += nt) {
+    const int zo = e / (N * P), ky = (e / P) % N, kx = e % P;
+    const int z = P - 1 + zo;
+    T re = 0, im = 0;
+    for (int kz = 0; kz < N; ++kz) {
+      const int m = (kz * z) % N;
+      const int a = (kz * N + ky) * P + kx;
+      cmad(re, im, X[2 * a], X[2 * a + 1], w[2 * m], -w[2 * m + 1]);
+    }
+    Y1[2 * e] = re;
+    Y1[2 * e + 1] = im;
+  }
+  __syncthreads();
+  for (int e = tid; e < P3; e += nt) {
+    const int zo = e / (P * P), yo = (e / P) % P, kx = e % P;
+    const int y = P - 1 + yo;
+    T re = 0, im = 0;
+    for (int ky = 0; ky < N; ++ky) {
+      const int m = (ky * y) % N;
+      const int a = (zo * N + ky) * P + kx;
+      cmad(re, im, Y1[2 * a], Y1[2 * a + 1], w[2 * m], -w[2 * m + 1]);
+    }
+    Y2[2 * e] = re;
+    Y2[2 * e + 1] = im;
+  }
+  __syncthreads();
+  const double sc = tscale[tar];
+  for (int i = tid; i < ns; i += nt) {
+    const int xo = surf_ijk[3 * i], yo = surf_ijk[3 * i + 1], zo = surf_ijk[3 * i + 2];
+    const int x = P - 1 + xo;
+    const T* row = Y2 + 2 * ((zo * P + yo) * P);
+    T v = row[0];
+    T acc = 0;
+    for (int kx = 1; kx < P; ++kx) {
+      const int m = (kx * x) % N;
+      // Re(Y * conj(w^m)) = Yr * wr + Yi * wi
+      acc = fma(row[2 * kx], w[2 * m], acc);
+      acc = fma(row[2 * kx + 1], w[2 * m + 1], acc);
+    }
+    v += T(2) * acc;
+    p_check[(size_t)child * ns + i] += (double)v * sc;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// post: far + near, dipole correction (kernel.cpp:1580-1596), 1/(4 pi)
+// (body.cpp:88-96), and the scatter back to input order (body.cpp:177-190).
+// ---------------------------------------------------------------------------
+constexpr int kDipBlocks = 256;
+
+__global__ void k_dipole_partial(const double4* __restrict__ body64, int n, double* __restrict__ partial) {
+  __shared__ double s[3][256];
+  double ax = 0, ay = 0, az = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double4 b = body64[i];
+    ax += b.x * b.w;
+    ay += b.y * b.w;
+    az += b.z * b.w;
+  }
+  s[0][threadIdx.x] = ax;
+  s[1][threadIdx.x] = ay;
+  s[2][threadIdx.x] = az;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h)
+      for (int k = 0; k < 3; ++k) s[k][threadIdx.x] += s[k][threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; ++k) partial[blockIdx.x * 3 + k] = s[k][0];
+}
+
+__global__ void k_dipole_final(double* __restrict__ partial) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double d[3] = {0, 0, 0};
+  for (int b = 0; b < kDipBlocks; ++b)
+    for (int k = 0; k < 3; ++k) d[k] += partial[b * 3 + k];
+  for (int k = 0; k < 3; ++k) partial[3 * kDipBlocks + k] = d[k];
+}
+
+__global__ void k_post(const double* __restrict__ phi_far, const double* __restrict__ grad_far,
+                       const double* __restrict__ phi_near, const double* __restrict__ grad_near,
+                       const double4* __restrict__ body64, const int64_t* __restrict__ perm, int n,
+                       const double* __restrict__ dip, double coef, int dipole, double out_scale,
+                       double* __restrict__ out_phi, double* __restrict__ out_grad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double p = 0, g0 = 0, g1 = 0, g2 = 0;
+  if (phi_far) {
+    p += phi_far[i];
+    g0 += grad_far[3 * i];
+    g1 += grad_far[3 * i + 1];
+    g2 += grad_far[3 * i + 2];
+  }
+  if (phi_near) {
+    p += phi_near[i];
+    g0 += grad_near[3 * i];
+    g1 += grad_near[3 * i + 1];
+    g2 += grad_near[3 * i + 2];
+  }
+  if (dipole) {
+    const double dx = dip[0], dy = dip[1], dz = dip[2];
+    const double dnorm = dx * dx + dy * dy + dz * dz;
+    p -= coef * dnorm / n / body64[i].w;
+    g0 -= coef * dx;
+    g1 -= coef * dy;
+    g2 -= coef * dz;
+  }
+  const int64_t o = perm[i];
+  out_phi[o] = p * out_scale;
+  out_grad[3 * o + 0] = g0 * out_scale;
+  out_grad[3 * o + 1] = g1 * out_scale;
+  out_grad[3 * o + 2] = g2 * out_scale;
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+static inline int cdiv(int64_t a, int b) { return (int)((a + b - 1) / b); }
+
+cudaError_t launch_gather_bodies(const double* x_in, const double* q_in, const int64_t* perm, int n,
+                                 double4* body64, cudaStream_t st) {
+  if (n > 0) k_gather_bodies<<<cdiv(n, 256), 256, 0, st>>>(x_in, q_in, perm, n, body64);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_prep32(const double4* body64, const int* body_leaf, const LeafInfo* leaves,
+                          float4* body32, int n, cudaStream_t st) {
+  if (n > 0) k_prep32<<<cdiv(n, 256), 256, 0, st>>>(body64, body_leaf, leaves, body32, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_p2p32(const float4* body32, const LeafInfo* leaves, const P2PItem* items, int nitems,
+                         const int* list_off, const P2PSrc32* list, double* phi, double* grad,
+                         cudaStream_t st) {
+  if (nitems > 0)
+    k_p2p32<<<cdiv(nitems, kP2PWarps), 32 * kP2PWarps, 0, st>>>(body32, leaves, items, nitems, list_off,
+                                                               list, phi, grad);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_p2p64(const double4* body64, const LeafInfo* leaves, const P2PItem* items, int nitems,
+                         const int* list_off, const P2PSrc64* list, double* phi, double* grad,
+                         cudaStream_t st) {
+  if (nitems > 0)
+    k_p2p64<<<cdiv(nitems, kP2PWarps), 32 * kP2PWarps, 0, st>>>(body64, leaves, items, nitems, list_off,
+                                                               list, phi, grad);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_p2m_check(const double4* body64, const LeafInfo* leaves, int nleaf,
+                             const double* surf_unit, int ns, double* out, cudaStream_t st) {
+  if (nleaf > 0) k_p2m_check<<<nleaf, kSurfThreads, 0, st>>>(body64, leaves, surf_unit, ns, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_l2p_eval(const double4* body64, const LeafInfo* leaves, int nleaf,
+                            const double* surf_unit, int ns, const double* q_down, double* phi,
+                            double* grad, cudaStream_t st) {
+  if (nleaf > 0) {
+    const size_t sm = sizeof(double4) * ns;
+    if (sm > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(k_l2p_eval, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      if (e != cudaSuccess) return e;
+    }
+    k_l2p_eval<<<nleaf, kSurfThreads, sm, st>>>(body64, leaves, surf_unit, ns, q_down, phi, grad);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_apply(const ApplyBatch& b, cudaStream_t st) {
+  if (b.max_rows > 0 && b.groups > 0) {
+    dim3 grid(cdiv(b.ns, kTN), cdiv(b.max_rows, kTM), b.groups);
+    k_apply_f64<<<grid, 256, 0, st>>>(b);
+  }
+  return cudaGetLastError();
+}
+
+template <typename T>
+static size_t up_smem(int P) {
+  const int N = 2 * P - 1;
+  return sizeof(T) * ((size_t)3 * P * P * P + 2 * (size_t)P * N * P + 2 * N);
+}
+template <typename T>
+static size_t down_smem(int P) {
+  const int N = 2 * P - 1;
+  return sizeof(T) * (2 * (size_t)N * N * P + 2 * (size_t)P * N * P + 2 * (size_t)P * P * P + 2 * N);
+}
+
+template <typename T>
+cudaError_t launch_m2l_up(const double* q_equiv, const int* items, int nitems, const int* surf_ijk,
+                          const double* twiddle, int P, int ns, T* Q, cudaStream_t st) {
+  if (nitems > 0) {
+    const size_t sm = up_smem<T>(P);
+    cudaError_t e = cudaFuncSetAttribute(k_m2l_up<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    k_m2l_up<T><<<nitems, 256, sm, st>>>(q_equiv, items, surf_ijk, twiddle, P, ns, Q);
+  }
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_m2l_hadamard8(const T* Q, const T* G, const int* tsrc, int ntar, int Nf, T* Pk,
+                                 cudaStream_t st) {
+  if (ntar > 0) {
+    dim3 grid(cdiv(ntar, kHadTargets), cdiv(Nf, 32));
+    k_m2l_hadamard8<T><<<grid, dim3(32, kHadWarps), 0, st>>>(Q, G, tsrc, ntar, Nf, Pk);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_m2l_hadamard27(const double* Q, const double* G27, const int* tsrc, int ntar, int Nf,
+                                  double* Pk, cudaStream_t st) {
+  if (ntar > 0) {
+    dim3 grid(cdiv(Nf, 128), ntar);
+    k_m2l_hadamard27<<<grid, 128, 0, st>>>(Q, G27, tsrc, ntar, Nf, Pk);
+  }
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_m2l_down(const T* Pk, const int* items, const double* tscale, int nitems,
+                            const int* surf_ijk, const double* twiddle, int P, int ns, double* p_check,
+                            cudaStream_t st) {
+  if (nitems > 0) {
+    const size_t sm = down_smem<T>(P);
+    cudaError_t e = cudaFuncSetAttribute(k_m2l_down<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    k_m2l_down<T><<<nitems, 256, sm, st>>>(Pk, items, tscale, surf_ijk, twiddle, P, ns, p_check);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dipole(const double4* body64, int n, double* partial, cudaStream_t st) {
+  k_dipole_partial<<<kDipBlocks, 256, 0, st>>>(body64, n, partial);
+  k_dipole_final<<<1, 32, 0, st>>>(partial);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_post(const double* phi_far, const double* grad_far, const double* phi_near,
+                        const double* grad_near, const double4* body64, const int64_t* perm, int n,
+                        const double* dipole_partial, double coef, int dipole, double out_scale,
+                        double* out_phi, double* out_grad, cudaStream_t st) {
+  if (n > 0)
+    k_post<<<cdiv(n, 256), 256, 0, st>>>(phi_far, grad_far, phi_near, grad_near, body64, perm, n,
+                                          dipole_partial + 3 * kDipBlocks, coef, dipole, out_scale, out_phi,
+                                          out_grad);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_m2l_up<float>(const double*, const int*, int, const int*, const double*, int, int,
+                                          float*, cudaStream_t);
+template cudaError_t launch_m2l_up<double>(const double*, const int*, int, const int*, const double*, int, int,
+                                           double*, cudaStream_t);
+template cudaError_t launch_m2l_hadamard8<float>(const float*, const float*, const int*, int, int, float*,
+                                                 cudaStream_t);
+template cudaError_t launch_m2l_hadamard8<double>(const double*, const double*, const int*, int, int, double*,
+                                                  cudaStream_t);
+template cudaError_t launch_m2l_down<float>(const float*, const int*, const double*, int, const int*,
+                                            const double*, int, int, double*, cudaStream_t);
+template cudaError_t launch_m2l_down<double>(const double*, const int*, const double*, int, const int*,
+                                             const double*, int, int, double*, cudaStream_t);
+
+}  // namespace rtfmm_b200

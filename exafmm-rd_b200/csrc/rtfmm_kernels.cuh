@@ -1,0 +1,87 @@
+// Device kernels of the evaluation pass (sm_100a).  Declarations shared by
+// rtfmm_kernels.cu and the orchestration in rtfmm_capi.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace rtfmm_b200 {
+
+// Leaf table: one entry per leaf cell.
+struct LeafInfo {
+  double cx, cy, cz;   // centre
+  double r;            // half edge
+  double scale;        // 0.5^depth (P2M / L2P operator rescaling)
+  int cell;            // cell index
+  int boff, bnum;      // bodies in tree order
+};
+
+// FP32 P2P work item: up to 32 targets of one leaf.
+struct P2PItem {
+  int leaf;   // leaf-table index of the target leaf
+  int t0;     // first target (offset inside the leaf)
+};
+
+// One P2P list entry (source leaf) of a target leaf, both precisions.
+struct P2PSrc32 {
+  float dx, dy, dz;   // c_src + offset - c_tar, for leaf-relative FP32 positions
+  int leaf;           // leaf-table index of the source leaf
+  int self;           // source == target with zero offset (mask r == 0)
+  int pad[3];
+};
+struct P2PSrc64 {
+  double ox, oy, oz;  // periodic offset added to the source positions
+  int leaf;
+  int self;
+};
+
+// Batched FP64 operator application (see k_apply_f64).
+struct ApplyBatch {
+  const double* A;      // input vectors, row stride ns
+  const int* inrow;     // rows*S input row indices (-1 = zero vector)
+  const double* B;      // groups x S x ns x ns operator stack, row-major [s][j][n]
+  const int* outrow;    // output row indices
+  const double* scale;  // per-row scale (nullptr = 1)
+  const int* group_off; // groups+1 row offsets
+  double* C;            // output vectors, row stride ns
+  int groups, S, ns, beta;
+  int max_rows;         // rows of the largest group (grid sizing)
+};
+
+// Launch helpers (all asynchronous on `st`; return cudaGetLastError()).
+cudaError_t launch_prep32(const double4* body64, const int* body_leaf, const LeafInfo* leaves,
+                          float4* body32, int n, cudaStream_t st);
+cudaError_t launch_p2p32(const float4* body32, const LeafInfo* leaves, const P2PItem* items, int nitems,
+                         const int* list_off, const P2PSrc32* list, double* phi, double* grad,
+                         cudaStream_t st);
+cudaError_t launch_p2p64(const double4* body64, const LeafInfo* leaves, const P2PItem* items, int nitems,
+                         const int* list_off, const P2PSrc64* list, double* phi, double* grad,
+                         cudaStream_t st);
+cudaError_t launch_p2m_check(const double4* body64, const LeafInfo* leaves, int nleaf,
+                             const double* surf_unit, int ns, double* out, cudaStream_t st);
+cudaError_t launch_apply(const ApplyBatch& b, cudaStream_t st);
+template <typename T>
+cudaError_t launch_m2l_up(const double* q_equiv, const int* items /*(src,slot,child)*/, int nitems,
+                          const int* surf_ijk, const double* twiddle, int P, int ns, T* Q,
+                          cudaStream_t st);
+template <typename T>
+cudaError_t launch_m2l_hadamard8(const T* Q, const T* G, const int* tsrc, int ntar, int Nf, T* Pk,
+                                 cudaStream_t st);
+cudaError_t launch_m2l_hadamard27(const double* Q, const double* G27, const int* tsrc, int ntar, int Nf,
+                                  double* Pk, cudaStream_t st);
+template <typename T>
+cudaError_t launch_m2l_down(const T* Pk, const int* items /*(tar,slot,child)*/, const double* tscale,
+                            int nitems, const int* surf_ijk, const double* twiddle, int P, int ns,
+                            double* p_check, cudaStream_t st);
+cudaError_t launch_l2p_eval(const double4* body64, const LeafInfo* leaves, int nleaf,
+                            const double* surf_unit, int ns, const double* q_down, double* phi,
+                            double* grad, cudaStream_t st);
+cudaError_t launch_dipole(const double4* body64, int n, double* partial /*>= 4*1024*/, cudaStream_t st);
+cudaError_t launch_post(const double* phi_far, const double* grad_far, const double* phi_near,
+                        const double* grad_near, const double4* body64, const int64_t* perm, int n,
+                        const double* dipole_partial, double coef, int dipole, double out_scale,
+                        double* out_phi, double* out_grad, cudaStream_t st);
+cudaError_t launch_gather_bodies(const double* x_in, const double* q_in, const int64_t* perm, int n,
+                                 double4* body64, cudaStream_t st);
+
+}  // namespace rtfmm_b200

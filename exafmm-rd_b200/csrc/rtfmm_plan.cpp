@@ -1,0 +1,629 @@
+// Host-side set-up: adaptive octree, interaction lists and FP64 operator
+// tables.  These restate the reference's algorithms so that the lists and the
+// operators are the same sets the reference builds; the evaluation pass
+// itself runs on the GPU (rtfmm_kernels.cu).
+#include "rtfmm_plan.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <unordered_map>
+#include <utility>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
+namespace rtfmm_b200 {
+
+static const int kMaxDepth = 40;
+
+// ---------------------------------------------------------------------------
+// octree: Tree::build_nonuniform_octree (3dpp/src/tree.cpp:102-188)
+// ---------------------------------------------------------------------------
+static V3 child_center(const V3& xp, double rp, int octant) {
+  // Tree::get_child_cell_x, non-periodic branch (tree.cpp:198-209)
+  V3 c;
+  c[0] = xp[0] + ((octant & 4) ? rp / 2 : -rp / 2);
+  c[1] = xp[1] + ((octant & 2) ? rp / 2 : -rp / 2);
+  c[2] = xp[2] + ((octant & 1) ? rp / 2 : -rp / 2);
+  return c;
+}
+
+std::string build_tree(Plan& plan, const double* xin, const double* qin) {
+  const int64_t n = plan.n;
+  const Args& a = plan.args;
+  plan.r0 = a.cycle / 2;
+  plan.cells.clear();
+  plan.perm.resize(n);
+  for (int64_t i = 0; i < n; ++i) plan.perm[i] = i;
+  std::vector<int64_t> tmp(n);
+  std::vector<uint8_t> code(n);
+
+  Cell root;
+  root.octant = 13;
+  root.depth = 0;
+  root.r = plan.r0;
+  root.x = a.x;
+  root.coff = 0;
+  root.cnum = 0;
+  root.boff = 0;
+  root.bnum = (int)n;
+  plan.cells.push_back(root);
+  size_t head = 0;
+  while (head < plan.cells.size()) {
+    int c = (int)head++;
+    Cell cell = plan.cells[c];
+    if (cell.bnum <= a.ncrit) continue;
+    if (cell.depth >= kMaxDepth)
+      return "octree deeper than 40 levels: more than ncrit bodies share a position";
+    const int b0 = cell.boff, nb = cell.bnum;
+    int count[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int i = 0; i < nb; ++i) {
+      const double* p = xin + 3 * plan.perm[b0 + i];
+      int o = ((p[0] > cell.x[0]) << 2) + ((p[1] > cell.x[1]) << 1) + (p[2] > cell.x[2]);
+      code[b0 + i] = (uint8_t)o;
+      count[o]++;
+    }
+    int start[8], nchild = 0, s = 0;
+    for (int o = 0; o < 8; ++o) {
+      start[o] = s;
+      s += count[o];
+      if (count[o] > 0) nchild++;
+    }
+    int fill[8];
+    std::memcpy(fill, start, sizeof(fill));
+    for (int i = 0; i < nb; ++i) tmp[fill[code[b0 + i]]++] = plan.perm[b0 + i];
+    std::memcpy(&plan.perm[b0], tmp.data(), sizeof(int64_t) * nb);
+    const int insert = (int)plan.cells.size();
+    plan.cells[c].coff = insert;
+    plan.cells[c].cnum = nchild;
+    for (int o = 0; o < 8; ++o) {
+      if (count[o] == 0) continue;
+      Cell ch;
+      ch.octant = o;
+      ch.depth = cell.depth + 1;
+      ch.r = cell.r / 2;
+      ch.x = child_center(cell.x, cell.r, o);
+      ch.coff = 0;
+      ch.cnum = 0;
+      ch.boff = b0 + start[o];
+      ch.bnum = count[o];
+      plan.cells.push_back(ch);
+    }
+  }
+  plan.ntree = (int)plan.cells.size();
+  plan.x.resize(3 * n);
+  plan.q.resize(n);
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t k = plan.perm[i];
+    plan.x[3 * i + 0] = xin[3 * k + 0];
+    plan.x[3 * i + 1] = xin[3 * k + 1];
+    plan.x[3 * i + 2] = xin[3 * k + 2];
+    plan.q[i] = qin[k];
+  }
+  return "";
+}
+
+// ---------------------------------------------------------------------------
+// lists: Traverser (3dpp/src/traverser.cpp)
+// ---------------------------------------------------------------------------
+namespace {
+
+struct Walker {
+  Plan& p;
+  explicit Walker(Plan& pl) : p(pl) {}
+
+  // adjacent(a, b, offset): |x_a - x_b - offset| <= (r_a + r_b) * 1.001 per axis
+  // (traverser.cpp:314-321), evaluated with the same operation order.
+  bool adjacent(int a, int b, const V3& off) const {
+    const Cell& ca = p.cells[a];
+    const Cell& cb = p.cells[b];
+    const double dist = (ca.r + cb.r) * 1.001;
+    for (int k = 0; k < 3; ++k) {
+      double d = std::fabs((ca.x[k] - cb.x[k]) - off[k]);
+      if (!(d <= dist)) return false;
+    }
+    return true;
+  }
+  bool neighbour(int a, int b, const V3& off) const {
+    return adjacent(a, b, off) && p.cells[a].depth == p.cells[b].depth;
+  }
+  bool leaf(int c) const { return p.cells[c].cnum == 0; }
+
+  // horizontal_origin (traverser.cpp:70-148) with an explicit stack; children
+  // are visited in the reference's recursion order.  M2P/P2L cases become P2P
+  // (traverser.cpp:75-86); M2L pairs of the dual walk are counted only (the
+  // M2L of the pass uses the parent map).
+  void horizontal_origin(int tc0, int sc0, int tcp0, int scp0, const V3& off) {
+    struct Frame { int tc, sc, tcp, scp; };
+    std::vector<Frame> stack;
+    stack.push_back({tc0, sc0, tcp0, scp0});
+    while (!stack.empty()) {
+      Frame f = stack.back();
+      stack.pop_back();
+      int divide = 0;
+      const Cell& T = p.cells[f.tc];
+      const Cell& S = p.cells[f.sc];
+      if (!adjacent(f.tc, f.sc, off)) {
+        if (adjacent(f.tc, f.scp, off) && leaf(f.tc) && p.cells[f.scp].depth >= T.depth) {
+          p.p2p[f.tc].push_back({f.sc, off});
+        } else if (adjacent(f.tcp, f.sc, off) && leaf(f.sc) && p.cells[f.tcp].depth >= S.depth) {
+          p.p2p[f.tc].push_back({f.sc, off});
+        } else if (neighbour(f.tcp, f.scp, off)) {
+          // an M2L pair of the dual walk; served by the parent map
+        } else {
+          if (leaf(f.tc) && leaf(f.sc)) {
+          } else if (!leaf(f.tc) && leaf(f.sc)) {
+            divide = 1;
+          } else if (leaf(f.tc) && !leaf(f.sc)) {
+            divide = 2;
+          } else {
+            divide = T.r >= S.r ? 1 : 2;
+          }
+        }
+      } else {
+        if (leaf(f.tc) && leaf(f.sc)) {
+          p.p2p[f.tc].push_back({f.sc, off});
+        } else if (!leaf(f.tc) && leaf(f.sc)) {
+          divide = 1;
+        } else if (leaf(f.tc) && !leaf(f.sc)) {
+          divide = 2;
+        } else {
+          divide = T.r >= S.r ? 1 : 2;
+        }
+      }
+      if (divide == 1) {
+        for (int i = T.cnum - 1; i >= 0; --i) stack.push_back({T.coff + i, f.sc, f.tc, f.scp});
+      } else if (divide == 2) {
+        for (int i = S.cnum - 1; i >= 0; --i) stack.push_back({f.tc, S.coff + i, f.tcp, f.sc});
+      }
+    }
+  }
+};
+
+}  // namespace
+
+void traverse(Plan& plan) {
+  const Args& a = plan.args;
+  const double cycle = a.cycle;
+  Walker w(plan);
+  plan.p2p.clear();
+  plan.m2l.clear();
+  // The depth -1 super-cell exists before the tree-level M2L parent map is
+  // built (traverser.cpp:30-35); deeper image cells are added afterwards.
+  if (a.images == 0) {
+    w.horizontal_origin(0, 0, 0, 0, V3{0, 0, 0});
+  } else {
+    Cell c;
+    c.octant = 13;
+    c.depth = -1;
+    c.r = plan.cells[0].r * 3;
+    c.x = plan.cells[0].x;
+    c.coff = 0;
+    c.cnum = 1;
+    c.boff = 0;
+    c.bnum = plan.cells[0].bnum;
+    plan.cells.push_back(c);
+    const int cidx = (int)plan.cells.size() - 1;
+    for (int pz = -1; pz <= 1; ++pz)
+      for (int py = -1; py <= 1; ++py)
+        for (int px = -1; px <= 1; ++px) {
+          V3 off{px * cycle, py * cycle, pz * cycle};
+          w.horizontal_origin(0, 0, cidx, cidx, off);
+        }
+  }
+
+  // M2L parent map over the tree cells (make_M2L_parent_map and the
+  // periodic part of make_M2L_parent_map_i1, traverser.cpp:234-282).  The
+  // reference tests every cell pair; same-depth cells sit on a lattice of
+  // spacing 2r, so the same predicate is evaluated here through a hash of
+  // lattice coordinates: a source at lattice displacement v in {-1,0,1}^3
+  // (wrapped periodically when images >= 1) with offset p * cycle.
+  std::unordered_map<uint64_t, int> lattice;
+  auto key = [](int depth, int64_t i, int64_t j, int64_t k) {
+    return ((uint64_t)depth << 57) ^ ((uint64_t)i << 38) ^ ((uint64_t)j << 19) ^ (uint64_t)k;
+  };
+  const V3 lo{a.x[0] - plan.r0, a.x[1] - plan.r0, a.x[2] - plan.r0};
+  std::vector<std::array<int64_t, 3>> coord(plan.ntree);
+  for (int c = 0; c < plan.ntree; ++c) {
+    const Cell& cl = plan.cells[c];
+    for (int k = 0; k < 3; ++k)
+      coord[c][k] = (int64_t)std::llround((cl.x[k] - lo[k]) / (2 * cl.r) - 0.5);
+    if (cl.cnum > 0) lattice[key(cl.depth, coord[c][0], coord[c][1], coord[c][2])] = c;
+  }
+  for (int j = 0; j < plan.ntree; ++j) {
+    const Cell& T = plan.cells[j];
+    if (T.cnum == 0) continue;
+    const int64_t nside = (int64_t)1 << T.depth;
+    std::vector<M2LEntry> near, far;
+    for (int vz = -1; vz <= 1; ++vz)
+      for (int vy = -1; vy <= 1; ++vy)
+        for (int vx = -1; vx <= 1; ++vx) {
+          if (vx == 0 && vy == 0 && vz == 0) continue;
+          int64_t m[3] = {coord[j][0] + vx, coord[j][1] + vy, coord[j][2] + vz};
+          int pw[3] = {0, 0, 0};
+          bool inside = true;
+          for (int k = 0; k < 3; ++k) {
+            if (m[k] < 0) { m[k] += nside; pw[k] = -1; }
+            else if (m[k] >= nside) { m[k] -= nside; pw[k] = 1; }
+            if (pw[k] != 0) inside = false;
+          }
+          if (!inside && a.images == 0) continue;
+          auto it = lattice.find(key(T.depth, m[0], m[1], m[2]));
+          if (it == lattice.end()) continue;
+          V3 off{pw[0] * cycle, pw[1] * cycle, pw[2] * cycle};
+          // confirm with the reference's own predicate
+          if (!w.neighbour(j, it->second, off)) continue;
+          (inside ? near : far).push_back({it->second, off, 0});
+        }
+    if (!near.empty() || !far.empty()) {
+      auto& lst = plan.m2l[j];
+      lst.insert(lst.end(), near.begin(), near.end());
+      lst.insert(lst.end(), far.begin(), far.end());
+    }
+  }
+
+  if (a.images >= 2) {
+    // horizontal_periodic_far: image super-cells at depth -2 .. -images
+    // (traverser.cpp:178-196), each the single parent of the one above.
+    int child = (int)plan.cells.size() - 1;
+    for (int m = 1; m < a.images; ++m) {
+      Cell c;
+      c.octant = 13;
+      c.depth = -1 - m;
+      c.r = plan.cells[child].r * 3;
+      c.x = plan.cells[child].x;
+      c.coff = child;
+      c.cnum = 1;
+      c.boff = 0;
+      c.bnum = 0;
+      plan.cells.push_back(c);
+      child = (int)plan.cells.size() - 1;
+    }
+    // image-level parent entries (traverser.cpp:43-64)
+    const int idx = (int)plan.cells.size() - 1 - a.images;
+    for (int m = 1; m < a.images; ++m) {
+      const int ci = idx + m;
+      const double r = plan.cells[ci].r;
+      for (int pz = -1; pz <= 1; ++pz)
+        for (int py = -1; py <= 1; ++py)
+          for (int px = -1; px <= 1; ++px) {
+            if (px == 0 && py == 0 && pz == 0) continue;
+            V3 off{px * r * 2, py * r * 2, pz * r * 2};
+            plan.m2l[ci].push_back({ci, off, 1});
+          }
+    }
+  }
+  plan.dmin = plan.dmax = plan.cells[0].depth;
+  for (const Cell& c : plan.cells) {
+    plan.dmin = std::min(plan.dmin, c.depth);
+    plan.dmax = std::max(plan.dmax, c.depth);
+  }
+  plan.n_p2p = 0;
+  for (auto& kv : plan.p2p) plan.n_p2p += (int64_t)kv.second.size();
+  plan.n_m2l = 0;
+  for (auto& kv : plan.m2l) plan.n_m2l += (int64_t)kv.second.size();
+}
+
+// ---------------------------------------------------------------------------
+// dense helpers
+// ---------------------------------------------------------------------------
+// One-sided (Hestenes) Jacobi SVD of a square row-major matrix: rotate column
+// pairs of W = A V until they are mutually orthogonal; then W = U S.  Pairs
+// follow a round-robin tournament so that each round's rotations are
+// independent and run in parallel.
+void jacobi_svd(int n, const double* A, std::vector<double>& U, std::vector<double>& s,
+                std::vector<double>& V) {
+  const int m = n + (n & 1);
+  std::vector<double> W((size_t)m * n, 0.0), Vc((size_t)m * m, 0.0);
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) W[(size_t)j * n + i] = A[(size_t)i * n + j];
+  for (int j = 0; j < m; ++j) Vc[(size_t)j * m + j] = 1.0;
+  std::vector<int> ring(m);
+  for (int i = 0; i < m; ++i) ring[i] = i;
+  for (int sweep = 0; sweep < 40; ++sweep) {
+    double off_max = 0.0;
+    for (int round = 0; round < m - 1; ++round) {
+#pragma omp parallel for schedule(static) reduction(max : off_max)
+      for (int k = 0; k < m / 2; ++k) {
+        int p = ring[k], q = ring[m - 1 - k];
+        if (p > q) std::swap(p, q);
+        if (q >= n) continue;  // padding column
+        double* wp = &W[(size_t)p * n];
+        double* wq = &W[(size_t)q * n];
+        double alpha = 0, beta = 0, gamma = 0;
+        for (int i = 0; i < n; ++i) {
+          alpha += wp[i] * wp[i];
+          beta += wq[i] * wq[i];
+          gamma += wp[i] * wq[i];
+        }
+        if (alpha == 0.0 || beta == 0.0) continue;
+        const double rel = std::fabs(gamma) / std::sqrt(alpha * beta);
+        off_max = std::max(off_max, rel);
+        if (rel < 1e-15) continue;
+        const double zeta = (beta - alpha) / (2.0 * gamma);
+        const double t = (zeta >= 0 ? 1.0 : -1.0) / (std::fabs(zeta) + std::sqrt(1.0 + zeta * zeta));
+        const double c = 1.0 / std::sqrt(1.0 + t * t);
+        const double sn = c * t;
+        for (int i = 0; i < n; ++i) {
+          const double a1 = wp[i], b1 = wq[i];
+          wp[i] = c * a1 - sn * b1;
+          wq[i] = sn * a1 + c * b1;
+        }
+        double* vp = &Vc[(size_t)p * m];
+        double* vq = &Vc[(size_t)q * m];
+        for (int i = 0; i < n; ++i) {
+          const double a1 = vp[i], b1 = vq[i];
+          vp[i] = c * a1 - sn * b1;
+          vq[i] = sn * a1 + c * b1;
+        }
+      }
+      // rotate the tournament ring, keeping ring[0] fixed
+      int last = ring[m - 1];
+      for (int i = m - 1; i > 1; --i) ring[i] = ring[i - 1];
+      ring[1] = last;
+    }
+    if (off_max < 1e-15) break;
+  }
+  std::vector<std::pair<double, int>> sv(n);
+  for (int j = 0; j < n; ++j) {
+    double nr = 0;
+    for (int i = 0; i < n; ++i) nr += W[(size_t)j * n + i] * W[(size_t)j * n + i];
+    sv[j] = {std::sqrt(nr), j};
+  }
+  std::sort(sv.begin(), sv.end(), [](const std::pair<double, int>& x, const std::pair<double, int>& y) {
+    return x.first > y.first;
+  });
+  U.assign((size_t)n * n, 0.0);
+  V.assign((size_t)n * n, 0.0);
+  s.assign(n, 0.0);
+  for (int k = 0; k < n; ++k) {
+    const int j = sv[k].second;
+    s[k] = sv[k].first;
+    for (int i = 0; i < n; ++i) {
+      U[(size_t)i * n + k] = s[k] > 0 ? W[(size_t)j * n + i] / s[k] : 0.0;
+      V[(size_t)i * n + k] = Vc[(size_t)j * m + i];
+    }
+  }
+}
+
+// Real-to-complex 3D DFT of an N^3 grid stored [z][y][x] (x fastest), forward
+// sign e^{-2 pi i k.n / N}, unnormalised; output [kz][ky][kx] with
+// kx in [0, N/2] (the half-spectrum layout of an r2c transform).
+void dft3_r2c(int N, const double* in, double* out) {
+  const int Nh = N / 2 + 1;
+  std::vector<double> cs(N), sn(N);
+  for (int m = 0; m < N; ++m) {
+    cs[m] = std::cos(2.0 * M_PI * m / N);
+    sn[m] = -std::sin(2.0 * M_PI * m / N);
+  }
+  std::vector<double> a((size_t)N * N * Nh * 2), b((size_t)N * N * Nh * 2);
+  for (int z = 0; z < N; ++z)
+    for (int y = 0; y < N; ++y)
+      for (int kx = 0; kx < Nh; ++kx) {
+        double re = 0, im = 0;
+        for (int x = 0; x < N; ++x) {
+          const int t = (kx * x) % N;
+          const double v = in[((size_t)z * N + y) * N + x];
+          re += v * cs[t];
+          im += v * sn[t];
+        }
+        size_t o = (((size_t)z * N + y) * Nh + kx) * 2;
+        a[o] = re;
+        a[o + 1] = im;
+      }
+  for (int z = 0; z < N; ++z)
+    for (int ky = 0; ky < N; ++ky)
+      for (int kx = 0; kx < Nh; ++kx) {
+        double re = 0, im = 0;
+        for (int y = 0; y < N; ++y) {
+          const int t = (ky * y) % N;
+          size_t o = (((size_t)z * N + y) * Nh + kx) * 2;
+          re += a[o] * cs[t] - a[o + 1] * sn[t];
+          im += a[o] * sn[t] + a[o + 1] * cs[t];
+        }
+        size_t o = (((size_t)z * N + ky) * Nh + kx) * 2;
+        b[o] = re;
+        b[o + 1] = im;
+      }
+  for (int kz = 0; kz < N; ++kz)
+    for (int ky = 0; ky < N; ++ky)
+      for (int kx = 0; kx < Nh; ++kx) {
+        double re = 0, im = 0;
+        for (int z = 0; z < N; ++z) {
+          const int t = (kz * z) % N;
+          size_t o = (((size_t)z * N + ky) * Nh + kx) * 2;
+          re += b[o] * cs[t] - b[o + 1] * sn[t];
+          im += b[o] * sn[t] + b[o + 1] * cs[t];
+        }
+        size_t o = (((size_t)kz * N + ky) * Nh + kx) * 2;
+        out[o] = re;
+        out[o + 1] = im;
+      }
+}
+
+// ---------------------------------------------------------------------------
+// operators: LaplaceKernel::precompute / precompute_m2l (kernel.cpp:1638-1849)
+// ---------------------------------------------------------------------------
+static void surface(const Operators& o, double r, const V3& c, std::vector<double>& pts) {
+  pts.resize((size_t)o.ns * 3);
+  for (int i = 0; i < o.ns; ++i)
+    for (int k = 0; k < 3; ++k) pts[3 * i + k] = o.surf_unit[3 * i + k] * r + c[k];
+}
+
+// G[t][s] = 1/|x_t - y_s| (0 when coincident), get_p2p_matrix (kernel.cpp:1535-1556)
+static void p2p_matrix(int nt, const double* xt, int ns, const double* xs, std::vector<double>& G) {
+  G.resize((size_t)nt * ns);
+  for (int t = 0; t < nt; ++t)
+    for (int s = 0; s < ns; ++s) {
+      double d0 = xt[3 * t] - xs[3 * s], d1 = xt[3 * t + 1] - xs[3 * s + 1], d2 = xt[3 * t + 2] - xs[3 * s + 2];
+      double r = std::sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+      G[(size_t)t * ns + s] = r == 0 ? 0.0 : 1.0 / r;
+    }
+}
+
+static void matmul(int n, const double* A, const double* B, double* C) {
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; ++i) {
+    double* c = C + (size_t)i * n;
+    for (int j = 0; j < n; ++j) c[j] = 0.0;
+    for (int k = 0; k < n; ++k) {
+      const double a = A[(size_t)i * n + k];
+      const double* b = B + (size_t)k * n;
+      for (int j = 0; j < n; ++j) c[j] += a * b[j];
+    }
+  }
+}
+
+static int hash_rel(int i, int j, int k) {
+  // LaplaceKernel::hash (3dpp/include/kernel.h:136-141)
+  int signs = ((i < 0 ? 1 : 0) << 2) + ((j < 0 ? 1 : 0) << 1) + (k < 0 ? 1 : 0);
+  return std::abs(i) * 1000 + std::abs(j) * 100 + std::abs(k) * 10 + signs;
+}
+
+void build_operators(Operators& o, int P, double r0, int images) {
+  o.P = P;
+  o.r0 = r0;
+  o.images = images;
+  o.ns = surface_point_num(P);
+  o.N = 2 * P - 1;
+  o.Nh = o.N / 2 + 1;
+  o.Nf = o.N * o.N * o.Nh;
+  const int ns = o.ns, N = o.N, Nf = o.Nf;
+  // surface points (get_surface_points, surface.cpp:3-47, dir 0)
+  o.surf_unit.clear();
+  o.surf_ijk.clear();
+  for (int i = 0; i < P; ++i)
+    for (int j = 0; j < P; ++j)
+      for (int k = 0; k < P; ++k)
+        if (i == 0 || i == P - 1 || j == 0 || j == P - 1 || k == 0 || k == P - 1) {
+          o.surf_ijk.push_back(i);
+          o.surf_ijk.push_back(j);
+          o.surf_ijk.push_back(k);
+          o.surf_unit.push_back(-1.0 + i * 2.0 / (P - 1));
+          o.surf_unit.push_back(-1.0 + j * 2.0 / (P - 1));
+          o.surf_unit.push_back(-1.0 + k * 2.0 / (P - 1));
+        }
+  std::vector<double> xc, xe, e2c;
+  surface(o, r0 * 2.95, V3{0, 0, 0}, xc);
+  surface(o, r0 * 1.05, V3{0, 0, 0}, xe);
+  p2p_matrix(ns, xc.data(), ns, xe.data(), e2c);
+  std::vector<double> U, s, V;
+  jacobi_svd(ns, e2c.data(), U, s, V);
+  // pseudo_inverse: drop singular values <= 4e-16 * s_max (mathfunc.cpp:154-169)
+  double smax = 0;
+  for (double v : s) smax = std::max(smax, std::fabs(v));
+  std::vector<double> sinv(ns);
+  for (int k = 0; k < ns; ++k) sinv[k] = s[k] > smax * 4e-16 ? 1.0 / s[k] : 0.0;
+  o.UT.assign((size_t)ns * ns, 0);
+  o.VSinv.assign((size_t)ns * ns, 0);
+  for (int i = 0; i < ns; ++i)
+    for (int k = 0; k < ns; ++k) {
+      o.UT[(size_t)k * ns + i] = U[(size_t)i * ns + k];
+      o.VSinv[(size_t)i * ns + k] = V[(size_t)i * ns + k] * sinv[k];
+    }
+  o.pinv_up.assign((size_t)ns * ns, 0);
+  matmul(ns, o.VSinv.data(), o.UT.data(), o.pinv_up.data());
+  o.pinv_down.assign((size_t)ns * ns, 0);
+  for (int i = 0; i < ns; ++i)
+    for (int j = 0; j < ns; ++j) o.pinv_down[(size_t)i * ns + j] = o.pinv_up[(size_t)j * ns + i];
+  // M2M[octant] = VSinv (UT G_child) (kernel.cpp:1660-1668)
+  std::vector<double> G, m1((size_t)ns * ns);
+  for (int oc = 0; oc < 8; ++oc) {
+    V3 cc = child_center(V3{0, 0, 0}, r0, oc);
+    std::vector<double> xch;
+    surface(o, r0 / 2 * 1.05, cc, xch);
+    p2p_matrix(ns, xc.data(), ns, xch.data(), G);
+    matmul(ns, o.UT.data(), G.data(), m1.data());
+    o.m2m[oc].assign((size_t)ns * ns, 0);
+    matmul(ns, o.VSinv.data(), m1.data(), o.m2m[oc].data());
+  }
+  // image M2M over the 27 children of a 3x3x3 super-cell (kernel.cpp:1671-1683)
+  o.m2m_img_sum.assign((size_t)ns * ns, 0);
+  o.l2l_img.assign((size_t)ns * ns, 0);
+  if (images > 0) {
+    std::vector<double> mi((size_t)ns * ns);
+    for (int oc = 0; oc < 27; ++oc) {
+      int kk = oc / 9 - 1, jj = (oc % 9) / 3 - 1, ii = oc % 3 - 1;
+      V3 cc{ii * (r0 * 2 / 3.0), jj * (r0 * 2 / 3.0), kk * (r0 * 2 / 3.0)};
+      std::vector<double> xch;
+      surface(o, r0 / 3 * 1.05, cc, xch);
+      p2p_matrix(ns, xc.data(), ns, xch.data(), G);
+      matmul(ns, o.UT.data(), G.data(), m1.data());
+      matmul(ns, o.VSinv.data(), m1.data(), mi.data());
+      for (size_t e = 0; e < mi.size(); ++e) o.m2m_img_sum[e] += mi[e];
+      if (oc == 13)
+        for (int i = 0; i < ns; ++i)
+          for (int j = 0; j < ns; ++j) o.l2l_img[(size_t)i * ns + j] = mi[(size_t)j * ns + i];
+    }
+  }
+  // kernel spectra over every non-adjacent child offset (kernel.cpp:1721-1769)
+  const int rng = images >= 2 ? 4 : 3;
+  std::vector<std::array<int, 3>> offs;
+  for (int k = -rng; k <= rng; ++k)
+    for (int j = -rng; j <= rng; ++j)
+      for (int i = -rng; i <= rng; ++i)
+        if (std::abs(i) >= 2 || std::abs(j) >= 2 || std::abs(k) >= 2) offs.push_back({i, j, k});
+  std::unordered_map<int, int> gidx;
+  for (size_t n = 0; n < offs.size(); ++n) gidx[hash_rel(offs[n][0], offs[n][1], offs[n][2])] = (int)n;
+  std::vector<double> gk(offs.size() * (size_t)Nf * 2);
+  const double delta = 2 * r0 / (P - 1) * 1.05;
+  const double gsize = r0 * 2 * 1.05;
+#pragma omp parallel for schedule(dynamic)
+  for (int n = 0; n < (int)offs.size(); ++n) {
+    std::vector<double> g((size_t)N * N * N);
+    const double rel[3] = {offs[n][0] * r0 * 2, offs[n][1] * r0 * 2, offs[n][2] * r0 * 2};
+    for (int k = 0; k < N; ++k)
+      for (int j = 0; j < N; ++j)
+        for (int i = 0; i < N; ++i) {
+          const double px = (-gsize + i * delta) - rel[0];
+          const double py = (-gsize + j * delta) - rel[1];
+          const double pz = (-gsize + k * delta) - rel[2];
+          const double r = std::sqrt(px * px + py * py + pz * pz);
+          g[((size_t)k * N + j) * N + i] = r == 0 ? 0.0 : 1.0 / r;
+        }
+    dft3_r2c(N, g.data(), &gk[(size_t)n * Nf * 2]);
+  }
+  // 8x8 sibling blocks per parent direction (kernel.cpp:1783-1811), stored
+  // [d][isrc][itar][f]; adjacent child pairs stay zero.
+  o.cc8.assign((size_t)26 * 64 * Nf * 2, 0.0);
+  int d = 0;
+  std::vector<std::array<int, 3>> dirs;
+  for (int k = -1; k <= 1; ++k)
+    for (int j = -1; j <= 1; ++j)
+      for (int i = -1; i <= 1; ++i)
+        if (i || j || k) dirs.push_back({i, j, k});
+  for (d = 0; d < 26; ++d) {
+    for (int isrc = 0; isrc < 8; ++isrc)
+      for (int itar = 0; itar < 8; ++itar) {
+        // child centres of parents of radius 1: parent offset 2*dir, child +-0.5
+        int dx[3];
+        const int sb[3] = {(isrc >> 2) & 1, (isrc >> 1) & 1, isrc & 1};
+        const int tb[3] = {(itar >> 2) & 1, (itar >> 1) & 1, itar & 1};
+        for (int k = 0; k < 3; ++k) dx[k] = 2 * dirs[d][k] + sb[k] - tb[k];
+        auto it = gidx.find(hash_rel(dx[0], dx[1], dx[2]));
+        if (it == gidx.end()) continue;
+        std::memcpy(&o.cc8[(((size_t)d * 8 + isrc) * 8 + itar) * Nf * 2], &gk[(size_t)it->second * Nf * 2],
+                    sizeof(double) * Nf * 2);
+      }
+  }
+  // 1x27 image blocks (kernel.cpp:1813-1849), summed over the 27 copies
+  o.cc27sum.assign((size_t)26 * Nf * 2, 0.0);
+  if (images >= 2) {
+    for (d = 0; d < 26; ++d)
+      for (int pz = -1; pz <= 1; ++pz)
+        for (int py = -1; py <= 1; ++py)
+          for (int px = -1; px <= 1; ++px) {
+            const int sx = 3 * dirs[d][0] + px, sy = 3 * dirs[d][1] + py, sz = 3 * dirs[d][2] + pz;
+            const int g = gidx.at(hash_rel(sx, sy, sz));
+            for (int f = 0; f < 2 * Nf; ++f) o.cc27sum[(size_t)d * Nf * 2 + f] += gk[(size_t)g * Nf * 2 + f];
+          }
+  }
+}
+
+}  // namespace rtfmm_b200

@@ -1,0 +1,94 @@
+// Host-side plan of one FMM evaluation: octree, interaction lists and
+// operator tables, in the layouts the device kernels consume.
+#pragma once
+
+#include <array>
+#include <cstdint>
+#include <map>
+#include <string>
+#include <vector>
+
+namespace rtfmm_b200 {
+
+using V3 = std::array<double, 3>;
+
+// One octree cell; the fields and their meaning follow Cell3
+// (3dpp/include/tree.h:9-47).  octant 13 marks the single central child of an
+// image super-cell (and the root).
+struct Cell {
+  int octant;
+  int depth;
+  double r;
+  V3 x;
+  int coff, cnum;   // children: contiguous range
+  int boff, bnum;   // bodies in tree order: contiguous range
+};
+
+struct P2PEntry {
+  int src;   // source leaf
+  V3 off;    // periodic offset added to the source positions
+};
+
+struct M2LEntry {
+  int src;
+  V3 off;
+  int single;  // is_single_parent (image-level 1x27 interaction)
+};
+
+// Operator tables for one (P, images) pair, built at the root radius r0 and
+// rescaled at use (kernel.cpp:1638-1849).
+struct Operators {
+  int P = 0, images = -1;
+  double r0 = 0;
+  int ns = 0;             // surface points
+  int N = 0, Nh = 0, Nf = 0;  // conv grid edge, half-spectrum edge, frequencies
+  std::vector<double> pinv_up;     // ns x ns: V S^-1 U^T of the upward e2c
+  std::vector<double> pinv_down;   // ns x ns: U S^-1 V^T (its transpose)
+  std::vector<double> UT, VSinv;   // factors as the reference keeps them
+  std::vector<double> m2m[8];      // ns x ns each
+  std::vector<double> m2m_img_sum; // sum of the 27 image M2M matrices
+  std::vector<double> l2l_img;     // M2M_img[13]^T
+  std::vector<double> cc8;         // [d][isrc][itar][f] complex (re,im)
+  std::vector<double> cc27sum;     // [d][f] complex: sum of the 27 image spectra
+  std::vector<double> surf_unit;   // ns x 3 unit-cube surface points
+  std::vector<int> surf_ijk;       // ns x 3 lattice coordinates (x,y,z)
+};
+
+struct Args {
+  int P = 4, ncrit = 16, images = 0;
+  double cycle = 6.283185307179586;
+  V3 x{0, 0, 0};
+  int dipole_correction = 1, divide_4pi = 0, precision = 0;
+  unsigned stages = 3;
+  int device = 0;
+};
+
+struct Plan {
+  Args args;
+  double r0 = 0;
+  int64_t n = 0;
+  std::vector<double> x, q;        // bodies in tree order (x: n*3)
+  std::vector<int64_t> perm;       // perm[i] = input index of tree-order body i
+  std::vector<Cell> cells;         // tree cells, then image cells
+  int ntree = 0;                   // cells before the image super-cells
+  int dmin = 0, dmax = 0;
+  std::map<int, std::vector<P2PEntry>> p2p;
+  std::map<int, std::vector<M2LEntry>> m2l;
+  int64_t n_p2p = 0, n_m2l = 0;
+};
+
+// Tree and lists (exact restatement of the reference's algorithms).
+std::string build_tree(Plan& plan, const double* x, const double* q);
+void traverse(Plan& plan);
+
+// Operator tables.
+void build_operators(Operators& ops, int P, double r0, int images);
+
+// Dense helpers.
+void jacobi_svd(int n, const double* A, std::vector<double>& U, std::vector<double>& s,
+                std::vector<double>& V);
+void dft3_r2c(int N, const double* in, double* out);  // out: N*N*(N/2+1) complex
+
+inline int surface_point_num(int p) { return 6 * (p - 1) * (p - 1) + 2; }
+
+}  // namespace rtfmm_b200

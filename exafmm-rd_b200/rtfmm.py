@@ -1,0 +1,336 @@
+"""Python mirror of the reference's FMM driver interface, over the C ABI.
+
+The reference (mumairsadiq/exafmm-rd, variant 3dpp) is driven as
+
+    Argument args(argc, argv);                    // 3dpp/src/argument.cpp:7-70
+    Bodies3 bs = generate_random_bodies(...);     // 3dpp/src/body.cpp:98-129
+    Bodies3 res = LaplaceFMM(bs, args).solve();   // 3dpp/src/fmm.cpp:13-81
+    compare(res, ref, ...).show();                // 3dpp/src/body.cpp:131-205
+
+This module keeps those names and meanings.  Bodies are passed as numpy
+arrays (positions (n,3), charges (n,)); results come back in input order as
+(potential (n,), gradient (n,3)), the reference's Body3::p and Body3::f.
+
+All arithmetic runs in librtfmm_b200.so (CUDA kernels for sm_100a and the
+host set-up in C++).  There is no CPU fallback: if the library is missing or
+no GPU is visible, the evaluation raises.
+"""
+import ctypes
+import math
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librtfmm_b200.so")
+
+RTFMM_OK, RTFMM_EINVAL, RTFMM_ENOMEM, RTFMM_ECUDA, RTFMM_ESTATE, RTFMM_ENOTSUP = range(6)
+FP64, FP32_MIXED = 0, 1
+STAGE_NEAR, STAGE_FAR, STAGE_ALL = 1, 2, 3
+STAGE_NAMES = ("prep", "P2M", "M2M", "M2L_up", "M2L_hadamard", "M2L_down", "L2L", "L2P", "P2P", "post")
+
+# Every entry point declared in include/rtfmm_b200.h.
+EXPORTS = (
+    "rtfmm_b200_default_args", "rtfmm_b200_create", "rtfmm_b200_destroy", "rtfmm_b200_setup",
+    "rtfmm_b200_evaluate", "rtfmm_b200_solve", "rtfmm_b200_upload", "rtfmm_b200_evaluate_device",
+    "rtfmm_b200_download", "rtfmm_b200_adjoint", "rtfmm_b200_stage_times", "rtfmm_b200_launch_count",
+    "rtfmm_b200_flush_l2", "rtfmm_b200_info", "rtfmm_b200_get_cells", "rtfmm_b200_get_perm",
+    "rtfmm_b200_get_p2p", "rtfmm_b200_get_m2l", "rtfmm_b200_get_cell_vectors", "rtfmm_b200_get_operator",
+    "rtfmm_b200_last_error", "rtfmm_b200_version",
+)
+
+
+class RtfmmError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("rtfmm_b200 error %d: %s" % (code, msg))
+        self.code = code
+
+
+class _Args(ctypes.Structure):
+    _fields_ = [("P", ctypes.c_int), ("ncrit", ctypes.c_int), ("images", ctypes.c_int),
+                ("cycle", ctypes.c_double), ("x", ctypes.c_double * 3),
+                ("dipole_correction", ctypes.c_int), ("divide_4pi", ctypes.c_int),
+                ("precision", ctypes.c_int), ("stages", ctypes.c_uint), ("device", ctypes.c_int)]
+
+
+_LIB = None
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int32)
+_lp = ctypes.POINTER(ctypes.c_int64)
+_fp = ctypes.POINTER(ctypes.c_float)
+_vp = ctypes.c_void_p
+
+
+def lib():
+    """Loads librtfmm_b200.so (raises if it has not been built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise RtfmmError(RTFMM_ENOTSUP, "librtfmm_b200.so not built (run exafmm-rd_b200/build.py)")
+    L = ctypes.CDLL(LIB_PATH)
+    sig = {
+        "rtfmm_b200_default_args": (None, [ctypes.POINTER(_Args)]),
+        "rtfmm_b200_create": (ctypes.c_int, [ctypes.POINTER(_Args), ctypes.POINTER(_vp)]),
+        "rtfmm_b200_destroy": (ctypes.c_int, [_vp]),
+        "rtfmm_b200_setup": (ctypes.c_int, [_vp, ctypes.c_int64, _dp, _dp]),
+        "rtfmm_b200_evaluate": (ctypes.c_int, [_vp, _dp, _dp, _dp]),
+        "rtfmm_b200_solve": (ctypes.c_int, [_vp, ctypes.c_int64, _dp, _dp, _dp, _dp]),
+        "rtfmm_b200_upload": (ctypes.c_int, [_vp]),
+        "rtfmm_b200_evaluate_device": (ctypes.c_int, [_vp, _fp]),
+        "rtfmm_b200_download": (ctypes.c_int, [_vp, _dp, _dp]),
+        "rtfmm_b200_adjoint": (ctypes.c_int, [_vp, _dp, _dp, _dp]),
+        "rtfmm_b200_stage_times": (ctypes.c_int, [_vp, _dp, ctypes.c_int]),
+        "rtfmm_b200_launch_count": (ctypes.c_int, [_vp, _lp]),
+        "rtfmm_b200_flush_l2": (ctypes.c_int, [_vp]),
+        "rtfmm_b200_info": (ctypes.c_int, [_vp, _lp, ctypes.c_int]),
+        "rtfmm_b200_get_cells": (ctypes.c_int, [_vp, _ip, _dp]),
+        "rtfmm_b200_get_perm": (ctypes.c_int, [_vp, _lp]),
+        "rtfmm_b200_get_p2p": (ctypes.c_int, [_vp, _ip, _dp]),
+        "rtfmm_b200_get_m2l": (ctypes.c_int, [_vp, _ip, _dp]),
+        "rtfmm_b200_get_cell_vectors": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
+        "rtfmm_b200_get_operator": (ctypes.c_int, [_vp, ctypes.c_int, _dp, ctypes.c_int64]),
+        "rtfmm_b200_last_error": (ctypes.c_char_p, []),
+        "rtfmm_b200_version": (ctypes.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = L
+    return L
+
+
+def _check(rc):
+    if rc != RTFMM_OK:
+        raise RtfmmError(rc, lib().rtfmm_b200_last_error().decode())
+    return rc
+
+
+def _ptr(a, typ=_dp):
+    return a.ctypes.data_as(typ) if a is not None else None
+
+
+class Argument:
+    """Run parameters with the names of rtfmm::Argument
+    (3dpp/include/argument.h:11-45).  Defaults follow argument.cpp:11-31;
+    ``r`` is cycle/2 and ``x`` is the box centre (argument.cpp:61-62).
+    ``setting_t`` applies the reference's override (argument.cpp:64-69)."""
+
+    def __init__(self, P=4, n=1000, ncrit=16, images=0, cycle=2 * math.pi, seed=5,
+                 dipole_correction=1, zero_netcharge=1, divide_4pi=0, setting_t=0,
+                 x=(0.0, 0.0, 0.0), precision=FP64, stages=STAGE_ALL, device=0, num_compare=-1,
+                 ewald_ksize=11):
+        self.P = P
+        self.n = n
+        self.ncrit = ncrit
+        self.images = images
+        self.cycle = cycle
+        self.seed = seed
+        self.dipole_correction = dipole_correction
+        self.zero_netcharge = zero_netcharge
+        self.divide_4pi = divide_4pi
+        self.setting_t = setting_t
+        self.x = tuple(x)
+        self.precision = precision
+        self.stages = stages
+        self.device = device
+        self.num_compare = n if num_compare == -1 else num_compare
+        self.ewald_ksize = ewald_ksize
+        if setting_t:
+            self.dipole_correction = 0
+            self.zero_netcharge = 0
+            self.divide_4pi = 1
+
+    @property
+    def r(self):
+        return self.cycle / 2
+
+    def _c(self):
+        a = _Args()
+        lib().rtfmm_b200_default_args(ctypes.byref(a))
+        a.P, a.ncrit, a.images, a.cycle = self.P, self.ncrit, self.images, self.cycle
+        for k in range(3):
+            a.x[k] = self.x[k]
+        a.dipole_correction = int(bool(self.dipole_correction))
+        a.divide_4pi = int(bool(self.divide_4pi))
+        a.precision = self.precision
+        a.stages = self.stages
+        a.device = self.device
+        return a
+
+
+class LaplaceFMM:
+    """``rtfmm::LaplaceFMM`` (3dpp/include/fmm.h:12-45): construct with the
+    bodies and the arguments, then ``solve()``.
+
+    ``x`` is (n,3) and ``q`` is (n,), float64.  ``solve()`` returns the
+    potential (n,) and its gradient (n,3) in input order."""
+
+    def __init__(self, x, q, args):
+        self.args = args
+        self.x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 3)
+        self.q = np.ascontiguousarray(q, dtype=np.float64).reshape(-1)
+        if self.x.shape[0] != self.q.shape[0]:
+            raise RtfmmError(RTFMM_EINVAL, "LaplaceFMM init body size error")
+        self.n = self.q.shape[0]
+        h = _vp()
+        ca = args._c()
+        _check(lib().rtfmm_b200_create(ctypes.byref(ca), ctypes.byref(h)))
+        self._h = h
+        self._set_up = False
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().rtfmm_b200_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- phases ---------------------------------------------------------------
+    def setup(self):
+        """Tree, lists and operator tables (host; fmm.cpp:15-49)."""
+        _check(lib().rtfmm_b200_setup(self._h, self.n, _ptr(self.x), _ptr(self.q)))
+        self._set_up = True
+
+    def evaluate(self, q=None):
+        """The evaluation pass with host buffers; returns (phi, grad)."""
+        if not self._set_up:
+            self.setup()
+        phi = np.empty(self.n)
+        grad = np.empty((self.n, 3))
+        qq = None if q is None else np.ascontiguousarray(q, dtype=np.float64)
+        _check(lib().rtfmm_b200_evaluate(self._h, _ptr(qq), _ptr(phi), _ptr(grad)))
+        return phi, grad
+
+    def solve(self):
+        """``LaplaceFMM::solve`` (fmm.cpp:13-81)."""
+        self.setup()
+        return self.evaluate()
+
+    # -- device-resident timing -------------------------------------------------
+    def upload(self):
+        _check(lib().rtfmm_b200_upload(self._h))
+
+    def evaluate_device(self):
+        ms = ctypes.c_float(0)
+        _check(lib().rtfmm_b200_evaluate_device(self._h, ctypes.byref(ms)))
+        return ms.value
+
+    def download(self):
+        phi = np.empty(self.n)
+        grad = np.empty((self.n, 3))
+        _check(lib().rtfmm_b200_download(self._h, _ptr(phi), _ptr(grad)))
+        return phi, grad
+
+    def flush_l2(self):
+        _check(lib().rtfmm_b200_flush_l2(self._h))
+
+    def stage_times(self):
+        v = np.zeros(len(STAGE_NAMES))
+        lib().rtfmm_b200_stage_times(self._h, _ptr(v), len(v))
+        return dict(zip(STAGE_NAMES, v.tolist()))
+
+    def launch_count(self):
+        v = ctypes.c_int64(0)
+        _check(lib().rtfmm_b200_launch_count(self._h, ctypes.byref(v)))
+        return v.value
+
+    def adjoint(self, w):
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        dq = np.empty(self.n)
+        dx = np.empty((self.n, 3))
+        _check(lib().rtfmm_b200_adjoint(self._h, _ptr(w), _ptr(dq), _ptr(dx)))
+        return dq, dx
+
+    # -- introspection ------------------------------------------------------------
+    def info(self):
+        v = np.zeros(8, dtype=np.int64)
+        lib().rtfmm_b200_info(self._h, _ptr(v, _lp), 8)
+        keys = ("ncell", "nleaf", "depth_min", "depth_max", "n_p2p", "n_m2l_parents", "n_m2l", "num_surf")
+        return dict(zip(keys, v.tolist()))
+
+    def cells(self):
+        nc = self.info()["ncell"]
+        ints = np.zeros((nc, 7), dtype=np.int32)
+        reals = np.zeros((nc, 4))
+        _check(lib().rtfmm_b200_get_cells(self._h, _ptr(ints, _ip), _ptr(reals)))
+        return ints, reals
+
+    def perm(self):
+        p = np.zeros(self.n, dtype=np.int64)
+        _check(lib().rtfmm_b200_get_perm(self._h, _ptr(p, _lp)))
+        return p
+
+    def p2p_lists(self):
+        m = self.info()["n_p2p"]
+        ints = np.zeros((m, 2), dtype=np.int32)
+        off = np.zeros((m, 3))
+        _check(lib().rtfmm_b200_get_p2p(self._h, _ptr(ints, _ip), _ptr(off)))
+        return ints, off
+
+    def m2l_lists(self):
+        m = self.info()["n_m2l"]
+        ints = np.zeros((m, 3), dtype=np.int32)
+        off = np.zeros((m, 3))
+        _check(lib().rtfmm_b200_get_m2l(self._h, _ptr(ints, _ip), _ptr(off)))
+        return ints, off
+
+    def cell_vectors(self, which):
+        inf = self.info()
+        out = np.zeros((inf["ncell"], inf["num_surf"]))
+        _check(lib().rtfmm_b200_get_cell_vectors(self._h, which, _ptr(out)))
+        return out
+
+    def operator(self, which, size):
+        out = np.zeros(size)
+        _check(lib().rtfmm_b200_get_operator(self._h, which, _ptr(out), size))
+        return out
+
+
+# ----------------------------------------------------------------------------
+# bodies and the comparison metric
+# ----------------------------------------------------------------------------
+def drand48_stream(seed, count):
+    """glibc srand48/drand48: 48-bit LCG, a = 0x5DEECE66D, c = 0xB, state
+    (seed << 16) | 0x330E; returns ``count`` doubles state / 2^48."""
+    a, c, m = 0x5DEECE66D, 0xB, (1 << 48) - 1
+    x = ((seed & 0xFFFFFFFF) << 16) | 0x330E
+    out = np.empty(count)
+    for i in range(count):
+        x = (a * x + c) & m
+        out[i] = x / float(1 << 48)
+    return out
+
+
+def generate_random_bodies(n, r, offset=(0.0, 0.0, 0.0), seed=5, zero_netcharge=1):
+    """``generate_random_bodies`` (3dpp/src/body.cpp:98-129)."""
+    u = drand48_stream(seed, 4 * n).reshape(n, 4)
+    x = u[:, :3] * r * 2 - r + np.asarray(offset, dtype=np.float64)
+    q = u[:, 3] - 0.5
+    if zero_netcharge and n:
+        q = q - (sum(q.tolist()) / n)
+    return x, q
+
+
+def compare(p1, f1, q1, p2, f2, q2):
+    """``compare`` (3dpp/src/body.cpp:131-175); the second set is the norm."""
+    p1, p2 = np.asarray(p1), np.asarray(p2)
+    f1, f2 = np.asarray(f1).reshape(-1, 3), np.asarray(f2).reshape(-1, 3)
+    pdif = float(np.sum((p1 - p2) ** 2))
+    pnrm = float(np.sum(p2 ** 2))
+    fdif = float(np.sum((f1 - f2) ** 2))
+    fnrm = float(np.sum(f2 ** 2))
+    e1 = float(np.sum(p1 * q1))
+    e2 = float(np.sum(p2 * q2))
+    n = len(p1)
+    return {"l2p": math.sqrt(pdif / pnrm) if pnrm else float("nan"),
+            "l2f": math.sqrt(fdif / fnrm) if fnrm else float("nan"),
+            "l2e": abs(e1 - e2) / abs(e2) if e2 else float("nan"),
+            "rmsp": math.sqrt(pdif / n) if n else 0.0, "rmsf": math.sqrt(fdif / n) if n else 0.0,
+            "energy1": e1, "energy2": e2}

@@ -1,0 +1,191 @@
+/*
+ * rtfmm_b200 -- C ABI of the B200 (sm_100a) periodic kernel-independent
+ * Laplace FMM evaluation pass.
+ *
+ * The reference (mumairsadiq/exafmm-rd, variant 3dpp) has no FFI: its
+ * interface is the C++ driver class and its argument struct.  Each entry
+ * point below replaces one piece of that interface; the comment on each names
+ * the reference interface it replaces (path:line inside the reference
+ * project).  All pointers are plain host pointers unless the name says
+ * "_device"; sizes are element counts.  Nothing here allocates memory the
+ * caller must free, and no call ever exits the process: every function
+ * returns an rtfmm_status and rtfmm_b200_last_error() describes the last
+ * failure of the calling thread.
+ *
+ * Units and conventions follow the reference: the kernel is 1/r (1/(4 pi r)
+ * when divide_4pi is set), `grad` is the gradient of the potential (the
+ * reference's Body3::f, 3dpp/include/body.h:8-15), and outputs are in the
+ * caller's input order (the reference re-sorts by idx, 3dpp/src/fmm.cpp:80).
+ */
+#ifndef RTFMM_B200_H
+#define RTFMM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum rtfmm_status {
+  RTFMM_OK = 0,
+  RTFMM_EINVAL = 1,   /* bad argument (sizes, P, ncrit, NaN/Inf inputs, ...) */
+  RTFMM_ENOMEM = 2,   /* host or device allocation failed                   */
+  RTFMM_ECUDA = 3,    /* a CUDA runtime call or kernel launch failed         */
+  RTFMM_ESTATE = 4,   /* call out of order (e.g. evaluate before setup)      */
+  RTFMM_ENOTSUP = 5   /* option not supported by this build                  */
+} rtfmm_status;
+
+/* Arithmetic of the evaluation pass. */
+typedef enum rtfmm_precision {
+  RTFMM_FP64 = 0,        /* every stage in FP64                                  */
+  RTFMM_FP32_MIXED = 1   /* P2P and the 8x8 FFT-M2L in FP32 with FP64 accumulation;
+                            surface operators, image levels, outputs in FP64      */
+} rtfmm_precision;
+
+/* Stage mask bits for rtfmm_args.stages (all set = the full pass). */
+#define RTFMM_STAGE_NEAR 1u   /* P2P                                  */
+#define RTFMM_STAGE_FAR  2u   /* P2M, M2M, M2L, L2L, L2P              */
+#define RTFMM_STAGE_ALL  3u
+
+/*
+ * Run parameters.  Replaces rtfmm::Argument (3dpp/include/argument.h:11-45,
+ * 3dpp/src/argument.cpp:7-70): same field names and meaning; `r` is derived
+ * as cycle/2 and the box centre is `x` (the reference fixes it at the origin,
+ * argument.cpp:61-62).
+ */
+typedef struct rtfmm_args {
+  int P;                  /* surface points per edge (expansion order), >= 2      */
+  int ncrit;              /* a cell splits while it holds more bodies than this   */
+  int images;             /* periodic image levels (0 = free space)               */
+  double cycle;           /* period / root cell edge                              */
+  double x[3];            /* root cell centre                                     */
+  int dipole_correction;  /* reference's dipole correction (kernel.cpp:1580-1596) */
+  int divide_4pi;         /* scale outputs by 1/(4 pi)                            */
+  int precision;          /* rtfmm_precision                                      */
+  unsigned stages;        /* RTFMM_STAGE_* mask; 0 means RTFMM_STAGE_ALL          */
+  int device;             /* CUDA device ordinal                                  */
+} rtfmm_args;
+
+typedef struct rtfmm_fmm rtfmm_fmm;
+
+/* Fills `a` with the reference's defaults (argument.cpp:11-31): P=4,
+ * ncrit=16, images=0, cycle=2*pi, dipole_correction=1, divide_4pi=0, plus
+ * precision=FP64, stages=ALL, device=0. */
+void rtfmm_b200_default_args(rtfmm_args* a);
+
+/* Creates a solver.  Replaces LaplaceFMM::LaplaceFMM(const Bodies3&,
+ * const Argument&) (3dpp/include/fmm.h:12-16, 3dpp/src/fmm.cpp:7-11) minus the
+ * body copy, which moves to rtfmm_b200_setup.  Touches no GPU. */
+int rtfmm_b200_create(const rtfmm_args* args, rtfmm_fmm** out);
+
+/* Releases the solver and every buffer it owns (host and device). */
+int rtfmm_b200_destroy(rtfmm_fmm* fmm);
+
+/*
+ * Host-side set-up for one body set: builds the adaptive octree
+ * (Tree::build_nonuniform_octree, 3dpp/src/tree.cpp:102-188), the P2P and
+ * M2L lists with the periodic image cells (Traverser::traverse,
+ * 3dpp/src/traverser.cpp:19-68) and the operator tables
+ * (LaplaceKernel::precompute / precompute_m2l, 3dpp/src/kernel.cpp:1638-1849;
+ * cached inside the handle across calls with the same P and images).
+ * This is LaplaceFMM::solve up to its hot block (fmm.cpp:15-49).  x is n*3
+ * (x0,y0,z0,x1,...), q is n.  Touches no GPU.
+ */
+int rtfmm_b200_setup(rtfmm_fmm* fmm, int64_t n, const double* x, const double* q);
+
+/*
+ * The evaluation pass with host buffers: copies q (and the positions the
+ * tree was built on) to the device, runs P2M, M2M, M2L, L2L, L2P and P2P
+ * (the hot block, 3dpp/src/fmm.cpp:51-60), then the dipole correction, the
+ * 1/(4 pi) scaling and the re-sort (fmm.cpp:75-80) on the device, and copies
+ * phi (n) and grad (n*3) back.  q may be NULL to reuse the charges given to
+ * setup.
+ */
+int rtfmm_b200_evaluate(rtfmm_fmm* fmm, const double* q, double* phi, double* grad);
+
+/* setup + evaluate: replaces LaplaceFMM::solve() (3dpp/src/fmm.cpp:13-81). */
+int rtfmm_b200_solve(rtfmm_fmm* fmm, int64_t n, const double* x, const double* q,
+                     double* phi, double* grad);
+
+/*
+ * The evaluation pass on device-resident data: the bodies uploaded by the
+ * last evaluate/upload call, results left in device memory.  Returns the
+ * pass time in milliseconds measured with CUDA events on the solver's own
+ * stream (`ms` may be NULL).  For throughput measurement.
+ */
+int rtfmm_b200_upload(rtfmm_fmm* fmm);
+int rtfmm_b200_evaluate_device(rtfmm_fmm* fmm, float* ms);
+
+/* Copies the outputs of the last device pass to the host (input order). */
+int rtfmm_b200_download(rtfmm_fmm* fmm, double* phi, double* grad);
+
+/*
+ * Adjoint of the evaluation pass (no reference counterpart: the reference
+ * has no gradient code).  For L = sum_i w_i phi_i it returns dL/dq (n) and
+ * dL/dx (n*3) by applying the transposed operator chain P2P^T, L2P^T, L2L^T,
+ * M2L^T (conjugated kernel spectra), M2M^T, P2M^T; upward coefficients are
+ * recomputed.  Requires a previous evaluate on the same bodies.  The
+ * divide_4pi scaling applies; the dipole correction is excluded.
+ */
+int rtfmm_b200_adjoint(rtfmm_fmm* fmm, const double* w, double* dLdq, double* dLdx);
+
+/* Per-stage device times of the last pass, in ms, in this order:
+ * prep, P2M, M2M, M2L_up, M2L_hadamard, M2L_down, L2L, L2P, P2P, post.
+ * Writes min(cap, 10) values; returns the number of stages. */
+int rtfmm_b200_stage_times(rtfmm_fmm* fmm, double* ms, int cap);
+
+/* Counters of the last pass: kernels launched by this library. */
+int rtfmm_b200_launch_count(rtfmm_fmm* fmm, int64_t* launches);
+
+/* Writes L2-sized garbage on the solver's stream (cache flush between timed
+ * passes). */
+int rtfmm_b200_flush_l2(rtfmm_fmm* fmm);
+
+/* ---- introspection (host data after setup; used by parity tests) ---- */
+
+/* Tree and list sizes.  info[0..7] = ncell (incl. image cells), nleaf,
+ * depth_min, depth_max, n_p2p_entries, n_m2l_parents, n_m2l_entries,
+ * num_surf. */
+int rtfmm_b200_info(rtfmm_fmm* fmm, int64_t* info, int cap);
+
+/* Cells in the reference's order (Cell3, 3dpp/include/tree.h:9-47):
+ * ints[7*c..] = octant, depth, crange.offset, crange.number, brange.offset,
+ * brange.number, 0; reals[4*c..] = r, x, y, z.  Either pointer may be NULL. */
+int rtfmm_b200_get_cells(rtfmm_fmm* fmm, int32_t* ints, double* reals);
+
+/* perm[i] = input index of the i-th body in tree order. */
+int rtfmm_b200_get_perm(rtfmm_fmm* fmm, int64_t* perm);
+
+/* P2P lists (Traverser::P2P_map, traverser.cpp:70-148): entry e is
+ * (target leaf, source leaf) = ints[2e], ints[2e+1] with source offset
+ * off[3e..3e+2]. */
+int rtfmm_b200_get_p2p(rtfmm_fmm* fmm, int32_t* ints, double* off);
+
+/* M2L parent map (Traverser::M2L_parent_map, traverser.cpp:234-282 and
+ * 43-64): entry e is (target, source, is_single_parent) = ints[3e..3e+2]
+ * with offset off[3e..3e+2]. */
+int rtfmm_b200_get_m2l(rtfmm_fmm* fmm, int32_t* ints, double* off);
+
+/* Per-cell surface vectors after the last pass (device -> host):
+ * which = 0 for q_equiv, 1 for p_check; out is ncell*num_surf. */
+int rtfmm_b200_get_cell_vectors(rtfmm_fmm* fmm, int which, double* out);
+
+/* Operator tables (host FP64), for comparison with the reference's
+ * LaplaceKernel members (3dpp/include/kernel.h:197-229):
+ * which = 0: pinv of the upward equivalent->check operator (ns*ns),
+ *         1: M2M for octants 0..7 (8*ns*ns),  2: sum of the 27 image M2M
+ *            (ns*ns),  3: 8x8 kernel spectra (26*8*8*Nfreq complex, as
+ *            interleaved re,im). */
+int rtfmm_b200_get_operator(rtfmm_fmm* fmm, int which, double* out, int64_t cap);
+
+/* Last error message of the calling thread ("" if none). */
+const char* rtfmm_b200_last_error(void);
+
+/* Library version string. */
+const char* rtfmm_b200_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RTFMM_B200_H */

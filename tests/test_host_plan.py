@@ -1,0 +1,187 @@
+"""CPU tests of the C-ABI library's host side: exported symbols, octree,
+interaction lists, operator tables and error behaviour.  No GPU needed: the
+set-up phase (rtfmm_b200_setup) touches no device."""
+import math
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "rtfmm_b200.h")
+
+
+def header_symbols():
+    src = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(rtfmm_b200_\w+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol(pkg):
+    L = pkg.lib()
+    syms = header_symbols()
+    assert len(syms) >= 20
+    for s in syms:
+        assert hasattr(L, s), s
+    assert set(syms) == set(pkg.rtfmm.EXPORTS)
+    assert b"sm_100a" in L.rtfmm_b200_version()
+
+
+def uniform(n, seed):
+    rng = np.random.default_rng(seed)
+    x = rng.random((n, 3)) - 0.5
+    q = rng.random(n) * 2 - 1
+    return x, q - q.mean()
+
+
+def blobs(n, nblob, sigma, seed):
+    rng = np.random.default_rng(seed)
+    c = rng.random((nblob, 3))
+    x = c[rng.integers(0, nblob, n)] + sigma * rng.standard_normal((n, 3))
+    x = np.mod(x, 1.0) - 0.5
+    q = np.where(rng.random(n) < 0.5, -1.0, 1.0)
+    return x, q - q.mean()
+
+
+def lists_of(f):
+    pi, po = f.p2p_lists()
+    p2p = sorted((int(a), int(b), tuple(np.round(o, 12))) for (a, b), o in zip(pi, po))
+    mi, mo = f.m2l_lists()
+    m2l = sorted((int(a), int(b), int(c), tuple(np.round(o, 12))) for (a, b, c), o in zip(mi, mo))
+    return p2p, m2l
+
+
+def oracle_lists(F):
+    p2p = sorted((t, s, tuple(np.round(off, 12))) for t, l in F.trav.p2p.items() for (s, off) in l)
+    m2l = sorted((t, s, sg, tuple(np.round(off, 12))) for t, l in F.trav.m2l_parent.items()
+                 for (s, off, sg) in l)
+    return p2p, m2l
+
+
+CASES = [
+    ("uniform", 3000, 32, 0), ("uniform", 3000, 32, 1), ("uniform", 2500, 16, 3),
+    ("blobs", 4000, 16, 2), ("single_leaf", 50, 64, 2), ("tiny", 9, 1, 1),
+]
+
+
+@pytest.mark.parametrize("kind,n,ncrit,images", CASES)
+def test_tree_and_lists_match_oracle(pkg, oracle, kind, n, ncrit, images):
+    if kind == "blobs":
+        x, q = blobs(n, 4, 0.03, 7)
+    else:
+        x, q = uniform(n, n)
+    f = pkg.LaplaceFMM(x, q, pkg.Argument(P=4, ncrit=ncrit, images=images, cycle=1.0))
+    f.setup()
+    F = oracle.FMM(x, q, 4, ncrit, images, 1.0)
+    ints, reals = f.cells()
+    C = F.cells
+    assert len(C) == ints.shape[0]
+    for c in range(len(C)):
+        assert tuple(ints[c, :6]) == (C.octant[c], C.depth[c], C.coff[c], C.cnum[c], C.boff[c], C.bnum[c])
+        assert reals[c, 0] == C.r[c]
+        assert tuple(reals[c, 1:]) == tuple(C.x[c])
+    assert np.array_equal(f.perm(), F.perm)
+    assert lists_of(f) == oracle_lists(F)
+
+
+def test_m2l_parent_map_is_symmetric(pkg):
+    """Every 8x8 parent pair appears in both directions with opposite offsets
+    (the transposed chain of the adjoint relies on it)."""
+    x, q = uniform(4000, 11)
+    f = pkg.LaplaceFMM(x, q, pkg.Argument(P=4, ncrit=24, images=2, cycle=1.0))
+    f.setup()
+    mi, mo = f.m2l_lists()
+    s = {(int(a), int(b), tuple(np.round(o, 12))) for (a, b, c), o in zip(mi, mo) if c == 0}
+    for (a, b, o) in s:
+        assert (b, a, tuple(-v + 0.0 for v in o)) in s
+
+
+def test_p2p_lists_symmetric(pkg):
+    x, q = blobs(3000, 3, 0.05, 5)
+    f = pkg.LaplaceFMM(x, q, pkg.Argument(P=4, ncrit=20, images=1, cycle=1.0))
+    f.setup()
+    pi, po = f.p2p_lists()
+    s = {(int(a), int(b), tuple(np.round(o, 12))) for (a, b), o in zip(pi, po)}
+    for (a, b, o) in s:
+        assert (b, a, tuple(-v + 0.0 for v in o)) in s
+
+
+@pytest.mark.parametrize("P", [4, 6])
+def test_kernel_spectra_match_oracle(pkg, oracle, P):
+    """8x8 sibling spectra (precompute_m2l, kernel.cpp:1783-1811): the
+    library's host DFT against numpy's rfftn in the oracle."""
+    x, q = uniform(200, 1)
+    f = pkg.LaplaceFMM(x, q, pkg.Argument(P=P, ncrit=64, images=2, cycle=1.0))
+    f.setup()
+    N = 2 * P - 1
+    Nf = N * N * P
+    got = f.operator(3, 26 * 64 * Nf * 2).reshape(26, 8, 8, Nf, 2)
+    got = got[..., 0] + 1j * got[..., 1]
+    ops = oracle.Operators(P, 0.5, 2)
+    ref = ops.cc8.reshape(26, 8, 8, Nf)
+    scale = np.abs(ref).max()
+    assert np.abs(got - ref).max() / scale < 1e-13
+
+
+@pytest.mark.parametrize("P", [4, 6, 8])
+def test_m2m_reproduces_child_potential(pkg, oracle, P):
+    """The parent equivalent density from M2M reproduces the child's field on
+    the parent check surface (the defining property of the operator,
+    kernel.cpp:1660-1668), and the library's pseudo-inverse agrees with the
+    oracle's in that sense."""
+    x, q = uniform(200, 2)
+    f = pkg.LaplaceFMM(x, q, pkg.Argument(P=P, ncrit=64, images=1, cycle=1.0))
+    f.setup()
+    ns = oracle.surface_point_num(P)
+    m2m = f.operator(1, 8 * ns * ns).reshape(8, ns, ns)
+    r0 = 0.5
+    xc = oracle.surface_points(P, r0 * 2.95)
+    xe = oracle.surface_points(P, r0 * 1.05)
+    A = oracle.p2p_matrix(xe, xc)
+    rng = np.random.default_rng(P)
+    for o in range(8):
+        xch = oracle.surface_points(P, r0 / 2 * 1.05, oracle.child_center(np.zeros(3), r0, o))
+        G = oracle.p2p_matrix(xch, xc)
+        qc = rng.standard_normal(ns)
+        target = G @ qc
+        err = np.linalg.norm(A @ (m2m[o] @ qc) - target) / np.linalg.norm(target)
+        assert err < {4: 1e-12, 6: 1e-10, 8: 1e-8}[P]
+
+
+def test_errors(pkg):
+    x, q = uniform(100, 3)
+    with pytest.raises(pkg.RtfmmError) as e:
+        pkg.LaplaceFMM(x, q, pkg.Argument(P=1))
+    assert e.value.code == 1
+    with pytest.raises(pkg.RtfmmError):
+        pkg.LaplaceFMM(x, q[:-1], pkg.Argument(P=4))
+    bad = x.copy()
+    bad[3, 1] = np.nan
+    f = pkg.LaplaceFMM(bad, q, pkg.Argument(P=4))
+    with pytest.raises(pkg.RtfmmError) as e:
+        f.setup()
+    assert e.value.code == 1
+    # more than ncrit coincident bodies: the reference would split forever
+    same = np.zeros((40, 3))
+    f = pkg.LaplaceFMM(same, np.ones(40), pkg.Argument(P=4, ncrit=8))
+    with pytest.raises(pkg.RtfmmError) as e:
+        f.setup()
+    assert "deeper" in str(e.value)
+    # out of order
+    f = pkg.LaplaceFMM(x, q, pkg.Argument(P=4))
+    with pytest.raises(pkg.RtfmmError) as e:
+        f.download()
+    assert e.value.code == 4
+
+
+def test_empty_input_setup(pkg):
+    f = pkg.LaplaceFMM(np.zeros((0, 3)), np.zeros(0), pkg.Argument(P=4, images=2, cycle=1.0))
+    f.setup()
+    assert f.info()["nleaf"] == 1
+
+
+def test_generate_random_bodies_matches_oracle(pkg, oracle):
+    x1, q1 = pkg.generate_random_bodies(500, math.pi, seed=5, zero_netcharge=1)
+    x2, q2 = oracle.generate_random_bodies(500, math.pi, seed=5, zero_netcharge=1)
+    assert np.array_equal(x1, x2) and np.array_equal(q1, q2)
