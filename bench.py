@@ -1,0 +1,373 @@
+"""Throughput of the periodic KIFMM evaluation pass on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the configuration the headline metric is quoted on): N = 2^20
+bodies i.i.d. uniform in [0,1)^3, charges uniform in [-1,1] shifted to zero
+net charge (seed 2), P = 8, ncrit = 256, 3 periodic image levels, cycle 1,
+kernel 1/(4 pi r), no dipole correction.  A step is one evaluation pass
+(the reference's FMM_kernels block: P2M, M2M, M2L, L2L, L2P, P2P, then the
+1/(4 pi) scaling and the re-sort), with the octree, lists and operator
+tables built beforehand, as the reference times it.
+
+ours:       value = N / pass time, FP32-mixed form, bodies resident in HBM,
+            256 MB L2 flush between steps; the FP64 form of the same pass is
+            timed beside it and its error against the FP64 form is reported.
+            e2e   = the same metric through the C ABI with pinned host
+            buffers (charges in, potential and gradient out) per step.
+reference:  the reference's own CPU FMM (compiled from its sources into
+            oracle/_ref, else the numpy oracle) on a bounded sample of the
+            same workload, all host threads.
+
+Multi-GPU (torchrun): the pass does not shard in this build, so each rank
+runs an independent replica on its own GPU; value = all ranks' bodies /
+max-over-ranks time.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+METRIC = "particles/s potential+force, N=1M P=8 PBC: FP32-mixed vs FP64 GPU at equal err"
+WORKLOAD = dict(N=1 << 20, P=8, ncrit=256, images=3, cycle=1.0, seed=2)
+
+
+def load_pkg():
+    import importlib.util
+    d = os.path.join(ROOT, "exafmm-rd_b200")
+    spec = importlib.util.spec_from_file_location("exafmm_rd_b200", os.path.join(d, "__init__.py"),
+                                                  submodule_search_locations=[d])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["exafmm_rd_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def make_bodies(n, seed):
+    rng = np.random.default_rng(seed)
+    x = rng.random((n, 3))
+    q = rng.random(n) * 2 - 1
+    return x, q - q.mean()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([v.strip() for v in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for k, nm in enumerate(names):
+                if len(s) > 4 + k and s[4 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def read_traffic(kernel):
+    """dram bytes per launch from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "%s_traffic.txt" % kernel)
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("traffic_bytes_per_launch:"):
+            return float(line.split(":", 1)[1])
+    return None
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------------------
+# reference arm / CPU baseline
+# ----------------------------------------------------------------------------
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "rtfmm_ref_pass")
+
+
+def reference_sample(n, threads, seed=2):
+    """One bounded sample of the workload on the reference's own CPU FMM:
+    returns (particles/s from its FMM_kernels timer, kind, note)."""
+    W = WORKLOAD
+    x, q = make_bodies(n, seed)
+    if os.path.exists(REF_BIN):
+        with tempfile.TemporaryDirectory() as td:
+            fin = os.path.join(td, "in.bin")
+            np.concatenate([x - 0.5, q[:, None]], axis=1).astype(np.float64).tofile(fin)
+            env = dict(os.environ, OPENBLAS_NUM_THREADS="1", OMP_NUM_THREADS=str(threads))
+            cmd = [REF_BIN, "--in", fin, "-n", str(n), "-P", str(W["P"]), "-m", str(W["ncrit"]),
+                   "-i", str(W["images"]), "-c", str(W["cycle"]), "--th_num", str(threads),
+                   "--dipole_correction", "0", "--divide_4pi", "1"]
+            out = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=1800).stdout
+        t = None
+        for line in out.splitlines():
+            if line.startswith("[FMM_kernels time measured"):
+                t = float(line.split(":")[1].split()[0])
+        if t is None:
+            raise RuntimeError("reference run printed no FMM_kernels timer")
+        return n / t, "reference", "FMM_kernels timer of the reference's LaplaceFMM::solve"
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import rtfmm_oracle as orc
+    F = orc.FMM(x, q, W["P"], W["ncrit"], W["images"], W["cycle"], center=(0.5, 0.5, 0.5), divide_4pi=1)
+    t0 = time.perf_counter()
+    F.solve()
+    return n / (time.perf_counter() - t0), "port", "numpy oracle pass (single process)"
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    n = args.ref_n
+    for _ in range(args.warmup):
+        reference_sample(n, threads)
+    vals = []
+    kind = note = None
+    for _ in range(args.steps):
+        v, kind, note = reference_sample(n, threads)
+        vals.append(v)
+    value = float(np.mean(vals))
+    W = WORKLOAD
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * n / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: uniform [0,1)^3, q~U[-1,1] net zero, seed 2",
+            "config": {"workload": "periodic KIFMM pass, P=8 ncrit=256 images=3 (bounded sample N=%d)" % n,
+                       "N": n, "P": W["P"], "ncrit": W["ncrit"], "images": W["images"]},
+            "cpu_baseline": {"value": value, "unit": "particles/s", "cores": threads, "kind": kind,
+                             "sample": "N=%d bodies of the workload per step; %s" % (n, note)},
+            "e2e": {"value": value, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------
+# our arm
+# ----------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    pkg = load_pkg()
+    W = WORKLOAD
+    n = args.n
+    x, q = make_bodies(n, W["seed"])
+    mk = lambda prec, stages=pkg.STAGE_ALL: pkg.Argument(
+        P=W["P"], ncrit=W["ncrit"], images=W["images"], cycle=W["cycle"], x=(0.5, 0.5, 0.5),
+        dipole_correction=0, divide_4pi=1, precision=prec, stages=stages, device=local)
+    t0 = time.perf_counter()
+    fm = pkg.LaplaceFMM(x, q, mk(pkg.FP32_MIXED))
+    fm.setup()
+    setup_s = time.perf_counter() - t0
+    fm.upload()
+    f64 = pkg.LaplaceFMM(x, q, mk(pkg.FP64))
+    f64.setup()
+    f64.upload()
+    info = fm.info()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(f, steps, warmup):
+        for _ in range(warmup):
+            f.evaluate_device()
+        barrier()
+        ms = []
+        for _ in range(steps):
+            f.flush_l2()
+            ms.append(f.evaluate_device())
+        barrier()
+        return ms
+
+    with ClockSampler(local) as clk:
+        ms_mixed = timed(fm, args.steps, args.warmup)
+    launches = fm.launch_count() * args.steps
+    st_mixed = fm.stage_times()
+    ms64 = timed(f64, args.steps, max(1, args.warmup // 2))
+    phi_m, grad_m = fm.download()
+    phi_d, grad_d = f64.download()
+    err = pkg.compare(phi_m, grad_m, q, phi_d, grad_d, q)
+    dphi = phi_m - phi_d
+    err_mr = float(np.linalg.norm(dphi - dphi.mean()) / np.linalg.norm(phi_d - phi_d.mean()))
+
+    # per-stage times with the stages serialised (diagnostic only)
+    fs = pkg.LaplaceFMM(x, q, mk(pkg.FP32_MIXED, pkg.STAGE_ALL | pkg.STAGE_SERIAL))
+    fs.setup()
+    fs.upload()
+    for _ in range(2):
+        fs.evaluate_device()
+    ser = []
+    for _ in range(max(3, args.steps // 2)):
+        fs.flush_l2()
+        fs.evaluate_device()
+        ser.append(fs.stage_times())
+    stage_serial = {k: float(np.mean([s[k] for s in ser])) for k in ser[0]}
+    fs.close()
+
+    # end to end through the C ABI: pinned host charges in, pinned outputs back
+    qh = torch.from_numpy(q.copy()).pin_memory()
+    ph = torch.empty(n, dtype=torch.float64).pin_memory()
+    gh = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+    qn, pn, gn = qh.numpy(), ph.numpy(), gh.numpy()
+    lib = pkg.lib()
+    import ctypes
+    dp = ctypes.POINTER(ctypes.c_double)
+    call = lambda: lib.rtfmm_b200_evaluate(fm._h, qn.ctypes.data_as(dp), pn.ctypes.data_as(dp),
+                                           gn.ctypes.data_as(dp))
+    for _ in range(args.warmup):
+        assert call() == 0
+    barrier()
+    e2e = []
+    for _ in range(args.steps):
+        fm.flush_l2()
+        t0 = time.perf_counter()
+        assert call() == 0
+        e2e.append(time.perf_counter() - t0)
+    barrier()
+
+    t_m = float(np.mean(ms_mixed))
+    t_d = float(np.mean(ms64))
+    t_e = float(np.mean(e2e))
+    if world > 1:
+        v = torch.tensor([t_m, t_d, t_e], dtype=torch.float64, device="cuda")
+        dist.all_reduce(v, op=dist.ReduceOp.MAX)
+        t_m, t_d, t_e = v.tolist()
+    if rank != 0:
+        dist.destroy_process_group()
+        return
+    clocks = clk.summary()
+    # roofline of the dominant kernel, from the serialised stage times
+    hbm, hbm_kind = measured_peaks()
+    sm_mhz = clocks.get("sm_mhz") or 1965.0
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    P = W["P"]
+    N = 2 * P - 1
+    Nf = N * N * P
+    had_bytes = Nf * 8 * 8 * (info["m2l8_sources"] + info["m2l8_targets"]) + 26 * 64 * Nf * 8
+    kern = {
+        "p2p32": {"bound": "fp32", "work": 20.0 * info["p2p_pairs"], "ms": stage_serial["P2P"],
+                  "peak": fp32_peak, "unit": "TFLOP/s",
+                  "peak_kind": "nominal 148 SM x 128 FMA/clk x 2 at the sampled SM clock"},
+        "m2l_hadamard8": {"bound": "hbm", "work": float(had_bytes), "ms": stage_serial["M2L_hadamard"],
+                          "peak": hbm, "unit": "GB/s", "peak_kind": hbm_kind},
+    }
+    for k, d in kern.items():
+        scale = 1e12 if d["unit"] == "TFLOP/s" else 1e9
+        d["achieved"] = d["work"] / (d["ms"] * 1e-3) / scale if d["ms"] > 0 else None
+        d["frac"] = d["achieved"] / d["peak"] if d["achieved"] else None
+    top = max(kern, key=lambda k: kern[k]["ms"])
+    K = kern[top]
+    roofline = {"kernel": top, "bound": K["bound"], "achieved": K["achieved"], "peak": K["peak"],
+                "unit": K["unit"], "frac": K["frac"], "peak_kind": K["peak_kind"],
+                "traffic": read_traffic(top),
+                "work_per_launch": K["work"], "launch_ms": K["ms"],
+                "others": {k: {"achieved": d["achieved"], "peak": d["peak"], "unit": d["unit"],
+                               "frac": d["frac"], "launch_ms": d["ms"]} for k, d in kern.items() if k != top}}
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            ncores = os.cpu_count() or 1
+            v, kind, note = reference_sample(args.ref_n, ncores)
+            cpu = {"value": v, "unit": "particles/s", "cores": ncores, "kind": kind,
+                   "sample": "N=%d bodies of the workload (P=8 ncrit=256 images=3); %s" % (args.ref_n, note)}
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "particles/s", "cores": 0, "kind": "none", "sample": "failed: %s" % e}
+    line = {
+        "metric": METRIC, "value": world * n / (t_m * 1e-3), "unit": "particles/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_m, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32-mixed",
+        "data": "synthetic: uniform [0,1)^3, q~U[-1,1] net zero, seed 2",
+        "config": {"workload": "periodic KIFMM evaluation pass N=%d P=8 ncrit=256 images=3" % n,
+                   "N": n, "P": P, "ncrit": W["ncrit"], "images": W["images"], "cycle": W["cycle"],
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "256 MB flush between timed steps",
+                   "setup_s": setup_s, "nleaf": info["nleaf"], "ncell": info["ncell"],
+                   "p2p_pairs": info["p2p_pairs"],
+                   "fp64_ms_per_step": t_d, "fp64_value": world * n / (t_d * 1e-3),
+                   "mixed_speedup_vs_fp64": t_d / t_m,
+                   "mixed_err_vs_fp64": {"l2p": err["l2p"], "l2f": err["l2f"], "l2p_mean_removed": err_mr},
+                   "stage_ms_overlapped": st_mixed, "stage_ms_serial": stage_serial},
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": {"value": world * n / t_e, "unit": "particles/s", "h2d_bytes_per_step": 8 * n + 24 * n,
+                "d2h_bytes_per_step": 8 * n + 24 * n, "ms_per_step": 1000 * t_e},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=WORKLOAD["N"])
+    ap.add_argument("--ref-n", type=int, default=1 << 17)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -8,6 +8,7 @@
 // This is LaplaceFMM::solve (3dpp/src/fmm.cpp:13-81) split at its hot block.
 #include <cmath>
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <new>
 #include <string>
@@ -64,6 +65,7 @@ struct rtfmm_fmm {
   bool device_ready = false;
   bool pass_done = false;
   std::vector<double> x_in;  // input-order positions of the set-up bodies
+  double* h_xin = nullptr;   // pinned copy of x_in (host -> device source)
   std::vector<double> q_in;
 
   // host plan tables
@@ -142,6 +144,10 @@ int dupload(rtfmm_fmm* f, T** p, const std::vector<T>& h) {
 
 void free_device(rtfmm_fmm* f) {
   if (f->dev >= 0) cudaSetDevice(f->dev);
+  if (f->h_xin) {
+    cudaFreeHost(f->h_xin);
+    f->h_xin = nullptr;
+  }
   for (void* p : f->allocs) cudaFree(p);
   f->allocs.clear();
   if (f->s0) cudaStreamDestroy(f->s0);
@@ -523,6 +529,10 @@ int upload_plan(rtfmm_fmm* f) {
   RC(dupload(f, &f->d_tscale27, f->tscale27));
   RC(dalloc(f, &f->d_dip, 3 * 256 + 3));
 #undef RC
+  if (f->h_xin) cudaFreeHost(f->h_xin);
+  f->h_xin = nullptr;
+  CK(cudaMallocHost(&f->h_xin, sizeof(double) * std::max<int64_t>(1, 3 * n)));
+  if (n > 0) std::memcpy(f->h_xin, f->x_in.data(), sizeof(double) * 3 * n);
   f->device_ready = true;
   return RTFMM_OK;
 }
@@ -553,25 +563,34 @@ int enqueue_pass(rtfmm_fmm* f) {
   const int n = (int)p.n, ns = o.ns, Nf = o.Nf, P = o.P;
   const int nleaf = (int)f->leaves.size();
   const bool mixed = f->args.precision == RTFMM_FP32_MIXED;
-  const unsigned stages = f->args.stages ? f->args.stages : RTFMM_STAGE_ALL;
+  const unsigned stages = f->args.stages;
   const bool near = stages & RTFMM_STAGE_NEAR, far = stages & RTFMM_STAGE_FAR;
-  cudaStream_t s0 = f->s0, s1 = f->s1;
+  const bool serial = stages & RTFMM_STAGE_SERIAL;
+  cudaStream_t s0 = f->s0, s1 = serial ? f->s0 : f->s1;
   f->launches = 0;
   CK(cudaEventRecord(f->ev_start, s0));
-  if (near) {
-    CK(cudaStreamWaitEvent(s1, f->ev_start, 0));
-    CK(cudaEventRecord(f->ev_near0, s1));
+  auto near_field = [&]() -> int {
+    if (!serial) CK(cudaStreamWaitEvent(s1, f->ev_start, 0));
     if (mixed) {
       CK(launch_prep32(f->d_body64, f->d_body_leaf, f->d_leaves, f->d_body32, n, s1));
+      f->launches++;
+    }
+    CK(cudaEventRecord(f->ev_near0, s1));
+    if (mixed) {
       CK(launch_p2p32(f->d_body32, f->d_leaves, f->d_items, (int)f->items.size(), f->d_list_off, f->d_list32,
                       f->d_near_phi, f->d_near_grad, s1));
-      f->launches += 2;
+      f->launches += 1;
     } else {
       CK(launch_p2p64(f->d_body64, f->d_leaves, f->d_items, (int)f->items.size(), f->d_list_off, f->d_list64,
                       f->d_near_phi, f->d_near_grad, s1));
       f->launches += 1;
     }
     CK(cudaEventRecord(f->ev_near, s1));
+    return RTFMM_OK;
+  };
+  if (near && !serial) {
+    int rc = near_field();
+    if (rc) return rc;
   }
   CK(cudaEventRecord(f->ev_st[ST_PREP], s0));
   if (far) {
@@ -636,7 +655,11 @@ int enqueue_pass(rtfmm_fmm* f) {
   } else {
     for (int k = ST_P2M; k <= ST_L2P; ++k) CK(cudaEventRecord(f->ev_st[k], s0));
   }
-  if (near) CK(cudaStreamWaitEvent(s0, f->ev_near, 0));
+  if (near && serial) {
+    int rc = near_field();
+    if (rc) return rc;
+  }
+  if (near && !serial) CK(cudaStreamWaitEvent(s0, f->ev_near, 0));
   CK(cudaEventRecord(f->ev_st[ST_P2P], s0));
   const Args& a = f->args;
   if (a.dipole_correction) {
@@ -662,8 +685,7 @@ int collect_times(rtfmm_fmm* f, float* total) {
   for (int k = 0; k < ST_N; ++k) {
     float t = 0;
     if (k == ST_P2P) {
-      const unsigned stages = f->args.stages ? f->args.stages : RTFMM_STAGE_ALL;
-      if (stages & RTFMM_STAGE_NEAR) CK(cudaEventElapsedTime(&t, f->ev_near0, f->ev_near));
+      if (f->args.stages & RTFMM_STAGE_NEAR) CK(cudaEventElapsedTime(&t, f->ev_near0, f->ev_near));
       f->stage_ms[k] = t;
       prev = f->ev_st[k];
       continue;
@@ -705,7 +727,7 @@ int rtfmm_b200_create(const rtfmm_args* a, rtfmm_fmm** out) {
   if (!(a->cycle > 0) || !std::isfinite(a->cycle)) return fail(RTFMM_EINVAL, "cycle must be positive and finite");
   if (a->precision != RTFMM_FP64 && a->precision != RTFMM_FP32_MIXED)
     return fail(RTFMM_EINVAL, "unknown precision");
-  if (a->stages & ~RTFMM_STAGE_ALL) return fail(RTFMM_EINVAL, "unknown stage bits");
+  if (a->stages & ~(RTFMM_STAGE_ALL | RTFMM_STAGE_SERIAL)) return fail(RTFMM_EINVAL, "unknown stage bits");
   for (int k = 0; k < 3; ++k)
     if (!std::isfinite(a->x[k])) return fail(RTFMM_EINVAL, "centre must be finite");
   rtfmm_fmm* f = new (std::nothrow) rtfmm_fmm();
@@ -718,7 +740,7 @@ int rtfmm_b200_create(const rtfmm_args* a, rtfmm_fmm** out) {
   f->args.dipole_correction = a->dipole_correction;
   f->args.divide_4pi = a->divide_4pi;
   f->args.precision = a->precision;
-  f->args.stages = a->stages ? a->stages : RTFMM_STAGE_ALL;
+  f->args.stages = (a->stages & RTFMM_STAGE_ALL) ? a->stages : (a->stages | RTFMM_STAGE_ALL);
   f->args.device = a->device;
   *out = f;
   return RTFMM_OK;
@@ -822,7 +844,7 @@ int rtfmm_b200_evaluate(rtfmm_fmm* f, const double* q, double* phi, double* grad
   }
   CK(cudaSetDevice(f->dev));
   // host -> device (input order), then gather into tree order on the device
-  CK(cudaMemcpyAsync(f->d_xin, f->x_in.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice, f->s0));
+  CK(cudaMemcpyAsync(f->d_xin, f->h_xin, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, f->s0));
   CK(cudaMemcpyAsync(f->d_qin, q ? q : f->q_in.data(), sizeof(double) * n, cudaMemcpyHostToDevice, f->s0));
   CK(launch_gather_bodies(f->d_xin, f->d_qin, f->d_perm, (int)n, f->d_body64, f->s0));
   int rc = enqueue_pass(f);
@@ -881,10 +903,16 @@ int rtfmm_b200_flush_l2(rtfmm_fmm* f) {
 int rtfmm_b200_info(rtfmm_fmm* f, int64_t* info, int cap) {
   if (!f || !info) return fail(RTFMM_EINVAL, "null argument");
   if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");
-  int64_t v[8] = {(int64_t)f->plan.cells.size(), (int64_t)f->leaves.size(), f->plan.dmin, f->plan.dmax,
-                  f->plan.n_p2p, (int64_t)f->plan.m2l.size(), f->plan.n_m2l, f->ops.ns};
-  for (int k = 0; k < 8 && k < cap; ++k) info[k] = v[k];
-  return 8;
+  int64_t pairs = 0;
+  for (size_t l = 0; l < f->leaves.size(); ++l)
+    for (int e = f->list_off[l]; e < f->list_off[l + 1]; ++e)
+      pairs += (int64_t)f->leaves[l].bnum * f->leaves[f->list32[e].leaf].bnum;
+  int64_t td = 0;
+  for (int v8 : f->tsrc8) td += v8 >= 0;
+  int64_t v[12] = {(int64_t)f->plan.cells.size(), (int64_t)f->leaves.size(), f->plan.dmin, f->plan.dmax,
+                   f->plan.n_p2p, (int64_t)f->plan.m2l.size(), f->plan.n_m2l, f->ops.ns, pairs, td, f->nS8, f->nT8};
+  for (int k = 0; k < 12 && k < cap; ++k) info[k] = v[k];
+  return 12;
 }
 
 int rtfmm_b200_get_cells(rtfmm_fmm* f, int32_t* ints, double* reals) {

@@ -26,7 +26,7 @@ LIB_PATH = os.path.join(HERE, "librtfmm_b200.so")
 
 RTFMM_OK, RTFMM_EINVAL, RTFMM_ENOMEM, RTFMM_ECUDA, RTFMM_ESTATE, RTFMM_ENOTSUP = range(6)
 FP64, FP32_MIXED = 0, 1
-STAGE_NEAR, STAGE_FAR, STAGE_ALL = 1, 2, 3
+STAGE_NEAR, STAGE_FAR, STAGE_ALL, STAGE_SERIAL = 1, 2, 3, 4
 STAGE_NAMES = ("prep", "P2M", "M2M", "M2L_up", "M2L_hadamard", "M2L_down", "L2L", "L2P", "P2P", "post")
 
 # Every entry point declared in include/rtfmm_b200.h.
@@ -250,9 +250,10 @@ class LaplaceFMM:
 
     # -- introspection ------------------------------------------------------------
     def info(self):
-        v = np.zeros(8, dtype=np.int64)
-        lib().rtfmm_b200_info(self._h, _ptr(v, _lp), 8)
-        keys = ("ncell", "nleaf", "depth_min", "depth_max", "n_p2p", "n_m2l_parents", "n_m2l", "num_surf")
+        v = np.zeros(12, dtype=np.int64)
+        lib().rtfmm_b200_info(self._h, _ptr(v, _lp), 12)
+        keys = ("ncell", "nleaf", "depth_min", "depth_max", "n_p2p", "n_m2l_parents", "n_m2l", "num_surf",
+                "p2p_pairs", "m2l8_pairs", "m2l8_sources", "m2l8_targets")
         return dict(zip(keys, v.tolist()))
 
     def cells(self):

@@ -46,6 +46,9 @@ typedef enum rtfmm_precision {
 #define RTFMM_STAGE_NEAR 1u   /* P2P                                  */
 #define RTFMM_STAGE_FAR  2u   /* P2M, M2M, M2L, L2L, L2P              */
 #define RTFMM_STAGE_ALL  3u
+/* Diagnostic bit: run P2P after the far field on one stream (no overlap), so
+ * that per-stage times are those of each stage alone. */
+#define RTFMM_STAGE_SERIAL 4u
 
 /*
  * Run parameters.  Replaces rtfmm::Argument (3dpp/include/argument.h:11-45,
@@ -143,9 +146,11 @@ int rtfmm_b200_flush_l2(rtfmm_fmm* fmm);
 
 /* ---- introspection (host data after setup; used by parity tests) ---- */
 
-/* Tree and list sizes.  info[0..7] = ncell (incl. image cells), nleaf,
+/* Tree and list sizes.  info[0..11] = ncell (incl. image cells), nleaf,
  * depth_min, depth_max, n_p2p_entries, n_m2l_parents, n_m2l_entries,
- * num_surf. */
+ * num_surf, P2P body pairs (sum over list entries of n_target * n_source),
+ * 8x8 M2L (target, direction) pairs, 8x8 M2L source parents, 8x8 M2L
+ * target parents.  Returns the number of values available (12). */
 int rtfmm_b200_info(rtfmm_fmm* fmm, int64_t* info, int cap);
 
 /* Cells in the reference's order (Cell3, 3dpp/include/tree.h:9-47):

@@ -702,34 +702,71 @@ def direct_periodic(x, q, images, cycle, targets=None):
     return phi, grad
 
 
-def ewald(x, q, cycle, ksize=11, targets=None):
-    """Ewald sum as in ``EwaldSolver`` (``3dpp/src/ewald.cpp``): alpha =
-    ksize/L, real part for r < L/2 (minimum image), k-space over the
-    (2 ksize + 1)^3 - 1 integer waves, self term -2 alpha q / sqrt(pi).
-    Returns phi and grad(phi) (no 1/4pi, no dipole term)."""
-    from math import erfc as _erfc  # noqa: F401  (scipy-free: vectorised below)
+def _ewald_real_pair(xt, xs, qs, alpha, cutoff):
+    d = xt[:, None, :] - xs[None, :, :]
+    r = np.sqrt(np.sum(d * d, axis=-1))
+    m = (r > 0) & (r < cutoff)
+    rs = np.where(m, r, 1.0)
     import scipy.special as sp
+    e = sp.erfc(alpha * rs)
+    pot = np.where(m, e / rs, 0.0) @ qs
+    coef = np.where(m, (e + 2 * alpha * rs * np.exp(-alpha * alpha * rs * rs) / math.sqrt(math.pi)) / rs ** 3, 0.0)
+    grad = -np.einsum("ts,tsk->tk", coef * qs[None, :], d)
+    return pot, grad
+
+
+def ewald(x, q, cycle, ksize=11, ncrit=64, center=(0.0, 0.0, 0.0), images="reference"):
+    """Ewald sum as ``EwaldSolver`` (``3dpp/src/ewald.cpp``) computes it:
+    alpha = ksize/L (``ewald.cpp:13``), real part for r < L/2, k-space over
+    the (2 ksize + 1)^3 - 1 integer waves (``16-30, 94-109, 177-202``), self
+    term -2 alpha q / sqrt(pi) (``112-118``).  Returns phi and grad(phi), in
+    input order, no 1/(4 pi) and no dipole term.
+
+    images="reference" restates how the reference picks the periodic image
+    of a real-space pair: one offset per pair of leaf cells of its own octree
+    (built with ``ncrit``), from the cell centres with a strict |dx| > L/2
+    test (``ewald.cpp:121-152``).  Leaf cells exactly L/2 apart therefore
+    keep offset 0, and particle pairs that are within the cutoff only through
+    the other image are left out.  images="minimum" uses the per-particle
+    minimum image instead."""
     x = np.asarray(x, dtype=np.float64)
     q = np.asarray(q, dtype=np.float64)
+    n = len(q)
     L = cycle
     alpha = ksize / L
     cutoff = L / 2
-    tgt = np.arange(len(q)) if targets is None else np.asarray(targets)
-    xt = x[tgt]
-    phi = np.zeros(len(tgt))
-    grad = np.zeros((len(tgt), 3))
-    for c0 in range(0, len(q), 1024):
-        xs = x[c0:c0 + 1024]
-        d = xt[:, None, :] - xs[None, :, :]
-        d -= L * np.round(d / L)
-        r = np.sqrt(np.sum(d * d, axis=-1))
-        m = (r > 0) & (r < cutoff)
-        rs = np.where(m, r, 1.0)
-        e = sp.erfc(alpha * rs)
-        pot = np.where(m, e / rs, 0.0)
-        phi += pot @ q[c0:c0 + 1024]
-        coef = np.where(m, (e + 2 * alpha * rs * np.exp(-alpha * alpha * rs * rs) / math.sqrt(math.pi)) / rs ** 3, 0.0)
-        grad -= np.einsum("ts,tsk->tk", coef * q[c0:c0 + 1024][None, :], d)
+    phi = np.zeros(n)
+    grad = np.zeros((n, 3))
+    if images == "reference":
+        cells, perm = build_nonuniform_octree(x, np.asarray(center, dtype=np.float64), L / 2, ncrit)
+        xs, qs = x[perm], q[perm]
+        leaves = [c for c in range(len(cells)) if cells.is_leaf(c)]
+        ph = np.zeros(n)
+        gr = np.zeros((n, 3))
+        for t in leaves:
+            t0, nt = cells.boff[t], cells.bnum[t]
+            for s in leaves:
+                s0, ns = cells.boff[s], cells.bnum[s]
+                dx = cells.x[t] - cells.x[s]
+                off = np.where(dx < -L / 2, -L, np.where(dx > L / 2, L, 0.0))
+                p_, g_ = _ewald_real_pair(xs[t0:t0 + nt], xs[s0:s0 + ns] + off, qs[s0:s0 + ns], alpha, cutoff)
+                ph[t0:t0 + nt] += p_
+                gr[t0:t0 + nt] += g_
+        phi[perm] = ph
+        grad[perm] = gr
+    else:
+        for c0 in range(0, n, 512):
+            xt = x[c0:c0 + 512]
+            d = xt[:, None, :] - x[None, :, :]
+            d -= L * np.round(d / L)
+            r = np.sqrt(np.sum(d * d, axis=-1))
+            m = (r > 0) & (r < cutoff)
+            rs = np.where(m, r, 1.0)
+            import scipy.special as sp
+            e = sp.erfc(alpha * rs)
+            phi[c0:c0 + 512] += np.where(m, e / rs, 0.0) @ q
+            coef = np.where(m, (e + 2 * alpha * rs * np.exp(-alpha * alpha * rs * rs) / math.sqrt(math.pi)) / rs ** 3, 0.0)
+            grad[c0:c0 + 512] -= np.einsum("ts,tsk->tk", coef * q[None, :], d)
     kr = np.arange(-ksize, ksize + 1)
     K = np.stack(np.meshgrid(kr, kr, kr, indexing="ij"), axis=-1).reshape(-1, 3)
     K = K[np.any(K != 0, axis=1)].astype(np.float64)
@@ -741,11 +778,10 @@ def ewald(x, q, cycle, ksize=11, targets=None):
         S = (q[:, None] * np.exp(-1j * ph_s)).sum(axis=0)
         k2 = np.sum(kw * kw, axis=1) * scale * scale
         S *= coef * np.exp(-k2 / (4 * alpha * alpha)) / k2
-        ph_t = (xt @ kw.T) * scale
-        e = np.exp(1j * ph_t) * S[None, :]
+        e = np.exp(1j * ph_s) * S[None, :]
         phi += e.real.sum(axis=1)
         grad += (np.real(e * 1j) * scale) @ kw
-    phi -= (2 / math.sqrt(math.pi)) * q[tgt] * alpha
+    phi -= (2 / math.sqrt(math.pi)) * q * alpha
     return phi, grad
 
 

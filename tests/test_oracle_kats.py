@@ -1,0 +1,90 @@
+"""Pins the CPU oracle (oracle/rtfmm_oracle.py) against the reference itself:
+
+* the FMM energies the reference printed in its published runs
+  (3dpp/exp/slurm-*.out, extracted to golden/log_kats.json), and
+* pointwise outputs of the reference's own LaplaceFMM::solve and EwaldSolver
+  (compiled from its sources; golden/golden_*.npz, made by make_golden.py).
+"""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+# glibc drand48 after srand48(5), printed by a C program
+DRAND48_SEED5 = [0.52483957943423221, 0.2728543017032905, 0.78859946834030481, 0.19806924261769865,
+                 0.51823299065025097, 0.86563752660002535, 0.16917097116524005, 0.47710532000663619]
+
+
+def test_drand48_restatement(oracle):
+    assert oracle.Drand48(5).draws(8).tolist() == DRAND48_SEED5
+
+
+def kat(driver, P, images):
+    kats = json.load(open(os.path.join(GOLDEN, "log_kats.json")))
+    for e in kats:
+        if e["driver"] == driver and e["params"]["P"] == str(P) and e["params"]["images"] == str(images):
+            return e
+    raise KeyError((driver, P, images))
+
+
+@pytest.mark.parametrize("P,images", [(4, 2), (6, 3), (8, 3)])
+def test_periodic_energy_matches_published_runs(oracle, P, images):
+    """test_pbc -n 24000 -m 128 -P P -i images (seed 5, dipole correction on)."""
+    x, q = oracle.generate_random_bodies(24000, math.pi, seed=5, zero_netcharge=1)
+    phi, grad = oracle.solve(x, q, P, 128, images, 2 * math.pi, dipole_correction=1, divide_4pi=0)
+    want = kat("test_pbc", P, images)["energy_fmm"]
+    got = float(np.sum(phi * q))
+    assert abs(got - want) / abs(want) < 1e-9, (got, want)
+
+
+def test_free_space_energy_matches_published_runs(oracle):
+    """test_fmm --setting_t 1 -n 24000 -m 128 -P 6 (non-periodic)."""
+    x, q = oracle.generate_random_bodies(24000, math.pi, seed=5, zero_netcharge=0)
+    phi, grad = oracle.solve(x, q, 6, 128, 0, 2 * math.pi, dipole_correction=0, divide_4pi=1)
+    want = kat("test_fmm", 6, 0)["energy_fmm"]
+    got = float(np.sum(phi * q))
+    assert abs(got - want) / abs(want) < 1e-11, (got, want)
+
+
+def l2(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def load(name):
+    d = np.load(os.path.join(GOLDEN, "golden_%s.npz" % name))
+    return {k: d[k] for k in d.files}
+
+
+@pytest.mark.parametrize("name", ["c1_small", "free_p8", "clustered_i2"])
+def test_oracle_matches_reference_outputs(oracle, name):
+    g = load(name)
+    phi, grad = oracle.solve(g["x"], g["q"], int(g["P"]), int(g["ncrit"]), int(g["images"]), float(g["cycle"]),
+                             dipole_correction=int(g["dipole_correction"]), divide_4pi=int(g["divide_4pi"]))
+    assert l2(grad, g["grad"]) < 1e-9
+    # periodic potentials are compared with their mean removed: rounding in the
+    # ill-conditioned equivalent densities leaves a tiny net charge that the
+    # image levels turn into a constant offset (the energy of a neutral system
+    # and the gradient do not see it)
+    assert l2(phi - phi.mean(), g["phi"] - g["phi"].mean()) < 1e-8
+    assert l2(phi, g["phi"]) < (1e-9 if int(g["images"]) == 0 else 1e-5)
+
+
+def test_oracle_ewald_matches_reference_ewald(oracle):
+    g = load("c1_small")
+    phi, grad = oracle.ewald(g["x"], g["q"], 1.0, ksize=11, ncrit=int(g["ncrit"]))
+    phi, grad = phi / (4 * math.pi), grad / (4 * math.pi)
+    assert l2(phi, g["ewald_phi"]) < 1e-12
+    assert l2(grad, g["ewald_grad"]) < 1e-12
+
+
+def test_fmm_gradient_error_vs_ewald_is_the_published_order(oracle):
+    """P=6 with 3 image levels: the reference's gradient error against Ewald
+    is ~2e-5 (slurm-153085.out: 2.16e-05 at N=24000); on the small fixture
+    the reference's own output sits at the same order."""
+    g = load("c1_small")
+    e = l2(g["grad"], g["ewald_grad"])
+    assert 1e-6 < e < 1e-4
