@@ -82,9 +82,11 @@ def test_oracle_ewald_matches_reference_ewald(oracle):
 
 
 def test_fmm_gradient_error_vs_ewald_is_the_published_order(oracle):
-    """P=6 with 3 image levels: the reference's gradient error against Ewald
-    is ~2e-5 (slurm-153085.out: 2.16e-05 at N=24000); on the small fixture
-    the reference's own output sits at the same order."""
+    """With the dipole correction on, the FMM gradient at P=6 with 3 image
+    levels sits at the image-truncation floor against Ewald: the reference
+    published 2.16e-05 (N=24000, slurm-153085.out:1613); on the 1500-body
+    fixture the oracle lands at the same order."""
     g = load("c1_small")
-    e = l2(g["grad"], g["ewald_grad"])
-    assert 1e-6 < e < 1e-4
+    phi, grad = oracle.solve(g["x"], g["q"], 6, 64, 3, 1.0, dipole_correction=1, divide_4pi=1)
+    e = l2(grad, g["ewald_grad"])
+    assert 1e-5 < e < 1e-4, e
