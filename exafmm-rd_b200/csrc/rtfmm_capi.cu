@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <algorithm>
 #include <cstring>
+#include <functional>
 #include <new>
 #include <string>
 #include <vector>
@@ -43,16 +44,25 @@ int fail(int code, const std::string& msg) {
 
 enum Stage { ST_PREP = 0, ST_P2M, ST_M2M, ST_UP, ST_HAD, ST_DOWN, ST_L2L, ST_L2P, ST_P2P, ST_POST, ST_N };
 
+// Vector buffers an operator application reads or writes (row stride ns).
+enum BufId { BUF_QEQ = 0, BUF_PCHK, BUF_LEAF, BUF_LEAF2, BUF_Y, BUF_NUM };
+
 struct ApplyCall {
   int groups, S, rows_max;
   size_t inrow_off, outrow_off, scale_off, goff_off;  // offsets into the index / scale pools
   int bsel;        // which operator stack
-  int a_is_leafvec, c_is_leafvec;  // A / C on the leaf scratch instead of the cell arrays
+  int abuf, cbuf;  // BufId of A and C
   int beta;
   bool has_scale;
+  size_t sum_off = 0;  // M2M levels: (parent, coff, cnum) triplets summed after the apply
+  int nsum = 0;
 };
 
-enum BSel { B_P2M = 0, B_L2P, B_M2MT, B_M2M, B_IMGSUMT, B_IMG13, B_NUM };
+// Operator stacks, each in the [s][j][n] layout of k_apply_f64:
+//   P2M  (p2m_precompute, kernel.cpp:369-370): y = U^T p, q = scale * V S^-1 y
+//   L2P  (l2p_precompute, kernel.cpp:1465-1467): y = V^T p, q = scale * U S^-1 y
+//   M2M per octant (transposed), L2L = M2M^T per octant, image sum / image 13
+enum BSel { B_P2M1 = 0, B_P2M2, B_L2P1, B_L2P2, B_M2MT, B_M2M, B_IMGSUMT, B_IMG13, B_NUM };
 
 }  // namespace
 
@@ -71,7 +81,8 @@ struct rtfmm_fmm {
   // host plan tables
   std::vector<LeafInfo> leaves;
   std::vector<int> body_leaf;
-  std::vector<P2PItem> items;
+  std::vector<P2PItem> items;    // 32 targets per item (FP64 P2P)
+  std::vector<P2PItem> items2;   // 64 targets per item (FP32 P2P)
   std::vector<int> list_off;
   std::vector<P2PSrc32> list32;
   std::vector<P2PSrc64> list64;
@@ -95,10 +106,11 @@ struct rtfmm_fmm {
   int64_t* d_perm = nullptr;
   double *d_xin = nullptr, *d_qin = nullptr;
   LeafInfo* d_leaves = nullptr;
-  double *d_qeq = nullptr, *d_pchk = nullptr, *d_leafvec = nullptr;
+  double *d_qeq = nullptr, *d_pchk = nullptr, *d_leafvec = nullptr, *d_leafvec2 = nullptr, *d_y = nullptr;
   double *d_far_phi = nullptr, *d_far_grad = nullptr, *d_near_phi = nullptr, *d_near_grad = nullptr;
   double *d_out_phi = nullptr, *d_out_grad = nullptr;
   P2PItem* d_items = nullptr;
+  P2PItem* d_items2 = nullptr;
   int* d_list_off = nullptr;
   P2PSrc32* d_list32 = nullptr;
   P2PSrc64* d_list64 = nullptr;
@@ -199,38 +211,66 @@ void build_tables(rtfmm_fmm* f) {
   for (int l = 0; l < (int)f->leaves.size(); ++l)
     for (int b = 0; b < f->leaves[l].bnum; ++b) f->body_leaf[f->leaves[l].boff + b] = l;
 
-  // P2P lists in CSR by target leaf; work items of 32 targets
+  // P2P lists in CSR by target leaf; work items of 32 / 64 targets.  The
+  // reference's M2P/P2L-to-P2P conversions (traverser.cpp:75-86) can pair a
+  // non-leaf cell with a leaf, evaluated over the cell's whole body range
+  // (p2p_1toN_256, kernel.cpp:276-301).  Such a pair is expanded here into
+  // the leaf pairs beneath it (same bodies, same sum), so that every list
+  // entry is leaf to leaf and FP32 positions can stay leaf-relative.
+  std::vector<std::vector<int>> under(p.ntree);
+  std::function<const std::vector<int>&(int)> leaves_under = [&](int c) -> const std::vector<int>& {
+    std::vector<int>& v = under[c];
+    if (!v.empty()) return v;
+    const Cell& cl = p.cells[c];
+    if (cl.cnum == 0) {
+      v.push_back(c);
+    } else {
+      for (int k = 0; k < cl.cnum; ++k) {
+        const std::vector<int>& w = leaves_under(cl.coff + k);
+        v.insert(v.end(), w.begin(), w.end());
+      }
+    }
+    return v;
+  };
+  std::vector<std::vector<P2PEntry>> leaf_lists(f->leaves.size());
+  for (auto& kv : p.p2p) {
+    const std::vector<int> tl = leaves_under(kv.first);
+    for (const P2PEntry& e : kv.second) {
+      const std::vector<int>& sl = leaves_under(e.src);
+      for (int t : tl)
+        for (int sc : sl) leaf_lists[leaf_of_cell[t]].push_back({sc, e.off});
+    }
+  }
   f->list_off.assign(f->leaves.size() + 1, 0);
   f->list32.clear();
   f->list64.clear();
   f->items.clear();
+  f->items2.clear();
   for (int l = 0; l < (int)f->leaves.size(); ++l) {
     f->list_off[l] = (int)f->list32.size();
     const int c = f->leaves[l].cell;
-    auto it = p.p2p.find(c);
-    if (it != p.p2p.end()) {
-      for (const P2PEntry& e : it->second) {
-        const int sl = leaf_of_cell[e.src];
-        const Cell& S = p.cells[e.src];
-        const Cell& T = p.cells[c];
-        P2PSrc32 a;
-        a.dx = (float)(S.x[0] + e.off[0] - T.x[0]);
-        a.dy = (float)(S.x[1] + e.off[1] - T.x[1]);
-        a.dz = (float)(S.x[2] + e.off[2] - T.x[2]);
-        a.leaf = sl;
-        a.self = (e.src == c && e.off[0] == 0 && e.off[1] == 0 && e.off[2] == 0) ? 1 : 0;
-        a.pad[0] = a.pad[1] = a.pad[2] = 0;
-        f->list32.push_back(a);
-        P2PSrc64 b;
-        b.ox = e.off[0];
-        b.oy = e.off[1];
-        b.oz = e.off[2];
-        b.leaf = sl;
-        b.self = a.self;
-        f->list64.push_back(b);
-      }
+    for (const P2PEntry& e : leaf_lists[l]) {
+      const int sl = leaf_of_cell[e.src];
+      const Cell& S = p.cells[e.src];
+      const Cell& T = p.cells[c];
+      P2PSrc32 a;
+      a.dx = (float)(S.x[0] + e.off[0] - T.x[0]);
+      a.dy = (float)(S.x[1] + e.off[1] - T.x[1]);
+      a.dz = (float)(S.x[2] + e.off[2] - T.x[2]);
+      a.leaf = sl;
+      a.self = (e.src == c && e.off[0] == 0 && e.off[1] == 0 && e.off[2] == 0) ? 1 : 0;
+      a.pad[0] = a.pad[1] = a.pad[2] = 0;
+      f->list32.push_back(a);
+      P2PSrc64 b;
+      b.ox = e.off[0];
+      b.oy = e.off[1];
+      b.oz = e.off[2];
+      b.leaf = sl;
+      b.self = a.self;
+      f->list64.push_back(b);
     }
     for (int t0 = 0; t0 < f->leaves[l].bnum; t0 += 32) f->items.push_back({l, t0});
+    for (int t0 = 0; t0 < f->leaves[l].bnum; t0 += 64) f->items2.push_back({l, t0});
   }
   f->list_off[f->leaves.size()] = (int)f->list32.size();
 
@@ -239,14 +279,14 @@ void build_tables(rtfmm_fmm* f) {
   f->scale_pool.clear();
   auto add_call = [&](std::vector<ApplyCall>& dst, int S, const std::vector<std::vector<int>>& in_by_group,
                       const std::vector<std::vector<int>>& out_by_group, const std::vector<double>* scale,
-                      int bsel, int a_leaf, int c_leaf, int beta) {
+                      int bsel, int abuf, int cbuf, int beta) {
     ApplyCall ac;
     ac.groups = (int)out_by_group.size();
     ac.S = S;
     ac.rows_max = 0;
     ac.bsel = bsel;
-    ac.a_is_leafvec = a_leaf;
-    ac.c_is_leafvec = c_leaf;
+    ac.abuf = abuf;
+    ac.cbuf = cbuf;
     ac.beta = beta;
     ac.has_scale = scale != nullptr;
     ac.goff_off = f->idx_pool.size();
@@ -277,34 +317,45 @@ void build_tables(rtfmm_fmm* f) {
       out.push_back(f->leaves[l].cell);
       sc.push_back(f->leaves[l].scale);
     }
-    add_call(f->p2m_call, 1, {in}, {out}, &sc, B_P2M, 1, 0, 0);
-    std::vector<int> in2, out2;
-    for (int l = 0; l < (int)f->leaves.size(); ++l) {
-      in2.push_back(f->leaves[l].cell);
-      out2.push_back(l);
-    }
-    add_call(f->l2p_call, 1, {in2}, {out2}, &sc, B_L2P, 0, 1, 0);
+    std::vector<int> lid(f->leaves.size());
+    for (int l = 0; l < (int)f->leaves.size(); ++l) lid[l] = l;
+    add_call(f->p2m_call, 1, {lid}, {lid}, nullptr, B_P2M1, BUF_LEAF, BUF_LEAF2, 0);
+    add_call(f->p2m_call, 1, {lid}, {out}, &sc, B_P2M2, BUF_LEAF2, BUF_QEQ, 0);
+    add_call(f->l2p_call, 1, {out}, {lid}, nullptr, B_L2P1, BUF_PCHK, BUF_LEAF, 0);
+    add_call(f->l2p_call, 1, {lid}, {lid}, &sc, B_L2P2, BUF_LEAF, BUF_LEAF2, 0);
   }
-  // M2M bottom-up (fmm.cpp:111-150): depth = dmax .. dmin+1
+  // M2M bottom-up (fmm.cpp:111-150): depth = dmax .. dmin+1.  For depth >= 0
+  // each child's contribution M2M[octant] q_child is one row of a batched
+  // apply grouped by octant (into the Y scratch), then each parent sums its
+  // children in crange order (m2m_precompute, kernel.cpp:395-404).
   for (int depth = p.dmax; depth > p.dmin; --depth) {
-    std::vector<int> in, out;
+    std::vector<std::vector<int>> in(8), out(8);
+    std::vector<int> in1, out1, sums;
     for (int c = 0; c < (int)p.cells.size(); ++c) {
       const Cell& cl = p.cells[c];
       if (cl.depth != depth || cl.cnum == 0) continue;
-      out.push_back(c);
       if (depth >= 0) {
-        int slot[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
-        for (int k = 0; k < cl.cnum; ++k) slot[p.cells[cl.coff + k].octant] = cl.coff + k;
-        in.insert(in.end(), slot, slot + 8);
+        for (int k = 0; k < cl.cnum; ++k) {
+          const int ch = cl.coff + k;
+          in[p.cells[ch].octant].push_back(ch);
+          out[p.cells[ch].octant].push_back(ch);
+        }
+        sums.push_back(c);
+        sums.push_back(cl.coff);
+        sums.push_back(cl.cnum);
       } else {
-        in.push_back(cl.coff);
+        in1.push_back(cl.coff);
+        out1.push_back(c);
       }
     }
-    if (out.empty()) continue;
-    if (depth >= 0)
-      add_call(f->m2m_calls, 8, {in}, {out}, nullptr, B_M2MT, 0, 0, 0);
-    else
-      add_call(f->m2m_calls, 1, {in}, {out}, nullptr, B_IMGSUMT, 0, 0, 0);
+    if (depth >= 0 && !sums.empty()) {
+      add_call(f->m2m_calls, 1, in, out, nullptr, B_M2MT, BUF_QEQ, BUF_Y, 0);
+      f->m2m_calls.back().sum_off = f->idx_pool.size();
+      f->m2m_calls.back().nsum = (int)sums.size() / 3;
+      f->idx_pool.insert(f->idx_pool.end(), sums.begin(), sums.end());
+    } else if (depth < 0 && !out1.empty()) {
+      add_call(f->m2m_calls, 1, {in1}, {out1}, nullptr, B_IMGSUMT, BUF_QEQ, BUF_QEQ, 0);
+    }
   }
   // L2L top-down (fmm.cpp:195-229): depth = dmin .. dmax-1
   for (int depth = p.dmin; depth < p.dmax; ++depth) {
@@ -327,9 +378,9 @@ void build_tables(rtfmm_fmm* f) {
     if (depth >= 0) {
       bool any = false;
       for (auto& g : out) any |= !g.empty();
-      if (any) add_call(f->l2l_calls, 1, in, out, nullptr, B_M2M, 0, 0, 1);
+      if (any) add_call(f->l2l_calls, 1, in, out, nullptr, B_M2M, BUF_PCHK, BUF_PCHK, 1);
     } else if (!out1.empty()) {
-      add_call(f->l2l_calls, 1, {in1}, {out1}, nullptr, B_IMG13, 0, 0, 1);
+      add_call(f->l2l_calls, 1, {in1}, {out1}, nullptr, B_IMG13, BUF_PCHK, BUF_PCHK, 1);
     }
   }
 
@@ -451,6 +502,8 @@ int upload_plan(rtfmm_fmm* f) {
   RC(dalloc(f, &f->d_qeq, ncell * ns));
   RC(dalloc(f, &f->d_pchk, ncell * ns));
   RC(dalloc(f, &f->d_leafvec, nleaf * ns));
+  RC(dalloc(f, &f->d_leafvec2, nleaf * ns));
+  RC(dalloc(f, &f->d_y, ncell * ns));
   RC(dalloc(f, &f->d_far_phi, n));
   RC(dalloc(f, &f->d_far_grad, 3 * n));
   RC(dalloc(f, &f->d_near_phi, n));
@@ -458,6 +511,7 @@ int upload_plan(rtfmm_fmm* f) {
   RC(dalloc(f, &f->d_out_phi, n));
   RC(dalloc(f, &f->d_out_grad, 3 * n));
   RC(dupload(f, &f->d_items, f->items));
+  RC(dupload(f, &f->d_items2, f->items2));
   RC(dupload(f, &f->d_list_off, f->list_off));
   RC(dupload(f, &f->d_list32, f->list32));
   RC(dupload(f, &f->d_list64, f->list64));
@@ -472,10 +526,18 @@ int upload_plan(rtfmm_fmm* f) {
   // operator stacks in the [s][j][n] layout of k_apply_f64
   const size_t nn = (size_t)ns * ns;
   std::vector<double> b;
-  b = o.pinv_down;  // P2M: B[j][n] = pinv_up[n][j]
-  RC(dupload(f, &f->d_B[B_P2M], b));
-  b = o.pinv_up;    // L2P: B[j][n] = pinv_down[n][j]
-  RC(dupload(f, &f->d_B[B_L2P], b));
+  b = o.U;  // y[n] = sum_j U^T[n][j] p[j]
+  RC(dupload(f, &f->d_B[B_P2M1], b));
+  b.assign(nn, 0.0);
+  for (int j = 0; j < ns; ++j)
+    for (int i = 0; i < ns; ++i) b[(size_t)j * ns + i] = o.V[(size_t)i * ns + j] * o.sinv[j];
+  RC(dupload(f, &f->d_B[B_P2M2], b));
+  b = o.V;  // y[n] = sum_j V^T[n][j] p[j]
+  RC(dupload(f, &f->d_B[B_L2P1], b));
+  b.assign(nn, 0.0);
+  for (int j = 0; j < ns; ++j)
+    for (int i = 0; i < ns; ++i) b[(size_t)j * ns + i] = o.U[(size_t)i * ns + j] * o.sinv[j];
+  RC(dupload(f, &f->d_B[B_L2P2], b));
   b.assign(8 * nn, 0.0);
   for (int oc = 0; oc < 8; ++oc)
     for (int j = 0; j < ns; ++j)
@@ -539,8 +601,9 @@ int upload_plan(rtfmm_fmm* f) {
 
 int run_apply(rtfmm_fmm* f, const ApplyCall& c) {
   ApplyBatch b;
-  b.A = c.a_is_leafvec ? f->d_leafvec : (c.bsel == B_L2P || c.bsel == B_M2M || c.bsel == B_IMG13 ? f->d_pchk : f->d_qeq);
-  b.C = c.c_is_leafvec ? f->d_leafvec : (c.bsel == B_M2M || c.bsel == B_IMG13 ? f->d_pchk : f->d_qeq);
+  double* bufs[BUF_NUM] = {f->d_qeq, f->d_pchk, f->d_leafvec, f->d_leafvec2, f->d_y};
+  b.A = bufs[c.abuf];
+  b.C = bufs[c.cbuf];
   b.inrow = f->d_idx_pool + c.inrow_off;
   b.outrow = f->d_idx_pool + c.outrow_off;
   b.group_off = f->d_idx_pool + c.goff_off;
@@ -553,6 +616,10 @@ int run_apply(rtfmm_fmm* f, const ApplyCall& c) {
   b.max_rows = c.rows_max;
   CK(launch_apply(b, f->s0));
   f->launches++;
+  if (c.nsum > 0) {
+    CK(launch_sum_children(f->d_idx_pool + c.sum_off, c.nsum, f->d_y, f->ops.ns, f->d_qeq, f->s0));
+    f->launches++;
+  }
   return RTFMM_OK;
 }
 
@@ -577,7 +644,7 @@ int enqueue_pass(rtfmm_fmm* f) {
     }
     CK(cudaEventRecord(f->ev_near0, s1));
     if (mixed) {
-      CK(launch_p2p32(f->d_body32, f->d_leaves, f->d_items, (int)f->items.size(), f->d_list_off, f->d_list32,
+      CK(launch_p2p32(f->d_body32, f->d_leaves, f->d_items2, (int)f->items2.size(), f->d_list_off, f->d_list32,
                       f->d_near_phi, f->d_near_grad, s1));
       f->launches += 1;
     } else {
@@ -648,7 +715,7 @@ int enqueue_pass(rtfmm_fmm* f) {
       int rc = run_apply(f, c);
       if (rc) return rc;
     }
-    CK(launch_l2p_eval(f->d_body64, f->d_leaves, nleaf, f->d_surf_unit, ns, f->d_leafvec, f->d_far_phi,
+    CK(launch_l2p_eval(f->d_body64, f->d_leaves, nleaf, f->d_surf_unit, ns, f->d_leafvec2, f->d_far_phi,
                        f->d_far_grad, s0));
     f->launches++;
     CK(cudaEventRecord(f->ev_st[ST_L2P], s0));

@@ -55,72 +55,104 @@ __global__ void k_prep32(const double4* __restrict__ body64, const int* __restri
 }
 
 // ---------------------------------------------------------------------------
-// P2P: one warp per (target leaf, 32 targets); sources staged 32 at a time in
-// a per-warp shared-memory slot and read as broadcasts.  FP32 partial sums
-// per source leaf are accumulated into FP64.
+// P2P: one warp per (target leaf, block of targets); sources staged 32 at a
+// time in a per-warp shared-memory slot and read as broadcasts.  FP32 partial
+// sums per source leaf are accumulated into FP64.
 // ---------------------------------------------------------------------------
 constexpr int kP2PWarps = 4;
 
+// Each source is staged twice-duplicated and pre-negated, so that one
+// packed f32x2 operation serves a lane's two targets:
+//   s[2k]   = (-x, -x, -y, -y),  s[2k+1] = (-z, -z, q, q)
 template <bool MASK>
-__device__ __forceinline__ void p2p32_tile(const float4* __restrict__ s, int cnt, float px, float py,
-                                           float pz, float& p, float& fx, float& fy, float& fz) {
-#pragma unroll 8
+__device__ __forceinline__ void p2p32_tile(const float4* __restrict__ s, int cnt, float2 px, float2 py,
+                                           float2 pz, float2& p, float2& fx, float2& fy, float2& fz) {
+#pragma unroll 4
   for (int k = 0; k < cnt; ++k) {
-    const float4 b = s[k];
-    const float dx = px - b.x, dy = py - b.y, dz = pz - b.z;
-    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-    float ir = rsqrt_approx(r2);
-    if (MASK) ir = r2 > 0.f ? ir : 0.f;
-    const float qir = b.w * ir;
-    p += qir;
-    const float q3 = qir * ir * ir;
-    fx = fmaf(q3, dx, fx);
-    fy = fmaf(q3, dy, fy);
-    fz = fmaf(q3, dz, fz);
+    const float4 u = s[2 * k], v = s[2 * k + 1];
+    const float2 dx = __fadd2_rn(px, make_float2(u.x, u.y));
+    const float2 dy = __fadd2_rn(py, make_float2(u.z, u.w));
+    const float2 dz = __fadd2_rn(pz, make_float2(v.x, v.y));
+    float2 r2 = __fmul2_rn(dz, dz);
+    r2 = __ffma2_rn(dy, dy, r2);
+    r2 = __ffma2_rn(dx, dx, r2);
+    float2 ir = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+    if (MASK) {
+      ir.x = r2.x > 0.f ? ir.x : 0.f;
+      ir.y = r2.y > 0.f ? ir.y : 0.f;
+    }
+    const float2 qir = __fmul2_rn(make_float2(v.z, v.w), ir);
+    p = __fadd2_rn(p, qir);
+    const float2 q3 = __fmul2_rn(__fmul2_rn(qir, ir), ir);
+    fx = __ffma2_rn(q3, dx, fx);
+    fy = __ffma2_rn(q3, dy, fy);
+    fz = __ffma2_rn(q3, dz, fz);
   }
 }
 
+// One warp per (target leaf, 64 targets): lane l owns targets t0+l and
+// t0+32+l and evaluates both with packed f32x2 arithmetic.
 __global__ void __launch_bounds__(32 * kP2PWarps)
     k_p2p32(const float4* __restrict__ body32, const LeafInfo* __restrict__ leaves,
             const P2PItem* __restrict__ items, int nitems, const int* __restrict__ list_off,
             const P2PSrc32* __restrict__ list, double* __restrict__ phi, double* __restrict__ grad) {
-  __shared__ float4 sbuf[kP2PWarps][32];
+  __shared__ float4 sbuf[kP2PWarps][64];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int item = blockIdx.x * kP2PWarps + warp;
   if (item >= nitems) return;  // warp-uniform
   const P2PItem it = items[item];
   const LeafInfo T = leaves[it.leaf];
-  const int t = it.t0 + lane;
-  const bool active = t < T.bnum;
-  const float4 xt = active ? body32[T.boff + t] : make_float4(0.f, 0.f, 0.f, 0.f);
-  double P = 0.0, Gx = 0.0, Gy = 0.0, Gz = 0.0;
+  const int ta = it.t0 + lane, tb = it.t0 + 32 + lane;
+  const bool va = ta < T.bnum, vb = tb < T.bnum;
+  const float4 xa = va ? body32[T.boff + ta] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float4 xb = vb ? body32[T.boff + tb] : make_float4(0.f, 0.f, 0.f, 0.f);
+  double Pa = 0.0, Gxa = 0.0, Gya = 0.0, Gza = 0.0;
+  double Pb = 0.0, Gxb = 0.0, Gyb = 0.0, Gzb = 0.0;
   const int e1 = list_off[it.leaf + 1];
+  float4* sw = sbuf[warp];
   for (int e = list_off[it.leaf]; e < e1; ++e) {
     const P2PSrc32 src = list[e];
     const LeafInfo S = leaves[src.leaf];
-    const float px = xt.x - src.dx, py = xt.y - src.dy, pz = xt.z - src.dz;
-    float p = 0.f, fx = 0.f, fy = 0.f, fz = 0.f;
+    const float2 px = make_float2(xa.x - src.dx, xb.x - src.dx);
+    const float2 py = make_float2(xa.y - src.dy, xb.y - src.dy);
+    const float2 pz = make_float2(xa.z - src.dz, xb.z - src.dz);
+    float2 p = make_float2(0.f, 0.f), fx = p, fy = p, fz = p;
     for (int c0 = 0; c0 < S.bnum; c0 += 32) {
       const int cnt = min(32, S.bnum - c0);
       __syncwarp();
-      if (lane < cnt) sbuf[warp][lane] = body32[S.boff + c0 + lane];
+      if (lane < cnt) {
+        const float4 b = body32[S.boff + c0 + lane];
+        sw[2 * lane] = make_float4(-b.x, -b.x, -b.y, -b.y);
+        sw[2 * lane + 1] = make_float4(-b.z, -b.z, b.w, b.w);
+      }
       __syncwarp();
       if (src.self)
-        p2p32_tile<true>(sbuf[warp], cnt, px, py, pz, p, fx, fy, fz);
+        p2p32_tile<true>(sw, cnt, px, py, pz, p, fx, fy, fz);
       else
-        p2p32_tile<false>(sbuf[warp], cnt, px, py, pz, p, fx, fy, fz);
+        p2p32_tile<false>(sw, cnt, px, py, pz, p, fx, fy, fz);
     }
-    P += (double)p;
-    Gx += (double)fx;
-    Gy += (double)fy;
-    Gz += (double)fz;
+    Pa += (double)p.x;
+    Gxa += (double)fx.x;
+    Gya += (double)fy.x;
+    Gza += (double)fz.x;
+    Pb += (double)p.y;
+    Gxb += (double)fx.y;
+    Gyb += (double)fy.y;
+    Gzb += (double)fz.y;
   }
-  if (active) {
-    const int b = T.boff + t;
-    phi[b] = P;
-    grad[3 * b + 0] = -Gx;
-    grad[3 * b + 1] = -Gy;
-    grad[3 * b + 2] = -Gz;
+  if (va) {
+    const int b = T.boff + ta;
+    phi[b] = Pa;
+    grad[3 * b + 0] = -Gxa;
+    grad[3 * b + 1] = -Gya;
+    grad[3 * b + 2] = -Gza;
+  }
+  if (vb) {
+    const int b = T.boff + tb;
+    phi[b] = Pb;
+    grad[3 * b + 0] = -Gxb;
+    grad[3 * b + 1] = -Gyb;
+    grad[3 * b + 2] = -Gzb;
   }
 }
 
@@ -334,6 +366,20 @@ __global__ void __launch_bounds__(256) k_apply_f64(ApplyBatch b) {
   }
 }
 
+// Sibling sum of the per-child M2M products, in crange order
+// (m2m_precompute accumulates child by child, kernel.cpp:398-403).
+__global__ void k_sum_children(const int* __restrict__ list, int nparents, const double* __restrict__ Y, int ns,
+                               double* __restrict__ q) {
+  const int pidx = blockIdx.x;
+  if (pidx >= nparents) return;
+  const int par = list[3 * pidx], coff = list[3 * pidx + 1], cnum = list[3 * pidx + 2];
+  for (int n = threadIdx.x; n < ns; n += blockDim.x) {
+    double acc = 0.0;
+    for (int c = 0; c < cnum; ++c) acc += Y[(size_t)(coff + c) * ns + n];
+    q[(size_t)par * ns + n] = acc;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // FFT-M2L.  Grids are N = 2P-1 points per edge, stored [z][y][x]; spectra are
 // the r2c half-spectrum [kz][ky][kx], kx < P.  The twiddle table holds
@@ -363,7 +409,7 @@ __global__ void __launch_bounds__(256)
   T* cube = sm;                    // P^3
   T* A = cube + P3;                // P^3 complex: [z][y][kx]
   T* Bm = A + 2 * P3;              // P*N*P complex: [z][ky][kx]
-  T* w = Bm + 2 * P * N * P;       // N complex
+  T* W = Bm + 2 * P * N * P;       // N*N complex: W[k][n] = w^(k n mod N)
   const int src = items[3 * blockIdx.x], slot = items[3 * blockIdx.x + 1], child = items[3 * blockIdx.x + 2];
   T* out = Q + ((size_t)src * 8 + slot) * Nf * 2;
   const int tid = threadIdx.x, nt = blockDim.x;
@@ -371,7 +417,11 @@ __global__ void __launch_bounds__(256)
     for (int f = tid; f < 2 * Nf; f += nt) out[f] = T(0);
     return;
   }
-  for (int m = tid; m < 2 * N; m += nt) w[m] = (T)twiddle[m];
+  for (int e = tid; e < N * N; e += nt) {
+    const int m = ((e / N) * (e % N)) % N;
+    W[2 * e] = (T)twiddle[2 * m];
+    W[2 * e + 1] = (T)twiddle[2 * m + 1];
+  }
   for (int e = tid; e < P3; e += nt) cube[e] = T(0);
   __syncthreads();
   for (int i = tid; i < ns; i += nt) {
@@ -383,10 +433,10 @@ __global__ void __launch_bounds__(256)
     const int z = e / (P * P), y = (e / P) % P, kx = e % P;
     T re = 0, im = 0;
     const T* row = cube + (z * P + y) * P;
+    const T* wk = W + 2 * kx * N;
     for (int x = 0; x < P; ++x) {
-      const int m = (kx * x) % N;
-      re = fma(row[x], w[2 * m], re);
-      im = fma(row[x], w[2 * m + 1], im);
+      re = fma(row[x], wk[2 * x], re);
+      im = fma(row[x], wk[2 * x + 1], im);
     }
     A[2 * e] = re;
     A[2 * e + 1] = im;
@@ -395,10 +445,10 @@ __global__ void __launch_bounds__(256)
   for (int e = tid; e < P * N * P; e += nt) {
     const int z = e / (N * P), ky = (e / P) % N, kx = e % P;
     T re = 0, im = 0;
+    const T* wk = W + 2 * ky * N;
     for (int y = 0; y < P; ++y) {
-      const int m = (ky * y) % N;
       const int a = (z * P + y) * P + kx;
-      cmad(re, im, A[2 * a], A[2 * a + 1], w[2 * m], w[2 * m + 1]);
+      cmad(re, im, A[2 * a], A[2 * a + 1], wk[2 * y], wk[2 * y + 1]);
     }
     Bm[2 * e] = re;
     Bm[2 * e + 1] = im;
@@ -407,10 +457,10 @@ __global__ void __launch_bounds__(256)
   for (int f = tid; f < Nf; f += nt) {
     const int kz = f / (N * P), ky = (f / P) % N, kx = f % P;
     T re = 0, im = 0;
+    const T* wk = W + 2 * kz * N;
     for (int z = 0; z < P; ++z) {
-      const int m = (kz * z) % N;
       const int b = (z * N + ky) * P + kx;
-      cmad(re, im, Bm[2 * b], Bm[2 * b + 1], w[2 * m], w[2 * m + 1]);
+      cmad(re, im, Bm[2 * b], Bm[2 * b + 1], wk[2 * z], wk[2 * z + 1]);
     }
     out[2 * f] = re;
     out[2 * f + 1] = im;
@@ -551,21 +601,25 @@ __global__ void __launch_bounds__(256)
   T* X = sm;                        // Nf complex
   T* Y1 = X + 2 * Nf;               // P*N*P complex: [zo][ky][kx]
   T* Y2 = Y1 + 2 * P * N * P;       // P^3 complex: [zo][yo][kx]
-  T* w = Y2 + 2 * P3;               // N complex
+  T* W = Y2 + 2 * P3;               // P*N complex: W[o][k] = conj(w)^(k (P-1+o) mod N)
   const int tar = items[3 * blockIdx.x], slot = items[3 * blockIdx.x + 1], child = items[3 * blockIdx.x + 2];
   const T* in = Pk + ((size_t)tar * 8 + slot) * Nf * 2;
   const int tid = threadIdx.x, nt = blockDim.x;
-  for (int m = tid; m < 2 * N; m += nt) w[m] = (T)twiddle[m];
+  for (int e = tid; e < P * N; e += nt) {
+    const int o = e / N, k = e % N;
+    const int m = (k * (P - 1 + o)) % N;
+    W[2 * e] = (T)twiddle[2 * m];
+    W[2 * e + 1] = -(T)twiddle[2 * m + 1];
+  }
   for (int e = tid; e < 2 * Nf; e += nt) X[e] = in[e];
   __syncthreads();
   for (int e = tid; e < P * N * P; e += nt) {
     const int zo = e / (N * P), ky = (e / P) % N, kx = e % P;
-    const int z = P - 1 + zo;
+    const T* wo = W + 2 * zo * N;
     T re = 0, im = 0;
     for (int kz = 0; kz < N; ++kz) {
-      const int m = (kz * z) % N;
       const int a = (kz * N + ky) * P + kx;
-      cmad(re, im, X[2 * a], X[2 * a + 1], w[2 * m], -w[2 * m + 1]);
+      cmad(re, im, X[2 * a], X[2 * a + 1], wo[2 * kz], wo[2 * kz + 1]);
     }
     Y1[2 * e] = re;
     Y1[2 * e + 1] = im;
@@ -573,12 +627,11 @@ __global__ void __launch_bounds__(256)
   __syncthreads();
   for (int e = tid; e < P3; e += nt) {
     const int zo = e / (P * P), yo = (e / P) % P, kx = e % P;
-    const int y = P - 1 + yo;
+    const T* wo = W + 2 * yo * N;
     T re = 0, im = 0;
     for (int ky = 0; ky < N; ++ky) {
-      const int m = (ky * y) % N;
       const int a = (zo * N + ky) * P + kx;
-      cmad(re, im, Y1[2 * a], Y1[2 * a + 1], w[2 * m], -w[2 * m + 1]);
+      cmad(re, im, Y1[2 * a], Y1[2 * a + 1], wo[2 * ky], wo[2 * ky + 1]);
     }
     Y2[2 * e] = re;
     Y2[2 * e + 1] = im;
@@ -587,17 +640,15 @@ __global__ void __launch_bounds__(256)
   const double sc = tscale[tar];
   for (int i = tid; i < ns; i += nt) {
     const int xo = surf_ijk[3 * i], yo = surf_ijk[3 * i + 1], zo = surf_ijk[3 * i + 2];
-    const int x = P - 1 + xo;
     const T* row = Y2 + 2 * ((zo * P + yo) * P);
-    T v = row[0];
+    const T* wo = W + 2 * xo * N;
     T acc = 0;
+    // Re(Y * conj(w)^m) summed over kx >= 1, doubled for the missing half
     for (int kx = 1; kx < P; ++kx) {
-      const int m = (kx * x) % N;
-      // Re(Y * conj(w^m)) = Yr * wr + Yi * wi
-      acc = fma(row[2 * kx], w[2 * m], acc);
-      acc = fma(row[2 * kx + 1], w[2 * m + 1], acc);
+      acc = fma(row[2 * kx], wo[2 * kx], acc);
+      acc = fma(-row[2 * kx + 1], wo[2 * kx + 1], acc);
     }
-    v += T(2) * acc;
+    const T v = row[0] + T(2) * acc;
     p_check[(size_t)child * ns + i] += (double)v * sc;
   }
 }
@@ -736,15 +787,21 @@ cudaError_t launch_apply(const ApplyBatch& b, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+cudaError_t launch_sum_children(const int* list, int nparents, const double* Y, int ns, double* q,
+                                cudaStream_t st) {
+  if (nparents > 0) k_sum_children<<<nparents, 128, 0, st>>>(list, nparents, Y, ns, q);
+  return cudaGetLastError();
+}
+
 template <typename T>
 static size_t up_smem(int P) {
   const int N = 2 * P - 1;
-  return sizeof(T) * ((size_t)3 * P * P * P + 2 * (size_t)P * N * P + 2 * N);
+  return sizeof(T) * ((size_t)3 * P * P * P + 2 * (size_t)P * N * P + 2 * (size_t)N * N);
 }
 template <typename T>
 static size_t down_smem(int P) {
   const int N = 2 * P - 1;
-  return sizeof(T) * (2 * (size_t)N * N * P + 2 * (size_t)P * N * P + 2 * (size_t)P * P * P + 2 * N);
+  return sizeof(T) * (2 * (size_t)N * N * P + 2 * (size_t)P * N * P + 2 * (size_t)P * P * P + 2 * (size_t)P * N);
 }
 
 template <typename T>

@@ -16,7 +16,8 @@ struct LeafInfo {
   int boff, bnum;      // bodies in tree order
 };
 
-// FP32 P2P work item: up to 32 targets of one leaf.
+// P2P work item: a block of targets of one leaf (64 for the FP32 kernel, 32
+// for the FP64 kernel).
 struct P2PItem {
   int leaf;   // leaf-table index of the target leaf
   int t0;     // first target (offset inside the leaf)
@@ -60,6 +61,10 @@ cudaError_t launch_p2p64(const double4* body64, const LeafInfo* leaves, const P2
 cudaError_t launch_p2m_check(const double4* body64, const LeafInfo* leaves, int nleaf,
                              const double* surf_unit, int ns, double* out, cudaStream_t st);
 cudaError_t launch_apply(const ApplyBatch& b, cudaStream_t st);
+// q[parent] = sum of Y[child] over the parent's children; `list` holds
+// (parent, coff, cnum) triplets
+cudaError_t launch_sum_children(const int* list, int nparents, const double* Y, int ns, double* q,
+                                cudaStream_t st);
 template <typename T>
 cudaError_t launch_m2l_up(const double* q_equiv, const int* items /*(src,slot,child)*/, int nitems,
                           const int* surf_ijk, const double* twiddle, int P, int ns, T* Q,

@@ -527,6 +527,9 @@ void build_operators(Operators& o, int P, double r0, int images) {
       o.UT[(size_t)k * ns + i] = U[(size_t)i * ns + k];
       o.VSinv[(size_t)i * ns + k] = V[(size_t)i * ns + k] * sinv[k];
     }
+  o.U = U;
+  o.V = V;
+  o.sinv = sinv;
   o.pinv_up.assign((size_t)ns * ns, 0);
   matmul(ns, o.VSinv.data(), o.UT.data(), o.pinv_up.data());
   o.pinv_down.assign((size_t)ns * ns, 0);

@@ -45,6 +45,7 @@ struct Operators {
   std::vector<double> pinv_up;     // ns x ns: V S^-1 U^T of the upward e2c
   std::vector<double> pinv_down;   // ns x ns: U S^-1 V^T (its transpose)
   std::vector<double> UT, VSinv;   // factors as the reference keeps them
+  std::vector<double> U, V, sinv;  // e2c = U diag(s) V^T (row-major), sinv = pseudo-inverted s
   std::vector<double> m2m[8];      // ns x ns each
   std::vector<double> m2m_img_sum; // sum of the 27 image M2M matrices
   std::vector<double> l2l_img;     // M2M_img[13]^T

@@ -185,3 +185,18 @@ def test_generate_random_bodies_matches_oracle(pkg, oracle):
     x1, q1 = pkg.generate_random_bodies(500, math.pi, seed=5, zero_netcharge=1)
     x2, q2 = oracle.generate_random_bodies(500, math.pi, seed=5, zero_netcharge=1)
     assert np.array_equal(x1, x2) and np.array_equal(q1, q2)
+
+
+def test_p2p_pairs_cover_reference_lists(pkg, oracle):
+    """The reference's P2P lists may pair a non-leaf cell with a leaf (its
+    M2P/P2L-to-P2P conversions, traverser.cpp:75-86); the library expands
+    those into leaf pairs.  The body-pair count must be unchanged."""
+    x, q = blobs(5000, 5, 0.02, 3)
+    f = pkg.LaplaceFMM(x, q, pkg.Argument(P=4, ncrit=32, images=3, cycle=1.0))
+    f.setup()
+    F = oracle.FMM(x, q, 4, 32, 3, 1.0)
+    C = F.cells
+    nonleaf = sum(1 for t, l in F.trav.p2p.items() for (s, off) in l if C.cnum[t] or C.cnum[s])
+    assert nonleaf > 0
+    pairs = sum(C.bnum[t] * C.bnum[s] for t, l in F.trav.p2p.items() for (s, off) in l)
+    assert f.info()["p2p_pairs"] == pairs
