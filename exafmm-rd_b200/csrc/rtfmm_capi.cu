@@ -89,7 +89,9 @@ struct rtfmm_fmm {
   std::vector<int> idx_pool;
   std::vector<double> scale_pool;
   std::vector<ApplyCall> p2m_call, m2m_calls, l2l_calls, l2p_call;
-  std::vector<int> up8_items, down8_items, up27_items, down27_items;
+  std::vector<int> up8_slots, down8_slots, up27_slots, down27_slots;  // 8 child cells per parent (-1 = none)
+  std::vector<int> up8_items, down8_items, up27_items, down27_items;  // 10 ints per block
+  int sp_up8 = 8, sp_down8 = 8, sp_up27 = 8, sp_down27 = 8;
   std::vector<int> tsrc8, tsrc27;
   std::vector<double> tscale8, tscale27;
   int nS8 = 0, nT8 = 0, nS27 = 0, nT27 = 0;
@@ -403,23 +405,15 @@ void build_tables(rtfmm_fmm* f) {
   f->nT8 = (int)t8cells.size();
   f->nT27 = (int)t27cells.size();
   auto child_slot = [&](int ch) { return p.cells[ch].octant == 13 ? 0 : p.cells[ch].octant; };
-  f->up8_items.clear();
-  f->up27_items.clear();
+  f->up8_slots.assign((size_t)f->nS8 * 8, -1);
+  f->up27_slots.assign((size_t)f->nS27 * 8, -1);
   for (auto& kv : s8) {
-    int slot[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
     const Cell& cl = p.cells[kv.first];
-    for (int c = 0; c < cl.cnum; ++c) slot[child_slot(cl.coff + c)] = cl.coff + c;
-    for (int sl = 0; sl < 8; ++sl) {
-      f->up8_items.push_back(kv.second);
-      f->up8_items.push_back(sl);
-      f->up8_items.push_back(slot[sl]);
-    }
+    for (int c = 0; c < cl.cnum; ++c) f->up8_slots[(size_t)kv.second * 8 + child_slot(cl.coff + c)] = cl.coff + c;
   }
   for (auto& kv : s27) {
     const Cell& cl = p.cells[kv.first];
-    f->up27_items.push_back(kv.second);
-    f->up27_items.push_back(0);
-    f->up27_items.push_back(cl.coff);
+    f->up27_slots[(size_t)kv.second * 8] = cl.coff;
   }
   auto direction = [&](int t, const M2LEntry& e) {
     const Cell& T = p.cells[t];
@@ -434,7 +428,7 @@ void build_tables(rtfmm_fmm* f) {
                           std::vector<int>& tsrc, std::vector<double>& tscale, std::vector<int>& down) {
     tsrc.assign(tcells.size() * 26, -1);
     tscale.assign(tcells.size(), 0.0);
-    down.clear();
+    down.assign(tcells.size() * 8, -1);
     for (int ti = 0; ti < (int)tcells.size(); ++ti) {
       const int t = tcells[ti];
       for (const M2LEntry& e : p.m2l[t]) {
@@ -443,15 +437,11 @@ void build_tables(rtfmm_fmm* f) {
       }
       const Cell& T = p.cells[t];
       tscale[ti] = std::pow(T.depth >= -1 ? 2.0 : 3.0, T.depth + 1) / N3;
-      for (int c = 0; c < T.cnum; ++c) {
-        down.push_back(ti);
-        down.push_back(child_slot(T.coff + c));
-        down.push_back(T.coff + c);
-      }
+      for (int c = 0; c < T.cnum; ++c) down[(size_t)ti * 8 + child_slot(T.coff + c)] = T.coff + c;
     }
   };
-  fill_targets(t8cells, false, s8, f->tsrc8, f->tscale8, f->down8_items);
-  fill_targets(t27cells, true, s27, f->tsrc27, f->tscale27, f->down27_items);
+  fill_targets(t8cells, false, s8, f->tsrc8, f->tscale8, f->down8_slots);
+  fill_targets(t27cells, true, s27, f->tsrc27, f->tscale27, f->down27_slots);
   (void)ns;
 }
 
@@ -556,10 +546,23 @@ int upload_plan(rtfmm_fmm* f) {
   RC(dupload(f, &f->d_B[B_IMG13], b));
   RC(dupload(f, &f->d_idx_pool, f->idx_pool));
   RC(dupload(f, &f->d_scale_pool, f->scale_pool));
-  // M2L
+  // M2L: kernel spectra re-laid frequency-major, G[f][d][pair]
+  std::vector<double> g64(o.cc8.size());
+  for (int d = 0; d < 26; ++d)
+    for (int pr = 0; pr < 64; ++pr)
+      for (int fq = 0; fq < Nf; ++fq) {
+        const size_t from = (((size_t)d * 64 + pr) * Nf + fq) * 2;
+        const size_t to = (((size_t)fq * 26 + d) * 64 + pr) * 2;
+        g64[to] = o.cc8[from];
+        g64[to + 1] = o.cc8[from + 1];
+      }
+  std::vector<int> tsrcT(f->tsrc8.size());
+  for (int t = 0; t < f->nT8; ++t)
+    for (int d = 0; d < 26; ++d) tsrcT[(size_t)d * f->nT8 + t] = f->tsrc8[(size_t)t * 26 + d];
+  RC(dupload(f, &f->d_tsrc8, tsrcT));
   if (mixed) {
-    std::vector<float> g(o.cc8.size());
-    for (size_t i = 0; i < g.size(); ++i) g[i] = (float)o.cc8[i];
+    std::vector<float> g(g64.size());
+    for (size_t i = 0; i < g.size(); ++i) g[i] = (float)g64[i];
     float* gp;
     RC(dupload(f, &gp, g));
     f->d_G8 = gp;
@@ -570,7 +573,7 @@ int upload_plan(rtfmm_fmm* f) {
     f->d_Pk8 = pp;
   } else {
     double* gp;
-    RC(dupload(f, &gp, o.cc8));
+    RC(dupload(f, &gp, g64));
     f->d_G8 = gp;
     double *qp, *pp;
     RC(dalloc(f, &qp, (size_t)f->nS8 * 8 * Nf * 2));
@@ -581,11 +584,32 @@ int upload_plan(rtfmm_fmm* f) {
   RC(dupload(f, &f->d_G27, o.cc27sum));
   RC(dalloc(f, &f->d_Q27, (size_t)f->nS27 * 8 * Nf * 2));
   RC(dalloc(f, &f->d_Pk27, (size_t)f->nT27 * 8 * Nf * 2));
+  // M2L up/down blocks: groups of sp child slots (sized to shared memory)
+  f->sp_up8 = mixed ? m2l_up_slots<float>(o.P) : m2l_up_slots<double>(o.P);
+  f->sp_down8 = mixed ? m2l_down_slots<float>(o.P) : m2l_down_slots<double>(o.P);
+  f->sp_up27 = m2l_up_slots<double>(o.P);
+  f->sp_down27 = m2l_down_slots<double>(o.P);
+  auto group = [](const std::vector<int>& slots, int sp, bool keep_empty, std::vector<int>& items) {
+    items.clear();
+    const size_t np = slots.size() / 8;
+    for (size_t pidx = 0; pidx < np; ++pidx)
+      for (int g0 = 0; g0 < 8; g0 += sp) {
+        bool any = false;
+        for (int j = 0; j < sp; ++j) any |= slots[pidx * 8 + g0 + j] >= 0;
+        if (!any && !keep_empty) continue;
+        items.push_back((int)pidx);
+        items.push_back(g0);
+        for (int j = 0; j < 8; ++j) items.push_back(j < sp ? slots[pidx * 8 + g0 + j] : -1);
+      }
+  };
+  group(f->up8_slots, f->sp_up8, true, f->up8_items);
+  group(f->down8_slots, f->sp_down8, false, f->down8_items);
+  group(f->up27_slots, f->sp_up27, true, f->up27_items);
+  group(f->down27_slots, f->sp_down27, false, f->down27_items);
   RC(dupload(f, &f->d_up8, f->up8_items));
   RC(dupload(f, &f->d_down8, f->down8_items));
   RC(dupload(f, &f->d_up27, f->up27_items));
   RC(dupload(f, &f->d_down27, f->down27_items));
-  RC(dupload(f, &f->d_tsrc8, f->tsrc8));
   RC(dupload(f, &f->d_tsrc27, f->tsrc27));
   RC(dupload(f, &f->d_tscale8, f->tscale8));
   RC(dupload(f, &f->d_tscale27, f->tscale27));
@@ -644,7 +668,7 @@ int enqueue_pass(rtfmm_fmm* f) {
     }
     CK(cudaEventRecord(f->ev_near0, s1));
     if (mixed) {
-      CK(launch_p2p32(f->d_body32, f->d_leaves, f->d_items2, (int)f->items2.size(), f->d_list_off, f->d_list32,
+      CK(launch_p2p32(f->d_body32, f->d_leaves, f->d_items, (int)f->items.size(), f->d_list_off, f->d_list32,
                       f->d_near_phi, f->d_near_grad, s1));
       f->launches += 1;
     } else {
@@ -674,36 +698,38 @@ int enqueue_pass(rtfmm_fmm* f) {
       if (rc) return rc;
     }
     CK(cudaEventRecord(f->ev_st[ST_M2M], s0));
-    const int nup8 = (int)f->up8_items.size() / 3, nup27 = (int)f->up27_items.size() / 3;
-    const int ndn8 = (int)f->down8_items.size() / 3, ndn27 = (int)f->down27_items.size() / 3;
+    const int nup8 = (int)f->up8_items.size() / 10, nup27 = (int)f->up27_items.size() / 10;
+    const int ndn8 = (int)f->down8_items.size() / 10, ndn27 = (int)f->down27_items.size() / 10;
     if (mixed) {
-      CK(launch_m2l_up<float>(f->d_qeq, f->d_up8, nup8, f->d_surf_ijk, f->d_twiddle, P, ns, (float*)f->d_Q8, s0));
+      CK(launch_m2l_up<float>(f->d_qeq, f->d_up8, nup8, f->d_surf_ijk, f->d_twiddle, P, ns, f->nS8, f->sp_up8,
+                              (float*)f->d_Q8, s0));
     } else {
-      CK(launch_m2l_up<double>(f->d_qeq, f->d_up8, nup8, f->d_surf_ijk, f->d_twiddle, P, ns, (double*)f->d_Q8,
-                               s0));
+      CK(launch_m2l_up<double>(f->d_qeq, f->d_up8, nup8, f->d_surf_ijk, f->d_twiddle, P, ns, f->nS8, f->sp_up8,
+                               (double*)f->d_Q8, s0));
     }
-    CK(launch_m2l_up<double>(f->d_qeq, f->d_up27, nup27, f->d_surf_ijk, f->d_twiddle, P, ns, f->d_Q27, s0));
+    CK(launch_m2l_up<double>(f->d_qeq, f->d_up27, nup27, f->d_surf_ijk, f->d_twiddle, P, ns, f->nS27,
+                             f->sp_up27, f->d_Q27, s0));
     f->launches += (nup8 > 0) + (nup27 > 0);
     CK(cudaEventRecord(f->ev_st[ST_UP], s0));
     if (mixed) {
-      CK(launch_m2l_hadamard8<float>((const float*)f->d_Q8, (const float*)f->d_G8, f->d_tsrc8, f->nT8, Nf,
-                                     (float*)f->d_Pk8, s0));
+      CK(launch_m2l_hadamard8<float>((const float*)f->d_Q8, (const float*)f->d_G8, f->d_tsrc8, f->nT8, f->nS8,
+                                     Nf, (float*)f->d_Pk8, s0));
     } else {
-      CK(launch_m2l_hadamard8<double>((const double*)f->d_Q8, (const double*)f->d_G8, f->d_tsrc8, f->nT8, Nf,
-                                      (double*)f->d_Pk8, s0));
+      CK(launch_m2l_hadamard8<double>((const double*)f->d_Q8, (const double*)f->d_G8, f->d_tsrc8, f->nT8,
+                                      f->nS8, Nf, (double*)f->d_Pk8, s0));
     }
-    CK(launch_m2l_hadamard27(f->d_Q27, f->d_G27, f->d_tsrc27, f->nT27, Nf, f->d_Pk27, s0));
+    CK(launch_m2l_hadamard27(f->d_Q27, f->d_G27, f->d_tsrc27, f->nT27, f->nS27, Nf, f->d_Pk27, s0));
     f->launches += (f->nT8 > 0) + (f->nT27 > 0);
     CK(cudaEventRecord(f->ev_st[ST_HAD], s0));
     if (mixed) {
       CK(launch_m2l_down<float>((const float*)f->d_Pk8, f->d_down8, f->d_tscale8, ndn8, f->d_surf_ijk,
-                                f->d_twiddle, P, ns, f->d_pchk, s0));
+                                f->d_twiddle, P, ns, f->nT8, f->sp_down8, f->d_pchk, s0));
     } else {
       CK(launch_m2l_down<double>((const double*)f->d_Pk8, f->d_down8, f->d_tscale8, ndn8, f->d_surf_ijk,
-                                 f->d_twiddle, P, ns, f->d_pchk, s0));
+                                 f->d_twiddle, P, ns, f->nT8, f->sp_down8, f->d_pchk, s0));
     }
     CK(launch_m2l_down<double>(f->d_Pk27, f->d_down27, f->d_tscale27, ndn27, f->d_surf_ijk, f->d_twiddle, P, ns,
-                               f->d_pchk, s0));
+                               f->nT27, f->sp_down27, f->d_pchk, s0));
     f->launches += (ndn8 > 0) + (ndn27 > 0);
     CK(cudaEventRecord(f->ev_st[ST_DOWN], s0));
     for (auto& c : f->l2l_calls) {

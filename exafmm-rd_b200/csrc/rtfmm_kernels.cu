@@ -25,6 +25,20 @@ namespace rtfmm_b200 {
 template <typename T> struct Cplx;
 template <> struct Cplx<float> { using type = float2; };
 template <> struct Cplx<double> { using type = double2; };
+// two complex values in one vector load
+template <typename T> struct Cplx2;
+template <> struct Cplx2<float> { using type = float4; };
+template <> struct Cplx2<double> { using type = double4; };
+
+// 32-byte (one sector) vector loads, sm_100: one lane reads a whole sector.
+__device__ __forceinline__ void ld_sector(const float* p, float (&v)[8]) {
+  asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
+               : "l"(p));
+}
+__device__ __forceinline__ void ld_sector(const double* p, double (&v)[4]) {
+  asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3]) : "l"(p));
+}
 
 __device__ __forceinline__ float rsqrt_approx(float x) {
   float y;
@@ -61,98 +75,67 @@ __global__ void k_prep32(const double4* __restrict__ body64, const int* __restri
 // ---------------------------------------------------------------------------
 constexpr int kP2PWarps = 4;
 
-// Each source is staged twice-duplicated and pre-negated, so that one
-// packed f32x2 operation serves a lane's two targets:
-//   s[2k]   = (-x, -x, -y, -y),  s[2k+1] = (-z, -z, q, q)
 template <bool MASK>
-__device__ __forceinline__ void p2p32_tile(const float4* __restrict__ s, int cnt, float2 px, float2 py,
-                                           float2 pz, float2& p, float2& fx, float2& fy, float2& fz) {
-#pragma unroll 4
+__device__ __forceinline__ void p2p32_tile(const float4* __restrict__ s, int cnt, float px, float py,
+                                           float pz, float& p, float& fx, float& fy, float& fz) {
+#pragma unroll 8
   for (int k = 0; k < cnt; ++k) {
-    const float4 u = s[2 * k], v = s[2 * k + 1];
-    const float2 dx = __fadd2_rn(px, make_float2(u.x, u.y));
-    const float2 dy = __fadd2_rn(py, make_float2(u.z, u.w));
-    const float2 dz = __fadd2_rn(pz, make_float2(v.x, v.y));
-    float2 r2 = __fmul2_rn(dz, dz);
-    r2 = __ffma2_rn(dy, dy, r2);
-    r2 = __ffma2_rn(dx, dx, r2);
-    float2 ir = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
-    if (MASK) {
-      ir.x = r2.x > 0.f ? ir.x : 0.f;
-      ir.y = r2.y > 0.f ? ir.y : 0.f;
-    }
-    const float2 qir = __fmul2_rn(make_float2(v.z, v.w), ir);
-    p = __fadd2_rn(p, qir);
-    const float2 q3 = __fmul2_rn(__fmul2_rn(qir, ir), ir);
-    fx = __ffma2_rn(q3, dx, fx);
-    fy = __ffma2_rn(q3, dy, fy);
-    fz = __ffma2_rn(q3, dz, fz);
+    const float4 b = s[k];
+    const float dx = px - b.x, dy = py - b.y, dz = pz - b.z;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    float ir = rsqrt_approx(r2);
+    if (MASK) ir = r2 > 0.f ? ir : 0.f;
+    const float qir = b.w * ir;
+    p += qir;
+    const float q3 = qir * ir * ir;
+    fx = fmaf(q3, dx, fx);
+    fy = fmaf(q3, dy, fy);
+    fz = fmaf(q3, dz, fz);
   }
 }
 
-// One warp per (target leaf, 64 targets): lane l owns targets t0+l and
-// t0+32+l and evaluates both with packed f32x2 arithmetic.
+// One warp per (target leaf, 32 targets), one target per lane.
 __global__ void __launch_bounds__(32 * kP2PWarps)
     k_p2p32(const float4* __restrict__ body32, const LeafInfo* __restrict__ leaves,
             const P2PItem* __restrict__ items, int nitems, const int* __restrict__ list_off,
             const P2PSrc32* __restrict__ list, double* __restrict__ phi, double* __restrict__ grad) {
-  __shared__ float4 sbuf[kP2PWarps][64];
+  __shared__ float4 sbuf[kP2PWarps][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int item = blockIdx.x * kP2PWarps + warp;
   if (item >= nitems) return;  // warp-uniform
   const P2PItem it = items[item];
   const LeafInfo T = leaves[it.leaf];
-  const int ta = it.t0 + lane, tb = it.t0 + 32 + lane;
-  const bool va = ta < T.bnum, vb = tb < T.bnum;
-  const float4 xa = va ? body32[T.boff + ta] : make_float4(0.f, 0.f, 0.f, 0.f);
-  const float4 xb = vb ? body32[T.boff + tb] : make_float4(0.f, 0.f, 0.f, 0.f);
-  double Pa = 0.0, Gxa = 0.0, Gya = 0.0, Gza = 0.0;
-  double Pb = 0.0, Gxb = 0.0, Gyb = 0.0, Gzb = 0.0;
+  const int t = it.t0 + lane;
+  const bool active = t < T.bnum;
+  const float4 xt = active ? body32[T.boff + t] : make_float4(0.f, 0.f, 0.f, 0.f);
+  double P = 0.0, Gx = 0.0, Gy = 0.0, Gz = 0.0;
   const int e1 = list_off[it.leaf + 1];
-  float4* sw = sbuf[warp];
   for (int e = list_off[it.leaf]; e < e1; ++e) {
     const P2PSrc32 src = list[e];
     const LeafInfo S = leaves[src.leaf];
-    const float2 px = make_float2(xa.x - src.dx, xb.x - src.dx);
-    const float2 py = make_float2(xa.y - src.dy, xb.y - src.dy);
-    const float2 pz = make_float2(xa.z - src.dz, xb.z - src.dz);
-    float2 p = make_float2(0.f, 0.f), fx = p, fy = p, fz = p;
+    const float px = xt.x - src.dx, py = xt.y - src.dy, pz = xt.z - src.dz;
+    float p = 0.f, fx = 0.f, fy = 0.f, fz = 0.f;
     for (int c0 = 0; c0 < S.bnum; c0 += 32) {
       const int cnt = min(32, S.bnum - c0);
       __syncwarp();
-      if (lane < cnt) {
-        const float4 b = body32[S.boff + c0 + lane];
-        sw[2 * lane] = make_float4(-b.x, -b.x, -b.y, -b.y);
-        sw[2 * lane + 1] = make_float4(-b.z, -b.z, b.w, b.w);
-      }
+      if (lane < cnt) sbuf[warp][lane] = body32[S.boff + c0 + lane];
       __syncwarp();
       if (src.self)
-        p2p32_tile<true>(sw, cnt, px, py, pz, p, fx, fy, fz);
+        p2p32_tile<true>(sbuf[warp], cnt, px, py, pz, p, fx, fy, fz);
       else
-        p2p32_tile<false>(sw, cnt, px, py, pz, p, fx, fy, fz);
+        p2p32_tile<false>(sbuf[warp], cnt, px, py, pz, p, fx, fy, fz);
     }
-    Pa += (double)p.x;
-    Gxa += (double)fx.x;
-    Gya += (double)fy.x;
-    Gza += (double)fz.x;
-    Pb += (double)p.y;
-    Gxb += (double)fx.y;
-    Gyb += (double)fy.y;
-    Gzb += (double)fz.y;
+    P += (double)p;
+    Gx += (double)fx;
+    Gy += (double)fy;
+    Gz += (double)fz;
   }
-  if (va) {
-    const int b = T.boff + ta;
-    phi[b] = Pa;
-    grad[3 * b + 0] = -Gxa;
-    grad[3 * b + 1] = -Gya;
-    grad[3 * b + 2] = -Gza;
-  }
-  if (vb) {
-    const int b = T.boff + tb;
-    phi[b] = Pb;
-    grad[3 * b + 0] = -Gxb;
-    grad[3 * b + 1] = -Gyb;
-    grad[3 * b + 2] = -Gzb;
+  if (active) {
+    const int b = T.boff + t;
+    phi[b] = P;
+    grad[3 * b + 0] = -Gx;
+    grad[3 * b + 1] = -Gy;
+    grad[3 * b + 2] = -Gz;
   }
 }
 
@@ -393,182 +376,197 @@ __device__ __forceinline__ void cmad(T& re, T& im, T ar, T ai, T br, T bi) {
   im = fma(ai, br, im);
 }
 
-// up: one block per (source parent, child slot): scatter the child's
-// equivalent density onto the [0,P)^3 corner of the grid
+// up: one block per (source parent, group of sp child slots): scatter each
+// child's equivalent density onto the [0,P)^3 corner of the grid
 // (surf_conv_idx_map_up, kernel.cpp:1246-1252, 1304-1315) and take its
-// forward DFT separably (x, then y, then z), writing Q[src][slot][f].
-template <typename T>
+// forward DFT separably (x, then y, then z).  The z pass of all sp slots runs
+// together so that each frequency's sp values are written contiguously into
+// the frequency-major spectrum Q[f][src][slot].
+// items: 10 ints per block = src, first slot, child cell per slot (-1 = none).
+// PP > 0 fixes P at compile time (cheap index arithmetic); PP = 0 takes it
+// from the argument.
+template <typename T, int PP>
 __global__ void __launch_bounds__(256)
     k_m2l_up(const double* __restrict__ q_equiv, const int* __restrict__ items,
-             const int* __restrict__ surf_ijk, const double* __restrict__ twiddle, int P, int ns,
-             T* __restrict__ Q) {
+             const int* __restrict__ surf_ijk, const double* __restrict__ twiddle, int P_, int ns, int nsrc,
+             int sp, T* __restrict__ Q) {
+  const int P = PP > 0 ? PP : P_;
   extern __shared__ unsigned char smem_raw[];
   T* sm = reinterpret_cast<T*>(smem_raw);
   const int N = 2 * P - 1;
-  const int P3 = P * P * P, Nf = N * N * P;
-  T* cube = sm;                    // P^3
+  const int P3 = P * P * P, Nf = N * N * P, PNP = P * N * P;
+  T* W = sm;                       // N*N complex: W[k][n] = w^(k n mod N)
+  T* cube = W + 2 * N * N;         // P^3
   T* A = cube + P3;                // P^3 complex: [z][y][kx]
-  T* Bm = A + 2 * P3;              // P*N*P complex: [z][ky][kx]
-  T* W = Bm + 2 * P * N * P;       // N*N complex: W[k][n] = w^(k n mod N)
-  const int src = items[3 * blockIdx.x], slot = items[3 * blockIdx.x + 1], child = items[3 * blockIdx.x + 2];
-  T* out = Q + ((size_t)src * 8 + slot) * Nf * 2;
+  T* Bm = A + 2 * P3;              // sp * P*N*P complex: [slot][z][ky][kx]
+  const int* it = items + 10 * blockIdx.x;
+  const int src = it[0], slot0 = it[1];
   const int tid = threadIdx.x, nt = blockDim.x;
-  if (child < 0) {
-    for (int f = tid; f < 2 * Nf; f += nt) out[f] = T(0);
-    return;
-  }
   for (int e = tid; e < N * N; e += nt) {
     const int m = ((e / N) * (e % N)) % N;
     W[2 * e] = (T)twiddle[2 * m];
     W[2 * e + 1] = (T)twiddle[2 * m + 1];
   }
-  for (int e = tid; e < P3; e += nt) cube[e] = T(0);
-  __syncthreads();
-  for (int i = tid; i < ns; i += nt) {
-    const int x = surf_ijk[3 * i], y = surf_ijk[3 * i + 1], z = surf_ijk[3 * i + 2];
-    cube[(z * P + y) * P + x] = (T)q_equiv[(size_t)child * ns + i];
-  }
-  __syncthreads();
-  for (int e = tid; e < P3; e += nt) {
-    const int z = e / (P * P), y = (e / P) % P, kx = e % P;
-    T re = 0, im = 0;
-    const T* row = cube + (z * P + y) * P;
-    const T* wk = W + 2 * kx * N;
-    for (int x = 0; x < P; ++x) {
-      re = fma(row[x], wk[2 * x], re);
-      im = fma(row[x], wk[2 * x + 1], im);
+  for (int j = 0; j < sp; ++j) {
+    const int child = it[2 + j];
+    T* Bj = Bm + 2 * (size_t)j * PNP;
+    if (child < 0) {
+      for (int e = tid; e < 2 * PNP; e += nt) Bj[e] = T(0);
+      continue;
     }
-    A[2 * e] = re;
-    A[2 * e + 1] = im;
-  }
-  __syncthreads();
-  for (int e = tid; e < P * N * P; e += nt) {
-    const int z = e / (N * P), ky = (e / P) % N, kx = e % P;
-    T re = 0, im = 0;
-    const T* wk = W + 2 * ky * N;
-    for (int y = 0; y < P; ++y) {
-      const int a = (z * P + y) * P + kx;
-      cmad(re, im, A[2 * a], A[2 * a + 1], wk[2 * y], wk[2 * y + 1]);
+    for (int e = tid; e < P3; e += nt) cube[e] = T(0);
+    __syncthreads();
+    for (int i = tid; i < ns; i += nt) {
+      const int x = surf_ijk[3 * i], y = surf_ijk[3 * i + 1], z = surf_ijk[3 * i + 2];
+      cube[(z * P + y) * P + x] = (T)q_equiv[(size_t)child * ns + i];
     }
-    Bm[2 * e] = re;
-    Bm[2 * e + 1] = im;
+    __syncthreads();
+    for (int e = tid; e < P3; e += nt) {
+      const int z = e / (P * P), y = (e / P) % P, kx = e % P;
+      T re = 0, im = 0;
+      const T* row = cube + (z * P + y) * P;
+      const T* wk = W + 2 * kx * N;
+      for (int x = 0; x < P; ++x) {
+        re = fma(row[x], wk[2 * x], re);
+        im = fma(row[x], wk[2 * x + 1], im);
+      }
+      A[2 * e] = re;
+      A[2 * e + 1] = im;
+    }
+    __syncthreads();
+    for (int e = tid; e < PNP; e += nt) {
+      const int z = e / (N * P), ky = (e / P) % N, kx = e % P;
+      T re = 0, im = 0;
+      const T* wk = W + 2 * ky * N;
+      for (int y = 0; y < P; ++y) {
+        const int a = (z * P + y) * P + kx;
+        cmad(re, im, A[2 * a], A[2 * a + 1], wk[2 * y], wk[2 * y + 1]);
+      }
+      Bj[2 * e] = re;
+      Bj[2 * e + 1] = im;
+    }
+    __syncthreads();
   }
   __syncthreads();
+  using V2 = typename Cplx2<T>::type;  // two complex values
   for (int f = tid; f < Nf; f += nt) {
     const int kz = f / (N * P), ky = (f / P) % N, kx = f % P;
-    T re = 0, im = 0;
     const T* wk = W + 2 * kz * N;
-    for (int z = 0; z < P; ++z) {
-      const int b = (z * N + ky) * P + kx;
-      cmad(re, im, Bm[2 * b], Bm[2 * b + 1], wk[2 * z], wk[2 * z + 1]);
+    T* out = Q + (((size_t)f * nsrc + src) * 8 + slot0) * 2;
+    for (int j = 0; j < sp; j += 2) {
+      T re0 = 0, im0 = 0, re1 = 0, im1 = 0;
+      const T* B0 = Bm + 2 * (size_t)j * PNP;
+      const T* B1 = B0 + 2 * (size_t)PNP;
+      for (int z = 0; z < P; ++z) {
+        const int b = (z * N + ky) * P + kx;
+        cmad(re0, im0, B0[2 * b], B0[2 * b + 1], wk[2 * z], wk[2 * z + 1]);
+        if (j + 1 < sp) cmad(re1, im1, B1[2 * b], B1[2 * b + 1], wk[2 * z], wk[2 * z + 1]);
+      }
+      if (j + 1 < sp) {
+        V2 v;
+        v.x = re0;
+        v.y = im0;
+        v.z = re1;
+        v.w = im1;
+        *reinterpret_cast<V2*>(out + 2 * j) = v;
+      } else {
+        out[2 * j] = re0;
+        out[2 * j + 1] = im0;
+      }
     }
-    out[2 * f] = re;
-    out[2 * f + 1] = im;
   }
 }
 
 // Hadamard 8x8 (hadamard_8x8 + c2c_8x8x2_avx, kernel.cpp:1012-1082, c2c.h:201-296):
-//   Pk[t][itar][f] = sum_d sum_isrc G[d][isrc][itar][f] * Q[src(t,d)][isrc][f]
-// Block = 32 frequencies x 8 warps; each warp owns 2 targets.  For each of
-// the 26 directions the block stages G_d for its 32 frequencies in shared
-// memory.  FP32 partial sums per direction are accumulated into FP64.
-constexpr int kHadWarps = 8, kHadTPW = 2, kHadTargets = kHadWarps * kHadTPW;
+//   Pk[f][t][itar] = sum_d sum_isrc G[f][d][isrc][itar] * Q[f][src(t,d)][isrc]
+// One thread per (target, frequency); a block holds one frequency's 26x64
+// kernel coefficients in shared memory, so every coefficient read is a
+// broadcast, and each (target, direction) reads one 64-byte source row.
+// FP32 partial sums per direction are accumulated into FP64.
+constexpr int kHadThreads = 256;
 
 template <typename T>
-__global__ void __launch_bounds__(32 * kHadWarps)
-    k_m2l_hadamard8(const T* __restrict__ Q, const T* __restrict__ G, const int* __restrict__ tsrc,
-                    int ntar, int Nf, T* __restrict__ Pk) {
+__global__ void __launch_bounds__(kHadThreads, sizeof(T) == 4 ? 2 : 1)
+    k_m2l_hadamard8(const T* __restrict__ Q, const T* __restrict__ G, const int* __restrict__ tsrcT, int ntar,
+                    int nsrc, int Nf, T* __restrict__ Pk) {
   using C2 = typename Cplx<T>::type;
-  __shared__ C2 Gs[64][32];
-  const int lane = threadIdx.x, warp = threadIdx.y;
-  const int tid = warp * 32 + lane;
-  const int f0 = blockIdx.y * 32;
-  const int f = f0 + lane;
-  int tt[kHadTPW];
-  bool tv[kHadTPW];
+  __shared__ __align__(32) C2 Gs[26 * 64];
+  const int f = blockIdx.y;
+  const C2* Gf = reinterpret_cast<const C2*>(G) + (size_t)f * 26 * 64;
+  for (int e = threadIdx.x; e < 26 * 64; e += kHadThreads) Gs[e] = Gf[e];
+  __syncthreads();
+  const int t = blockIdx.x * kHadThreads + threadIdx.x;
+  if (t >= ntar) return;
+  double ar[8], ai[8];
 #pragma unroll
-  for (int j = 0; j < kHadTPW; ++j) {
-    tt[j] = blockIdx.x * kHadTargets + warp * kHadTPW + j;
-    tv[j] = tt[j] < ntar;
-  }
-  double acc[kHadTPW][8][2];
+  for (int i = 0; i < 8; ++i) ar[i] = ai[i] = 0.0;
+  const C2* Qf = reinterpret_cast<const C2*>(Q) + (size_t)f * nsrc * 8;
+  constexpr int kPer = 32 / sizeof(T);  // values per 32-byte sector
+  // directions in pairs: both source rows are in flight together, and one
+  // FP64 accumulation follows the two FP32 partial sums
+  for (int d0 = 0; d0 < 26; d0 += 2) {
+    int sd[2];
+    sd[0] = tsrcT[d0 * ntar + t];
+    sd[1] = tsrcT[(d0 + 1) * ntar + t];
+    if (sd[0] < 0 && sd[1] < 0) continue;
+    C2 q[2][8];
 #pragma unroll
-  for (int j = 0; j < kHadTPW; ++j)
+    for (int h = 0; h < 2; ++h) {
+      if (sd[h] < 0) {
 #pragma unroll
-    for (int i = 0; i < 8; ++i) acc[j][i][0] = acc[j][i][1] = 0.0;
-  const C2* G2 = reinterpret_cast<const C2*>(G);
-  const C2* Q2 = reinterpret_cast<const C2*>(Q);
-  for (int d = 0; d < 26; ++d) {
-    int s[kHadTPW];
-    int any = 0;
+        for (int i = 0; i < 8; ++i) q[h][i].x = q[h][i].y = T(0);
+        continue;
+      }
+      const T* qrow = reinterpret_cast<const T*>(Qf + (size_t)sd[h] * 8);
 #pragma unroll
-    for (int j = 0; j < kHadTPW; ++j) {
-      s[j] = tv[j] ? tsrc[tt[j] * 26 + d] : -1;
-      any |= (s[j] >= 0);
-    }
-    if (!__syncthreads_or(any)) continue;
-    for (int e = tid; e < 64 * 32; e += 32 * kHadWarps) {
-      const int pair = e >> 5, fl = e & 31;
-      const int ff = f0 + fl;
-      C2 v;
-      v.x = T(0);
-      v.y = T(0);
-      if (ff < Nf) v = G2[((size_t)d * 64 + pair) * Nf + ff];
-      Gs[pair][fl] = v;
-    }
-    __syncthreads();
-    if (any && f < Nf) {
-      T pr[kHadTPW][8], pi[kHadTPW][8];
+      for (int c = 0; c < 16 / kPer; ++c) {
+        T v[kPer];
+        ld_sector(qrow + c * kPer, v);
 #pragma unroll
-      for (int j = 0; j < kHadTPW; ++j)
-#pragma unroll
-        for (int i = 0; i < 8; ++i) pr[j][i] = pi[j][i] = T(0);
-#pragma unroll
-      for (int isrc = 0; isrc < 8; ++isrc) {
-        C2 q[kHadTPW];
-#pragma unroll
-        for (int j = 0; j < kHadTPW; ++j) {
-          q[j].x = T(0);
-          q[j].y = T(0);
-          if (s[j] >= 0) q[j] = Q2[((size_t)s[j] * 8 + isrc) * Nf + f];
-        }
-#pragma unroll
-        for (int itar = 0; itar < 8; ++itar) {
-          const C2 gv = Gs[isrc * 8 + itar][lane];
-#pragma unroll
-          for (int j = 0; j < kHadTPW; ++j) cmad(pr[j][itar], pi[j][itar], gv.x, gv.y, q[j].x, q[j].y);
+        for (int k = 0; k < kPer / 2; ++k) {
+          q[h][c * kPer / 2 + k].x = v[2 * k];
+          q[h][c * kPer / 2 + k].y = v[2 * k + 1];
         }
       }
+    }
+    T pr[8], pi[8];
 #pragma unroll
-      for (int j = 0; j < kHadTPW; ++j)
+    for (int i = 0; i < 8; ++i) pr[i] = pi[i] = T(0);
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          acc[j][i][0] += (double)pr[j][i];
-          acc[j][i][1] += (double)pi[j][i];
+    for (int h = 0; h < 2; ++h) {
+      if (sd[h] < 0) continue;
+      const C2* g = Gs + (d0 + h) * 64;
+#pragma unroll
+      for (int isrc = 0; isrc < 8; ++isrc)
+#pragma unroll
+        for (int itar = 0; itar < 8; itar += 2) {
+          const typename Cplx2<T>::type gv =
+              *reinterpret_cast<const typename Cplx2<T>::type*>(g + isrc * 8 + itar);
+          cmad(pr[itar], pi[itar], gv.x, gv.y, q[h][isrc].x, q[h][isrc].y);
+          cmad(pr[itar + 1], pi[itar + 1], gv.z, gv.w, q[h][isrc].x, q[h][isrc].y);
         }
     }
-    __syncthreads();
-  }
-  if (f < Nf) {
-    C2* P2 = reinterpret_cast<C2*>(Pk);
 #pragma unroll
-    for (int j = 0; j < kHadTPW; ++j) {
-      if (!tv[j]) continue;
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        C2 v;
-        v.x = (T)acc[j][i][0];
-        v.y = (T)acc[j][i][1];
-        P2[((size_t)tt[j] * 8 + i) * Nf + f] = v;
-      }
+    for (int i = 0; i < 8; ++i) {
+      ar[i] += (double)pr[i];
+      ai[i] += (double)pi[i];
     }
+  }
+  C2* out = reinterpret_cast<C2*>(Pk) + ((size_t)f * ntar + t) * 8;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    C2 v;
+    v.x = (T)ar[i];
+    v.y = (T)ai[i];
+    out[i] = v;
   }
 }
 
 // Hadamard 1x27 (hadamard_1x27 + c2c_1x27x1_AVX, kernel.cpp:1084-1138) for the
 // image levels, FP64; the 27 image spectra of a direction are pre-summed.
 __global__ void k_m2l_hadamard27(const double* __restrict__ Q, const double* __restrict__ G27,
-                                 const int* __restrict__ tsrc, int ntar, int Nf, double* __restrict__ Pk) {
+                                 const int* __restrict__ tsrc, int ntar, int nsrc, int Nf,
+                                 double* __restrict__ Pk) {
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   const int t = blockIdx.y;
   if (f >= Nf || t >= ntar) return;
@@ -577,33 +575,37 @@ __global__ void k_m2l_hadamard27(const double* __restrict__ Q, const double* __r
     const int s = tsrc[t * 26 + d];
     if (s < 0) continue;
     const double gr = G27[((size_t)d * Nf + f) * 2], gi = G27[((size_t)d * Nf + f) * 2 + 1];
-    const size_t qo = (((size_t)s * 8 + 0) * Nf + f) * 2;
+    const size_t qo = (((size_t)f * nsrc + s) * 8 + 0) * 2;
     cmad(re, im, gr, gi, Q[qo], Q[qo + 1]);
   }
-  const size_t po = (((size_t)t * 8 + 0) * Nf + f) * 2;
+  const size_t po = (((size_t)f * ntar + t) * 8 + 0) * 2;
   Pk[po] = re;
   Pk[po + 1] = im;
 }
 
-// down: one block per (target parent, child): inverse DFT of Pk[t][slot]
-// evaluated only at the child's check-surface points, which sit at
-// [P-1, 2P-2]^3 of the grid (surf_conv_idx_map_down, kernel.cpp:1253-1259);
-// then p_check[child] += value * scale / N^3 (kernel.cpp:1369-1382).
-template <typename T>
+// down: one block per (target parent, group of sp child slots): read the sp
+// spectra of each frequency as one contiguous run of the frequency-major
+// Pk[f][tar][slot], then for each child the inverse DFT evaluated only at its
+// check-surface points, which sit at [P-1, 2P-2]^3 of the grid
+// (surf_conv_idx_map_down, kernel.cpp:1253-1259), and
+// p_check[child] += value * scale / N^3 (kernel.cpp:1369-1382).
+// items: 10 ints per block = tar, first slot, child cell per slot (-1 = none).
+template <typename T, int PP>
 __global__ void __launch_bounds__(256)
     k_m2l_down(const T* __restrict__ Pk, const int* __restrict__ items, const double* __restrict__ tscale,
-               const int* __restrict__ surf_ijk, const double* __restrict__ twiddle, int P, int ns,
-               double* __restrict__ p_check) {
+               const int* __restrict__ surf_ijk, const double* __restrict__ twiddle, int P_, int ns, int ntar,
+               int sp, double* __restrict__ p_check) {
+  const int P = PP > 0 ? PP : P_;
   extern __shared__ unsigned char smem_raw[];
   T* sm = reinterpret_cast<T*>(smem_raw);
   const int N = 2 * P - 1;
   const int P3 = P * P * P, Nf = N * N * P;
-  T* X = sm;                        // Nf complex
-  T* Y1 = X + 2 * Nf;               // P*N*P complex: [zo][ky][kx]
+  T* W = sm;                        // P*N complex: W[o][k] = conj(w)^(k (P-1+o) mod N)
+  T* Y1 = W + 2 * P * N;            // P*N*P complex: [zo][ky][kx]
   T* Y2 = Y1 + 2 * P * N * P;       // P^3 complex: [zo][yo][kx]
-  T* W = Y2 + 2 * P3;               // P*N complex: W[o][k] = conj(w)^(k (P-1+o) mod N)
-  const int tar = items[3 * blockIdx.x], slot = items[3 * blockIdx.x + 1], child = items[3 * blockIdx.x + 2];
-  const T* in = Pk + ((size_t)tar * 8 + slot) * Nf * 2;
+  T* X = Y2 + 2 * P3;               // sp * Nf complex: [slot][f]
+  const int* it = items + 10 * blockIdx.x;
+  const int tar = it[0], slot0 = it[1];
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int e = tid; e < P * N; e += nt) {
     const int o = e / N, k = e % N;
@@ -611,45 +613,68 @@ __global__ void __launch_bounds__(256)
     W[2 * e] = (T)twiddle[2 * m];
     W[2 * e + 1] = -(T)twiddle[2 * m + 1];
   }
-  for (int e = tid; e < 2 * Nf; e += nt) X[e] = in[e];
-  __syncthreads();
-  for (int e = tid; e < P * N * P; e += nt) {
-    const int zo = e / (N * P), ky = (e / P) % N, kx = e % P;
-    const T* wo = W + 2 * zo * N;
-    T re = 0, im = 0;
-    for (int kz = 0; kz < N; ++kz) {
-      const int a = (kz * N + ky) * P + kx;
-      cmad(re, im, X[2 * a], X[2 * a + 1], wo[2 * kz], wo[2 * kz + 1]);
+  if (sp >= 2) {
+    using V2 = typename Cplx2<T>::type;
+    const int hp = sp / 2;
+    for (int e = tid; e < Nf * hp; e += nt) {
+      const int f = e / hp, j = 2 * (e % hp);
+      const V2 v = *reinterpret_cast<const V2*>(Pk + (((size_t)f * ntar + tar) * 8 + slot0 + j) * 2);
+      X[2 * ((size_t)j * Nf + f)] = v.x;
+      X[2 * ((size_t)j * Nf + f) + 1] = v.y;
+      X[2 * ((size_t)(j + 1) * Nf + f)] = v.z;
+      X[2 * ((size_t)(j + 1) * Nf + f) + 1] = v.w;
     }
-    Y1[2 * e] = re;
-    Y1[2 * e + 1] = im;
-  }
-  __syncthreads();
-  for (int e = tid; e < P3; e += nt) {
-    const int zo = e / (P * P), yo = (e / P) % P, kx = e % P;
-    const T* wo = W + 2 * yo * N;
-    T re = 0, im = 0;
-    for (int ky = 0; ky < N; ++ky) {
-      const int a = (zo * N + ky) * P + kx;
-      cmad(re, im, Y1[2 * a], Y1[2 * a + 1], wo[2 * ky], wo[2 * ky + 1]);
+  } else {
+    for (int f = tid; f < Nf; f += nt) {
+      const T* in = Pk + (((size_t)f * ntar + tar) * 8 + slot0) * 2;
+      X[2 * f] = in[0];
+      X[2 * f + 1] = in[1];
     }
-    Y2[2 * e] = re;
-    Y2[2 * e + 1] = im;
   }
   __syncthreads();
   const double sc = tscale[tar];
-  for (int i = tid; i < ns; i += nt) {
-    const int xo = surf_ijk[3 * i], yo = surf_ijk[3 * i + 1], zo = surf_ijk[3 * i + 2];
-    const T* row = Y2 + 2 * ((zo * P + yo) * P);
-    const T* wo = W + 2 * xo * N;
-    T acc = 0;
-    // Re(Y * conj(w)^m) summed over kx >= 1, doubled for the missing half
-    for (int kx = 1; kx < P; ++kx) {
-      acc = fma(row[2 * kx], wo[2 * kx], acc);
-      acc = fma(-row[2 * kx + 1], wo[2 * kx + 1], acc);
+  for (int j = 0; j < sp; ++j) {
+    const int child = it[2 + j];
+    if (child < 0) continue;  // block-uniform
+    for (int e = tid; e < P * N * P; e += nt) {
+      const int zo = e / (N * P), ky = (e / P) % N, kx = e % P;
+      const T* wo = W + 2 * zo * N;
+      T re = 0, im = 0;
+      const T* Xj = X + 2 * (size_t)j * Nf;
+      for (int kz = 0; kz < N; ++kz) {
+        const int a = (kz * N + ky) * P + kx;
+        cmad(re, im, Xj[2 * a], Xj[2 * a + 1], wo[2 * kz], wo[2 * kz + 1]);
+      }
+      Y1[2 * e] = re;
+      Y1[2 * e + 1] = im;
     }
-    const T v = row[0] + T(2) * acc;
-    p_check[(size_t)child * ns + i] += (double)v * sc;
+    __syncthreads();
+    for (int e = tid; e < P3; e += nt) {
+      const int zo = e / (P * P), yo = (e / P) % P, kx = e % P;
+      const T* wo = W + 2 * yo * N;
+      T re = 0, im = 0;
+      for (int ky = 0; ky < N; ++ky) {
+        const int a = (zo * N + ky) * P + kx;
+        cmad(re, im, Y1[2 * a], Y1[2 * a + 1], wo[2 * ky], wo[2 * ky + 1]);
+      }
+      Y2[2 * e] = re;
+      Y2[2 * e + 1] = im;
+    }
+    __syncthreads();
+    for (int i = tid; i < ns; i += nt) {
+      const int xo = surf_ijk[3 * i], yo = surf_ijk[3 * i + 1], zo = surf_ijk[3 * i + 2];
+      const T* row = Y2 + 2 * ((zo * P + yo) * P);
+      const T* wo = W + 2 * xo * N;
+      T acc = 0;
+      // Re(Y * conj(w)^m) summed over kx >= 1, doubled for the missing half
+      for (int kx = 1; kx < P; ++kx) {
+        acc = fma(row[2 * kx], wo[2 * kx], acc);
+        acc = fma(-row[2 * kx + 1], wo[2 * kx + 1], acc);
+      }
+      const T v = row[0] + T(2) * acc;
+      p_check[(size_t)child * ns + i] += (double)v * sc;
+    }
+    __syncthreads();
   }
 }
 
@@ -794,58 +819,103 @@ cudaError_t launch_sum_children(const int* list, int nparents, const double* Y, 
 }
 
 template <typename T>
-static size_t up_smem(int P) {
+static size_t up_smem(int P, int sp) {
   const int N = 2 * P - 1;
-  return sizeof(T) * ((size_t)3 * P * P * P + 2 * (size_t)P * N * P + 2 * (size_t)N * N);
+  return sizeof(T) * ((size_t)2 * N * N + 3 * (size_t)P * P * P + 2 * (size_t)sp * P * N * P);
 }
 template <typename T>
-static size_t down_smem(int P) {
+static size_t down_smem(int P, int sp) {
   const int N = 2 * P - 1;
-  return sizeof(T) * (2 * (size_t)N * N * P + 2 * (size_t)P * N * P + 2 * (size_t)P * P * P + 2 * (size_t)P * N);
+  return sizeof(T) * (2 * (size_t)P * N + 2 * (size_t)P * N * P + 2 * (size_t)P * P * P +
+                      2 * (size_t)sp * N * N * P);
+}
+
+// Largest slot group (8, 4, 2, 1) whose working set fits in shared memory.
+static const size_t kSmemMax = 220 * 1024;
+// Capped at one 32-byte sector of spectrum per frequency (4 FP32 or 2 FP64
+// complex values), which keeps enough blocks in flight.
+template <typename T>
+int m2l_up_slots(int P) {
+  for (int sp = (int)(32 / (2 * sizeof(T))); sp > 1; sp /= 2)
+    if (up_smem<T>(P, sp) <= kSmemMax) return sp;
+  return 1;
+}
+template <typename T>
+int m2l_down_slots(int P) {
+  for (int sp = (int)(32 / (2 * sizeof(T))); sp > 1; sp /= 2)
+    if (down_smem<T>(P, sp) <= kSmemMax) return sp;
+  return 1;
+}
+template int m2l_up_slots<float>(int);
+template int m2l_up_slots<double>(int);
+template int m2l_down_slots<float>(int);
+template int m2l_down_slots<double>(int);
+
+template <typename T, int PP>
+static cudaError_t up_p(const double* q_equiv, const int* items, int nitems, const int* surf_ijk,
+                        const double* twiddle, int P, int ns, int nsrc, int sp, T* Q, cudaStream_t st) {
+  const size_t sm = up_smem<T>(P, sp);
+  cudaError_t e = cudaFuncSetAttribute(k_m2l_up<T, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  k_m2l_up<T, PP><<<nitems, 256, sm, st>>>(q_equiv, items, surf_ijk, twiddle, P, ns, nsrc, sp, Q);
+  return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_m2l_up(const double* q_equiv, const int* items, int nitems, const int* surf_ijk,
-                          const double* twiddle, int P, int ns, T* Q, cudaStream_t st) {
-  if (nitems > 0) {
-    const size_t sm = up_smem<T>(P);
-    cudaError_t e = cudaFuncSetAttribute(k_m2l_up<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
-    k_m2l_up<T><<<nitems, 256, sm, st>>>(q_equiv, items, surf_ijk, twiddle, P, ns, Q);
+                          const double* twiddle, int P, int ns, int nsrc, int sp, T* Q, cudaStream_t st) {
+  if (nitems <= 0) return cudaGetLastError();
+  switch (P) {
+    case 4: return up_p<T, 4>(q_equiv, items, nitems, surf_ijk, twiddle, P, ns, nsrc, sp, Q, st);
+    case 6: return up_p<T, 6>(q_equiv, items, nitems, surf_ijk, twiddle, P, ns, nsrc, sp, Q, st);
+    case 8: return up_p<T, 8>(q_equiv, items, nitems, surf_ijk, twiddle, P, ns, nsrc, sp, Q, st);
+    case 10: return up_p<T, 10>(q_equiv, items, nitems, surf_ijk, twiddle, P, ns, nsrc, sp, Q, st);
+    default: return up_p<T, 0>(q_equiv, items, nitems, surf_ijk, twiddle, P, ns, nsrc, sp, Q, st);
   }
-  return cudaGetLastError();
 }
 
 template <typename T>
-cudaError_t launch_m2l_hadamard8(const T* Q, const T* G, const int* tsrc, int ntar, int Nf, T* Pk,
+cudaError_t launch_m2l_hadamard8(const T* Q, const T* G, const int* tsrcT, int ntar, int nsrc, int Nf, T* Pk,
                                  cudaStream_t st) {
   if (ntar > 0) {
-    dim3 grid(cdiv(ntar, kHadTargets), cdiv(Nf, 32));
-    k_m2l_hadamard8<T><<<grid, dim3(32, kHadWarps), 0, st>>>(Q, G, tsrc, ntar, Nf, Pk);
+    dim3 grid(cdiv(ntar, kHadThreads), Nf);
+    k_m2l_hadamard8<T><<<grid, kHadThreads, 0, st>>>(Q, G, tsrcT, ntar, nsrc, Nf, Pk);
   }
   return cudaGetLastError();
 }
 
-cudaError_t launch_m2l_hadamard27(const double* Q, const double* G27, const int* tsrc, int ntar, int Nf,
-                                  double* Pk, cudaStream_t st) {
+cudaError_t launch_m2l_hadamard27(const double* Q, const double* G27, const int* tsrc, int ntar, int nsrc,
+                                  int Nf, double* Pk, cudaStream_t st) {
   if (ntar > 0) {
     dim3 grid(cdiv(Nf, 128), ntar);
-    k_m2l_hadamard27<<<grid, 128, 0, st>>>(Q, G27, tsrc, ntar, Nf, Pk);
+    k_m2l_hadamard27<<<grid, 128, 0, st>>>(Q, G27, tsrc, ntar, nsrc, Nf, Pk);
   }
+  return cudaGetLastError();
+}
+
+template <typename T, int PP>
+static cudaError_t down_p(const T* Pk, const int* items, const double* tscale, int nitems, const int* surf_ijk,
+                          const double* twiddle, int P, int ns, int ntar, int sp, double* p_check,
+                          cudaStream_t st) {
+  const size_t sm = down_smem<T>(P, sp);
+  cudaError_t e = cudaFuncSetAttribute(k_m2l_down<T, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  k_m2l_down<T, PP><<<nitems, 256, sm, st>>>(Pk, items, tscale, surf_ijk, twiddle, P, ns, ntar, sp, p_check);
   return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_m2l_down(const T* Pk, const int* items, const double* tscale, int nitems,
-                            const int* surf_ijk, const double* twiddle, int P, int ns, double* p_check,
-                            cudaStream_t st) {
-  if (nitems > 0) {
-    const size_t sm = down_smem<T>(P);
-    cudaError_t e = cudaFuncSetAttribute(k_m2l_down<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
-    k_m2l_down<T><<<nitems, 256, sm, st>>>(Pk, items, tscale, surf_ijk, twiddle, P, ns, p_check);
+                            const int* surf_ijk, const double* twiddle, int P, int ns, int ntar, int sp,
+                            double* p_check, cudaStream_t st) {
+  if (nitems <= 0) return cudaGetLastError();
+  switch (P) {
+    case 4: return down_p<T, 4>(Pk, items, tscale, nitems, surf_ijk, twiddle, P, ns, ntar, sp, p_check, st);
+    case 6: return down_p<T, 6>(Pk, items, tscale, nitems, surf_ijk, twiddle, P, ns, ntar, sp, p_check, st);
+    case 8: return down_p<T, 8>(Pk, items, tscale, nitems, surf_ijk, twiddle, P, ns, ntar, sp, p_check, st);
+    case 10: return down_p<T, 10>(Pk, items, tscale, nitems, surf_ijk, twiddle, P, ns, ntar, sp, p_check, st);
+    default: return down_p<T, 0>(Pk, items, tscale, nitems, surf_ijk, twiddle, P, ns, ntar, sp, p_check, st);
   }
-  return cudaGetLastError();
 }
 
 cudaError_t launch_dipole(const double4* body64, int n, double* partial, cudaStream_t st) {
@@ -866,16 +936,16 @@ cudaError_t launch_post(const double* phi_far, const double* grad_far, const dou
 }
 
 template cudaError_t launch_m2l_up<float>(const double*, const int*, int, const int*, const double*, int, int,
-                                          float*, cudaStream_t);
+                                          int, int, float*, cudaStream_t);
 template cudaError_t launch_m2l_up<double>(const double*, const int*, int, const int*, const double*, int, int,
-                                           double*, cudaStream_t);
-template cudaError_t launch_m2l_hadamard8<float>(const float*, const float*, const int*, int, int, float*,
+                                           int, int, double*, cudaStream_t);
+template cudaError_t launch_m2l_hadamard8<float>(const float*, const float*, const int*, int, int, int, float*,
                                                  cudaStream_t);
-template cudaError_t launch_m2l_hadamard8<double>(const double*, const double*, const int*, int, int, double*,
-                                                  cudaStream_t);
+template cudaError_t launch_m2l_hadamard8<double>(const double*, const double*, const int*, int, int, int,
+                                                  double*, cudaStream_t);
 template cudaError_t launch_m2l_down<float>(const float*, const int*, const double*, int, const int*,
-                                            const double*, int, int, double*, cudaStream_t);
+                                            const double*, int, int, int, int, double*, cudaStream_t);
 template cudaError_t launch_m2l_down<double>(const double*, const int*, const double*, int, const int*,
-                                             const double*, int, int, double*, cudaStream_t);
+                                             const double*, int, int, int, int, double*, cudaStream_t);
 
 }  // namespace rtfmm_b200

@@ -65,18 +65,25 @@ cudaError_t launch_apply(const ApplyBatch& b, cudaStream_t st);
 // (parent, coff, cnum) triplets
 cudaError_t launch_sum_children(const int* list, int nparents, const double* Y, int ns, double* q,
                                 cudaStream_t st);
+// FFT-M2L spectra are frequency-major: Q[f][src][slot], Pk[f][tar][slot],
+// G[f][d][isrc*8+itar] (complex, interleaved re/im).
+// items hold 10 ints per block: parent, first slot, child cell of each of the
+// sp slots of the group (-1 = absent); sp from m2l_up_slots / m2l_down_slots.
 template <typename T>
-cudaError_t launch_m2l_up(const double* q_equiv, const int* items /*(src,slot,child)*/, int nitems,
-                          const int* surf_ijk, const double* twiddle, int P, int ns, T* Q,
-                          cudaStream_t st);
+int m2l_up_slots(int P);
 template <typename T>
-cudaError_t launch_m2l_hadamard8(const T* Q, const T* G, const int* tsrc, int ntar, int Nf, T* Pk,
-                                 cudaStream_t st);
-cudaError_t launch_m2l_hadamard27(const double* Q, const double* G27, const int* tsrc, int ntar, int Nf,
-                                  double* Pk, cudaStream_t st);
+int m2l_down_slots(int P);
 template <typename T>
-cudaError_t launch_m2l_down(const T* Pk, const int* items /*(tar,slot,child)*/, const double* tscale,
-                            int nitems, const int* surf_ijk, const double* twiddle, int P, int ns,
+cudaError_t launch_m2l_up(const double* q_equiv, const int* items, int nitems, const int* surf_ijk,
+                          const double* twiddle, int P, int ns, int nsrc, int sp, T* Q, cudaStream_t st);
+template <typename T>
+cudaError_t launch_m2l_hadamard8(const T* Q, const T* G, const int* tsrcT /*[26][ntar]*/, int ntar, int nsrc,
+                                 int Nf, T* Pk, cudaStream_t st);
+cudaError_t launch_m2l_hadamard27(const double* Q, const double* G27 /*[d][f]*/, const int* tsrc /*[ntar][26]*/,
+                                  int ntar, int nsrc, int Nf, double* Pk, cudaStream_t st);
+template <typename T>
+cudaError_t launch_m2l_down(const T* Pk, const int* items, const double* tscale, int nitems,
+                            const int* surf_ijk, const double* twiddle, int P, int ns, int ntar, int sp,
                             double* p_check, cudaStream_t st);
 cudaError_t launch_l2p_eval(const double4* body64, const LeafInfo* leaves, int nleaf,
                             const double* surf_unit, int ns, const double* q_down, double* phi,
