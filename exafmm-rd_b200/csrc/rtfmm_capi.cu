@@ -1101,6 +1101,10 @@ int rtfmm_b200_get_operator(rtfmm_fmm* f, int which, double* out, int64_t cap) {
     v = o.m2m_img_sum;
   } else if (which == 3) {
     v = o.cc8;
+  } else if (which == 4) {
+    v = o.U;
+  } else if (which == 5) {
+    v = o.VSinv;
   } else {
     return fail(RTFMM_EINVAL, "unknown operator");
   }

@@ -180,7 +180,9 @@ int rtfmm_b200_get_cell_vectors(rtfmm_fmm* fmm, int which, double* out);
  * which = 0: pinv of the upward equivalent->check operator (ns*ns),
  *         1: M2M for octants 0..7 (8*ns*ns),  2: sum of the 27 image M2M
  *            (ns*ns),  3: 8x8 kernel spectra (26*8*8*Nfreq complex, as
- *            interleaved re,im). */
+ *            interleaved re,im),  4: U and 5: V S^-1 of the SVD
+ *            e2c = U S V^T with the pseudo-inverted S (UT_p2m_precompute^T
+ *            and VSinv_p2m_precompute, kernel.h:197-200), row-major ns*ns. */
 int rtfmm_b200_get_operator(rtfmm_fmm* fmm, int which, double* out, int64_t cap);
 
 /* Last error message of the calling thread ("" if none). */

@@ -200,3 +200,22 @@ def test_p2p_pairs_cover_reference_lists(pkg, oracle):
     assert nonleaf > 0
     pairs = sum(C.bnum[t] * C.bnum[s] for t, l in F.trav.p2p.items() for (s, off) in l)
     assert f.info()["p2p_pairs"] == pairs
+
+
+@pytest.mark.parametrize("P", [4, 6])
+def test_svd_factors(pkg, oracle, P):
+    """The exported SVD factors: U is orthogonal and V S^-1 U^T is the
+    pseudo-inverse of the equivalent-to-check matrix (kernel.cpp:1643-1651)."""
+    x, q = uniform(200, 4)
+    f = pkg.LaplaceFMM(x, q, pkg.Argument(P=P, ncrit=64, images=0, cycle=1.0))
+    f.setup()
+    ns = oracle.surface_point_num(P)
+    U = f.operator(4, ns * ns).reshape(ns, ns)
+    VS = f.operator(5, ns * ns).reshape(ns, ns)
+    assert np.abs(U.T @ U - np.eye(ns)).max() < 1e-12
+    xc = oracle.surface_points(P, 0.5 * 2.95)
+    xe = oracle.surface_points(P, 0.5 * 1.05)
+    A = oracle.p2p_matrix(xe, xc)
+    pinv = VS @ U.T
+    assert np.linalg.norm(A @ pinv @ A - A) / np.linalg.norm(A) < 1e-9
+    assert np.allclose(pinv, f.operator(0, ns * ns).reshape(ns, ns), rtol=0, atol=1e-9 * np.abs(pinv).max())
