@@ -792,6 +792,10 @@ int collect_times(rtfmm_fmm* f, float* total) {
 
 }  // namespace
 
+namespace rtfmm_b200 {
+void set_last_error(const std::string& msg) { g_err = msg; }
+}  // namespace rtfmm_b200
+
 // ===========================================================================
 // C ABI
 // ===========================================================================

@@ -36,7 +36,7 @@ EXPORTS = (
     "rtfmm_b200_download", "rtfmm_b200_adjoint", "rtfmm_b200_stage_times", "rtfmm_b200_launch_count",
     "rtfmm_b200_flush_l2", "rtfmm_b200_info", "rtfmm_b200_get_cells", "rtfmm_b200_get_perm",
     "rtfmm_b200_get_p2p", "rtfmm_b200_get_m2l", "rtfmm_b200_get_cell_vectors", "rtfmm_b200_get_operator",
-    "rtfmm_b200_last_error", "rtfmm_b200_version",
+    "rtfmm_b200_last_error", "rtfmm_b200_version", "rtfmm_b200_p2m_noalloc",
 )
 
 

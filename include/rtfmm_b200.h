@@ -185,6 +185,49 @@ int rtfmm_b200_get_cell_vectors(rtfmm_fmm* fmm, int which, double* out);
  *            and VSinv_p2m_precompute, kernel.h:197-200), row-major ns*ns. */
 int rtfmm_b200_get_operator(rtfmm_fmm* fmm, int which, double* out, int64_t cap);
 
+/* ---- P2M that allocates no device memory ----
+ *
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc,
+ * for example code running under another framework's device-memory pool,
+ * where an allocation outside the pool would escape its accounting or fail
+ * against its limits.  The call computes the P2M stage for a batch of leaves
+ * (check-surface potentials of the leaves' bodies, then
+ * q_equiv = 0.5^depth * (V S^-1) (U^T p_check)) exactly as the evaluation
+ * pass does, and allocates nothing: inputs and the output are the caller's
+ * device buffers, and its scratch is one fixed array of
+ * RTFMM_NOALLOC_SCRATCH_BYTES that every GPU loading this library holds
+ * until the process exits.
+ *
+ *   d_leaves   nleaf leaf records (rtfmm_leaf, in device memory)
+ *   d_bodies   bodies as (x, y, z, q) doubles, grouped by leaf
+ *   d_U        U of the SVD e2c = U S V^T, row-major num_surf x num_surf
+ *   d_VSinvT   (V S^-1)^T, row-major num_surf x num_surf
+ *              (rtfmm_b200_get_operator gives U and V S^-1 for a set-up)
+ *   d_q_equiv  output, nleaf x num_surf, row l for leaf l
+ *   stream     cudaStream_t to run on (NULL: the default stream)
+ *
+ * The batch must fit the scratch: 2*nleaf*num_surf + 3*num_surf + 1.5*nleaf
+ * doubles (at P=8, up to 1766 leaves); larger batches return RTFMM_EINVAL
+ * and should be split.  The first call on a device looks up the scratch
+ * array's device address (cudaGetSymbolAddress), so make that first call
+ * before any stream capture.  Every call reuses the same scratch and
+ * overwrites what it reads, so nothing carries over between calls; calls
+ * that overlap on the GPU (other streams, other host threads) race on it and
+ * must be serialised by the caller. */
+#define RTFMM_NOALLOC_SCRATCH_BYTES (8u << 20)
+
+typedef struct rtfmm_leaf {
+  double cx, cy, cz;   /* leaf centre                         */
+  double r;            /* half edge                           */
+  double scale;        /* 0.5^depth                           */
+  int32_t cell;        /* caller's cell id (not read)         */
+  int32_t boff, bnum;  /* the leaf's bodies in d_bodies       */
+  int32_t pad;
+} rtfmm_leaf;
+
+int rtfmm_b200_p2m_noalloc(int P, int64_t nleaf, const rtfmm_leaf* d_leaves, const double* d_bodies,
+                           const double* d_U, const double* d_VSinvT, double* d_q_equiv, void* stream);
+
 /* Last error message of the calling thread ("" if none). */
 const char* rtfmm_b200_last_error(void);
 
