@@ -62,7 +62,11 @@ struct ApplyCall {
 //   P2M  (p2m_precompute, kernel.cpp:369-370): y = U^T p, q = scale * V S^-1 y
 //   L2P  (l2p_precompute, kernel.cpp:1465-1467): y = V^T p, q = scale * U S^-1 y
 //   M2M per octant (transposed), L2L = M2M^T per octant, image sum / image 13
-enum BSel { B_P2M1 = 0, B_P2M2, B_L2P1, B_L2P2, B_M2MT, B_M2M, B_IMGSUMT, B_IMG13, B_NUM };
+//   adjoint image levels: the transposes swap roles, so the upward step uses
+//   M2M_img[13] (the transpose of the forward L2L_img) and the downward step
+//   the transposed 27-image sum
+enum BSel { B_P2M1 = 0, B_P2M2, B_L2P1, B_L2P2, B_M2MT, B_M2M, B_IMGSUMT, B_IMG13, B_ADJ_IMG_UP, B_ADJ_IMG_DOWN,
+            B_NUM };
 
 }  // namespace
 
@@ -544,6 +548,10 @@ int upload_plan(rtfmm_fmm* f) {
   for (int j = 0; j < ns; ++j)
     for (int i = 0; i < ns; ++i) b[(size_t)j * ns + i] = o.l2l_img[(size_t)i * ns + j];
   RC(dupload(f, &f->d_B[B_IMG13], b));
+  // adjoint: upward y = M2M_img[13] x (B[j][n] = L2L_img[j][n]); downward
+  // y = (sum of M2M_img)^T x (B[j][n] = sum[j][n])
+  RC(dupload(f, &f->d_B[B_ADJ_IMG_UP], o.l2l_img));
+  RC(dupload(f, &f->d_B[B_ADJ_IMG_DOWN], o.m2m_img_sum));
   RC(dupload(f, &f->d_idx_pool, f->idx_pool));
   RC(dupload(f, &f->d_scale_pool, f->scale_pool));
   // M2L: kernel spectra re-laid frequency-major, G[f][d][pair]
@@ -623,7 +631,7 @@ int upload_plan(rtfmm_fmm* f) {
   return RTFMM_OK;
 }
 
-int run_apply(rtfmm_fmm* f, const ApplyCall& c) {
+int run_apply(rtfmm_fmm* f, const ApplyCall& c, bool adjoint = false) {
   ApplyBatch b;
   double* bufs[BUF_NUM] = {f->d_qeq, f->d_pchk, f->d_leafvec, f->d_leafvec2, f->d_y};
   b.A = bufs[c.abuf];
@@ -632,7 +640,10 @@ int run_apply(rtfmm_fmm* f, const ApplyCall& c) {
   b.outrow = f->d_idx_pool + c.outrow_off;
   b.group_off = f->d_idx_pool + c.goff_off;
   b.scale = c.has_scale ? f->d_scale_pool + c.scale_off : nullptr;
-  b.B = f->d_B[c.bsel];
+  int bsel = c.bsel;
+  if (adjoint && bsel == B_IMGSUMT) bsel = B_ADJ_IMG_UP;
+  if (adjoint && bsel == B_IMG13) bsel = B_ADJ_IMG_DOWN;
+  b.B = f->d_B[bsel];
   b.groups = c.groups;
   b.S = c.S;
   b.ns = f->ops.ns;
@@ -647,8 +658,12 @@ int run_apply(rtfmm_fmm* f, const ApplyCall& c) {
   return RTFMM_OK;
 }
 
-// One evaluation pass on the device-resident bodies (d_body64).
-int enqueue_pass(rtfmm_fmm* f) {
+// One evaluation pass on the device-resident bodies (d_body64).  With
+// `adjoint` the pass applies the transposed operator chain to the body
+// charges (which then hold the weights w): P2P, M2L and the tree-level
+// M2M/L2L and P2M/L2P pairs are their own transposes on the symmetric lists,
+// only the image-level operators swap; no dipole correction.
+int enqueue_pass(rtfmm_fmm* f, bool adjoint = false, bool no_dipole = false) {
   const Plan& p = f->plan;
   const Operators& o = f->ops;
   const int n = (int)p.n, ns = o.ns, Nf = o.Nf, P = o.P;
@@ -694,7 +709,7 @@ int enqueue_pass(rtfmm_fmm* f) {
     }
     CK(cudaEventRecord(f->ev_st[ST_P2M], s0));
     for (auto& c : f->m2m_calls) {
-      int rc = run_apply(f, c);
+      int rc = run_apply(f, c, adjoint);
       if (rc) return rc;
     }
     CK(cudaEventRecord(f->ev_st[ST_M2M], s0));
@@ -733,7 +748,7 @@ int enqueue_pass(rtfmm_fmm* f) {
     f->launches += (ndn8 > 0) + (ndn27 > 0);
     CK(cudaEventRecord(f->ev_st[ST_DOWN], s0));
     for (auto& c : f->l2l_calls) {
-      int rc = run_apply(f, c);
+      int rc = run_apply(f, c, adjoint);
       if (rc) return rc;
     }
     CK(cudaEventRecord(f->ev_st[ST_L2L], s0));
@@ -755,13 +770,14 @@ int enqueue_pass(rtfmm_fmm* f) {
   if (near && !serial) CK(cudaStreamWaitEvent(s0, f->ev_near, 0));
   CK(cudaEventRecord(f->ev_st[ST_P2P], s0));
   const Args& a = f->args;
-  if (a.dipole_correction) {
+  const int dipole = (adjoint || no_dipole) ? 0 : a.dipole_correction;
+  if (dipole) {
     CK(launch_dipole(f->d_body64, n, f->d_dip, s0));
     f->launches += 2;
   }
   const double coef = 4 * M_PI / (3 * a.cycle * a.cycle * a.cycle);
   CK(launch_post(far ? f->d_far_phi : nullptr, f->d_far_grad, near ? f->d_near_phi : nullptr, f->d_near_grad,
-                 f->d_body64, f->d_perm, n, f->d_dip, coef, a.dipole_correction,
+                 f->d_body64, f->d_perm, n, f->d_dip, coef, dipole,
                  a.divide_4pi ? 1.0 / (4 * M_PI) : 1.0, f->d_out_phi, f->d_out_grad, s0));
   f->launches++;
   CK(cudaEventRecord(f->ev_st[ST_POST], s0));
@@ -964,11 +980,42 @@ int rtfmm_b200_solve(rtfmm_fmm* f, int64_t n, const double* x, const double* q, 
 }
 
 int rtfmm_b200_adjoint(rtfmm_fmm* f, const double* w, double* dLdq, double* dLdx) {
-  (void)w;
-  (void)dLdq;
-  (void)dLdx;
   if (!f) return fail(RTFMM_EINVAL, "null handle");
-  return fail(RTFMM_ENOTSUP, "adjoint not built yet");
+  if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");
+  const int64_t n = f->plan.n;
+  if (n == 0) return RTFMM_OK;
+  if (!w) return fail(RTFMM_EINVAL, "null weights");
+  if (!finite_all(w, n)) return fail(RTFMM_EINVAL, "non-finite weight");
+  if (!f->device_ready) {
+    int rc = upload_plan(f);
+    if (rc) return rc;
+  }
+  CK(cudaSetDevice(f->dev));
+  std::vector<double> gw(3 * n), gq(3 * n), pw(n);
+  // 1) transposed chain on the weights: dL/dq and grad(psi_w) at the bodies
+  CK(cudaMemcpyAsync(f->d_xin, f->h_xin, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, f->s0));
+  CK(cudaMemcpyAsync(f->d_qin, w, sizeof(double) * n, cudaMemcpyHostToDevice, f->s0));
+  CK(launch_gather_bodies(f->d_xin, f->d_qin, f->d_perm, (int)n, f->d_body64, f->s0));
+  int rc = enqueue_pass(f, true);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(pw.data(), f->d_out_phi, sizeof(double) * n, cudaMemcpyDeviceToHost, f->s0));
+  CK(cudaMemcpyAsync(gw.data(), f->d_out_grad, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, f->s0));
+  // 2) the forward field of the charges, recomputed (nothing kept from the
+  //    forward call): grad(phi_q) at the bodies
+  CK(cudaMemcpyAsync(f->d_qin, f->q_in.data(), sizeof(double) * n, cudaMemcpyHostToDevice, f->s0));
+  CK(launch_gather_bodies(f->d_xin, f->d_qin, f->d_perm, (int)n, f->d_body64, f->s0));
+  rc = enqueue_pass(f, false, true);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(gq.data(), f->d_out_grad, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, f->s0));
+  CK(cudaStreamSynchronize(f->s0));
+  CK(cudaGetLastError());
+  // dL/dx_i = w_i grad(phi_q)(x_i) + q_i grad(psi_w)(x_i)
+  if (dLdq) std::memcpy(dLdq, pw.data(), sizeof(double) * n);
+  if (dLdx)
+    for (int64_t i = 0; i < n; ++i)
+      for (int k = 0; k < 3; ++k) dLdx[3 * i + k] = w[i] * gq[3 * i + k] + f->q_in[i] * gw[3 * i + k];
+  f->pass_done = true;
+  return RTFMM_OK;
 }
 
 int rtfmm_b200_stage_times(rtfmm_fmm* f, double* ms, int cap) {

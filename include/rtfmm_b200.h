@@ -127,8 +127,10 @@ int rtfmm_b200_download(rtfmm_fmm* fmm, double* phi, double* grad);
  * has no gradient code).  For L = sum_i w_i phi_i it returns dL/dq (n) and
  * dL/dx (n*3) by applying the transposed operator chain P2P^T, L2P^T, L2L^T,
  * M2L^T (conjugated kernel spectra), M2M^T, P2M^T; upward coefficients are
- * recomputed.  Requires a previous evaluate on the same bodies.  The
- * divide_4pi scaling applies; the dipole correction is excluded.
+ * recomputed.  Works on the bodies and charges given to setup (w is n, in
+ * input order; dLdq n, dLdx n*3, either may be NULL).  For a quadratic L
+ * (w depending on q) the caller adds the explicit term.  The divide_4pi
+ * scaling applies; the dipole correction is excluded.
  */
 int rtfmm_b200_adjoint(rtfmm_fmm* fmm, const double* w, double* dLdq, double* dLdx);
 
