@@ -59,11 +59,11 @@ def make_bodies(n, seed):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clock and throttle reasons sampled through NVML (read-only) every
+    10 ms during the timed region."""
 
-    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4}
 
     def __init__(self, index):
         self.index = index
@@ -72,16 +72,19 @@ class ClockSampler:
         self._t = None
 
     def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                     timeout=5).stdout.strip()
-                if out:
-                    self.samples.append([v.strip() for v in out.split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByIndex(self.index)
+            mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            while not self._stop.is_set():
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+                self.samples.append((sm, mx, rs))
+                self._stop.wait(0.01)
+            nv.nvmlShutdown()
+        except Exception:
+            pass
 
     def __enter__(self):
         self._t = threading.Thread(target=self._run, daemon=True)
@@ -94,22 +97,17 @@ class ClockSampler:
 
     def summary(self):
         if not self.samples:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = set()
-        for s in self.samples:
-            for k, nm in enumerate(names):
-                if len(s) > 4 + k and s[4 + k].lower().startswith("active"):
-                    reasons.add(nm)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.samples)}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        reasons = sorted({nm for (_, _, r) in self.samples for nm, bit in self.REASONS.items() if r & bit})
+        return {"sm_mhz": float(np.median([s[0] for s in self.samples])),
+                "sm_max_mhz": float(max(s[1] for s in self.samples)), "reasons": reasons,
+                "samples": len(self.samples)}
 
 
 def read_traffic(kernel):
-    """dram bytes per launch from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, "profiles", "%s_traffic.txt" % kernel)
+    """dram bytes per launch of the default workload, from the committed ncu
+    summary, if present."""
+    path = os.path.join(ROOT, "profiles", "k_%s_n1M_p8_traffic.txt" % kernel)
     if not os.path.exists(path):
         return None
     for line in open(path):
@@ -279,6 +277,21 @@ def run_ours(args):
         e2e.append(time.perf_counter() - t0)
     barrier()
 
+    # forward + adjoint through the C ABI (host buffers), both precisions:
+    # the north-star comparison of the mixed and FP64 forms on the full step
+    wts = np.random.default_rng(4).standard_normal(n)
+
+    def fwd_adj(f):
+        t0 = time.perf_counter()
+        f.evaluate(q)
+        f.adjoint(wts)
+        return time.perf_counter() - t0
+
+    fwd_adj(fm)
+    fwd_adj(f64)
+    fa_m = float(np.mean([fwd_adj(fm) for _ in range(3)]))
+    fa_d = float(np.mean([fwd_adj(f64) for _ in range(3)]))
+
     t_m = float(np.mean(ms_mixed))
     t_d = float(np.mean(ms64))
     t_e = float(np.mean(e2e))
@@ -340,6 +353,8 @@ def run_ours(args):
                    "fp64_ms_per_step": t_d, "fp64_value": world * n / (t_d * 1e-3),
                    "mixed_speedup_vs_fp64": t_d / t_m,
                    "mixed_err_vs_fp64": {"l2p": err["l2p"], "l2f": err["l2f"], "l2p_mean_removed": err_mr},
+                   "fwd_adj_ms_mixed": 1000 * fa_m, "fwd_adj_ms_fp64": 1000 * fa_d,
+                   "fwd_adj_mixed_speedup_vs_fp64": fa_d / fa_m,
                    "stage_ms_overlapped": st_mixed, "stage_ms_serial": stage_serial},
         "roofline": roofline,
         "cpu_baseline": cpu,
