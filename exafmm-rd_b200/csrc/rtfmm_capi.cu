@@ -86,7 +86,7 @@ struct rtfmm_fmm {
   std::vector<LeafInfo> leaves;
   std::vector<int> body_leaf;
   std::vector<P2PItem> items;    // 32 targets per item (FP64 P2P)
-  std::vector<P2PItem> items2;   // 64 targets per item (FP32 P2P)
+  std::vector<P2PItem32> items2; // FP32 P2P items (target groups)
   std::vector<int> list_off;
   std::vector<P2PSrc32> list32;
   std::vector<P2PSrc64> list64;
@@ -116,7 +116,7 @@ struct rtfmm_fmm {
   double *d_far_phi = nullptr, *d_far_grad = nullptr, *d_near_phi = nullptr, *d_near_grad = nullptr;
   double *d_out_phi = nullptr, *d_out_grad = nullptr;
   P2PItem* d_items = nullptr;
-  P2PItem* d_items2 = nullptr;
+  P2PItem32* d_items2 = nullptr;
   int* d_list_off = nullptr;
   P2PSrc32* d_list32 = nullptr;
   P2PSrc64* d_list64 = nullptr;
@@ -265,7 +265,9 @@ void build_tables(rtfmm_fmm* f) {
       a.dz = (float)(S.x[2] + e.off[2] - T.x[2]);
       a.leaf = sl;
       a.self = (e.src == c && e.off[0] == 0 && e.off[1] == 0 && e.off[2] == 0) ? 1 : 0;
-      a.pad[0] = a.pad[1] = a.pad[2] = 0;
+      a.boff = f->leaves[sl].boff;
+      a.bnum = f->leaves[sl].bnum;
+      a.pad = 0;
       f->list32.push_back(a);
       P2PSrc64 b;
       b.ox = e.off[0];
@@ -276,7 +278,14 @@ void build_tables(rtfmm_fmm* f) {
       f->list64.push_back(b);
     }
     for (int t0 = 0; t0 < f->leaves[l].bnum; t0 += 32) f->items.push_back({l, t0});
-    for (int t0 = 0; t0 < f->leaves[l].bnum; t0 += 64) f->items2.push_back({l, t0});
+    // FP32 items: 32 targets each; the last <= 16 targets of a leaf take a
+    // narrower group (W = 16, 8 or 4 lanes) and split the sources 32/W ways
+    for (int t0 = 0; t0 < f->leaves[l].bnum; t0 += 32) {
+      const int rem = std::min(32, f->leaves[l].bnum - t0);
+      int lw = 5;
+      while (lw > 2 && rem <= (1 << (lw - 1))) --lw;
+      f->items2.push_back({l, f->leaves[l].boff + t0, rem, lw});
+    }
   }
   f->list_off[f->leaves.size()] = (int)f->list32.size();
 
@@ -683,7 +692,7 @@ int enqueue_pass(rtfmm_fmm* f, bool adjoint = false, bool no_dipole = false) {
     }
     CK(cudaEventRecord(f->ev_near0, s1));
     if (mixed) {
-      CK(launch_p2p32(f->d_body32, f->d_leaves, f->d_items, (int)f->items.size(), f->d_list_off, f->d_list32,
+      CK(launch_p2p32(f->d_body32, f->d_items2, (int)f->items2.size(), f->d_list_off, f->d_list32,
                       f->d_near_phi, f->d_near_grad, s1));
       f->launches += 1;
     } else {
@@ -701,7 +710,7 @@ int enqueue_pass(rtfmm_fmm* f, bool adjoint = false, bool no_dipole = false) {
   CK(cudaEventRecord(f->ev_st[ST_PREP], s0));
   if (far) {
     CK(cudaMemsetAsync(f->d_pchk, 0, sizeof(double) * p.cells.size() * ns, s0));
-    CK(launch_p2m_check(f->d_body64, f->d_leaves, nleaf, f->d_surf_unit, ns, f->d_leafvec, s0));
+    CK(launch_p2m_check(f->d_body64, f->d_leaves, nleaf, f->d_surf_unit, ns, f->d_leafvec, s0, mixed ? 1 : 2));
     f->launches++;
     for (auto& c : f->p2m_call) {
       int rc = run_apply(f, c);
@@ -757,7 +766,7 @@ int enqueue_pass(rtfmm_fmm* f, bool adjoint = false, bool no_dipole = false) {
       if (rc) return rc;
     }
     CK(launch_l2p_eval(f->d_body64, f->d_leaves, nleaf, f->d_surf_unit, ns, f->d_leafvec2, f->d_far_phi,
-                       f->d_far_grad, s0));
+                       f->d_far_grad, s0, mixed ? 1 : 2));
     f->launches++;
     CK(cudaEventRecord(f->ev_st[ST_L2P], s0));
   } else {

@@ -17,6 +17,29 @@
 
 #include <cuda_runtime.h>
 
+// FP32 P2P: inner unroll and resident blocks per SM
+#ifndef P2P_UNROLL
+#define P2P_UNROLL 8
+#endif
+#ifndef P2P_MINB
+#define P2P_MINB 6
+#endif
+// FP32 Hadamard: targets per thread, directions per FP32 partial sum,
+// resident blocks per SM
+#ifndef HAD_TT
+#define HAD_TT 1
+#endif
+#ifndef HAD_DF
+#define HAD_DF 2
+#endif
+#ifndef HAD_MINB
+#define HAD_MINB 2
+#endif
+// FP64 operator application: output rows per block (64 or 128)
+#ifndef APPLY_TM
+#define APPLY_TM 64
+#endif
+
 namespace rtfmm_b200 {
 
 // ---------------------------------------------------------------------------
@@ -46,6 +69,22 @@ __device__ __forceinline__ float rsqrt_approx(float x) {
   return y;
 }
 
+// 1/sqrt(x) in FP64 by Newton-Raphson from the FP32 hardware approximation:
+// y <- y (3/2 - x y^2 / 2).  The approximation is good to about 2^-22, so
+// one step gives ~1e-13 and two give full double precision.  Arguments
+// outside the normal FP32 range (pairs closer than ~1e-19 or farther than
+// ~1e19) take the FP64 library function instead.
+template <int NR>
+__device__ __forceinline__ double rsqrt_nr(double x) {
+  const float xf = (float)x;
+  if (!(xf >= 1.2e-38f && xf <= 3.0e38f)) return rsqrt(x);
+  double y = (double)rsqrt_approx(xf);
+  const double h = 0.5 * x;
+#pragma unroll
+  for (int i = 0; i < NR; ++i) y = y * fma(-h * y, y, 1.5);
+  return y;
+}
+
 // ---------------------------------------------------------------------------
 // body preparation
 // ---------------------------------------------------------------------------
@@ -69,17 +108,20 @@ __global__ void k_prep32(const double4* __restrict__ body64, const int* __restri
 }
 
 // ---------------------------------------------------------------------------
-// P2P: one warp per (target leaf, block of targets); sources staged 32 at a
-// time in a per-warp shared-memory slot and read as broadcasts.  FP32 partial
-// sums per source leaf are accumulated into FP64.
+// P2P: one warp per work item (up to 32 targets of one leaf); sources staged
+// 32 at a time in a per-warp shared-memory slot and read as broadcasts, the
+// next tile's bodies and the next list entry loaded while the current tile is
+// computed.  FP32 partial sums per source leaf are accumulated into FP64.
 // ---------------------------------------------------------------------------
 constexpr int kP2PWarps = 4;
+constexpr int kP2PUnroll = P2P_UNROLL;
 
-template <bool MASK>
-__device__ __forceinline__ void p2p32_tile(const float4* __restrict__ s, int cnt, float px, float py,
+// Lanes of group `k0` (of G groups) take the tile's sources k0, k0+G, ...
+template <int G, bool MASK>
+__device__ __forceinline__ void p2p32_tile(const float4* __restrict__ s, int k0, int cnt, float px, float py,
                                            float pz, float& p, float& fx, float& fy, float& fz) {
-#pragma unroll 8
-  for (int k = 0; k < cnt; ++k) {
+#pragma unroll kP2PUnroll
+  for (int k = k0; k < cnt; k += G) {
     const float4 b = s[k];
     const float dx = px - b.x, dy = py - b.y, dz = pz - b.z;
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
@@ -94,48 +136,92 @@ __device__ __forceinline__ void p2p32_tile(const float4* __restrict__ s, int cnt
   }
 }
 
-// One warp per (target leaf, 32 targets), one target per lane.
-__global__ void __launch_bounds__(32 * kP2PWarps)
-    k_p2p32(const float4* __restrict__ body32, const LeafInfo* __restrict__ leaves,
-            const P2PItem* __restrict__ items, int nitems, const int* __restrict__ list_off,
-            const P2PSrc32* __restrict__ list, double* __restrict__ phi, double* __restrict__ grad) {
-  __shared__ float4 sbuf[kP2PWarps][32];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int item = blockIdx.x * kP2PWarps + warp;
-  if (item >= nitems) return;  // warp-uniform
-  const P2PItem it = items[item];
-  const LeafInfo T = leaves[it.leaf];
-  const int t = it.t0 + lane;
-  const bool active = t < T.bnum;
-  const float4 xt = active ? body32[T.boff + t] : make_float4(0.f, 0.f, 0.f, 0.f);
+// One work item: W = 32/G lanes per target group, G groups per warp.
+template <int G>
+__device__ __forceinline__ void p2p32_item(const float4* __restrict__ body32, const P2PItem32& it,
+                                           const int* __restrict__ list_off, const P2PSrc32* __restrict__ list,
+                                           float4* __restrict__ sw, int lane, double* __restrict__ phi,
+                                           double* __restrict__ grad) {
+  constexpr int W = 32 / G;
+  const int grp = lane / W, ti = lane % W;
+  const bool active = ti < it.nt;
+  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+  const float4 xt = active ? body32[it.boff + ti] : zero;
   double P = 0.0, Gx = 0.0, Gy = 0.0, Gz = 0.0;
+  int e = list_off[it.leaf];
   const int e1 = list_off[it.leaf + 1];
-  for (int e = list_off[it.leaf]; e < e1; ++e) {
-    const P2PSrc32 src = list[e];
-    const LeafInfo S = leaves[src.leaf];
-    const float px = xt.x - src.dx, py = xt.y - src.dy, pz = xt.z - src.dz;
-    float p = 0.f, fx = 0.f, fy = 0.f, fz = 0.f;
-    for (int c0 = 0; c0 < S.bnum; c0 += 32) {
-      const int cnt = min(32, S.bnum - c0);
-      __syncwarp();
-      if (lane < cnt) sbuf[warp][lane] = body32[S.boff + c0 + lane];
-      __syncwarp();
-      if (src.self)
-        p2p32_tile<true>(sbuf[warp], cnt, px, py, pz, p, fx, fy, fz);
-      else
-        p2p32_tile<false>(sbuf[warp], cnt, px, py, pz, p, fx, fy, fz);
-    }
-    P += (double)p;
-    Gx += (double)fx;
-    Gy += (double)fy;
-    Gz += (double)fz;
+  P2PSrc32 cur{}, nxt{};
+  float4 stage = zero;
+  if (e < e1) {
+    cur = list[e];
+    if (lane < cur.bnum) stage = body32[cur.boff + lane];
   }
-  if (active) {
-    const int b = T.boff + t;
+  if (e + 1 < e1) nxt = list[e + 1];
+  int c0 = 0;
+  float p = 0.f, fx = 0.f, fy = 0.f, fz = 0.f;
+  while (e < e1) {
+    const int cnt = min(32, cur.bnum - c0);
+    __syncwarp();
+    sw[lane] = stage;
+    __syncwarp();
+    // next tile: the rest of this source leaf, else the first of the next
+    const bool last = c0 + 32 >= cur.bnum;
+    stage = zero;
+    if (!last) {
+      if (lane < cur.bnum - c0 - 32) stage = body32[cur.boff + c0 + 32 + lane];
+    } else if (e + 1 < e1) {
+      if (lane < nxt.bnum) stage = body32[nxt.boff + lane];
+    }
+    const float px = xt.x - cur.dx, py = xt.y - cur.dy, pz = xt.z - cur.dz;
+    if (cur.self)
+      p2p32_tile<G, true>(sw, grp, cnt, px, py, pz, p, fx, fy, fz);
+    else
+      p2p32_tile<G, false>(sw, grp, cnt, px, py, pz, p, fx, fy, fz);
+    if (last) {
+      P += (double)p;
+      Gx += (double)fx;
+      Gy += (double)fy;
+      Gz += (double)fz;
+      p = fx = fy = fz = 0.f;
+      ++e;
+      c0 = 0;
+      cur = nxt;
+      if (e + 1 < e1) nxt = list[e + 1];
+    } else {
+      c0 += 32;
+    }
+  }
+  // sum the source groups (lanes ti, ti + W, ...)
+#pragma unroll
+  for (int o = W; o < 32; o <<= 1) {
+    P += __shfl_xor_sync(0xffffffffu, P, o);
+    Gx += __shfl_xor_sync(0xffffffffu, Gx, o);
+    Gy += __shfl_xor_sync(0xffffffffu, Gy, o);
+    Gz += __shfl_xor_sync(0xffffffffu, Gz, o);
+  }
+  if (active && grp == 0) {
+    const int b = it.boff + ti;
     phi[b] = P;
     grad[3 * b + 0] = -Gx;
     grad[3 * b + 1] = -Gy;
     grad[3 * b + 2] = -Gz;
+  }
+}
+
+__global__ void __launch_bounds__(32 * kP2PWarps, P2P_MINB)
+    k_p2p32(const float4* __restrict__ body32, const P2PItem32* __restrict__ items, int nitems,
+            const int* __restrict__ list_off, const P2PSrc32* __restrict__ list, double* __restrict__ phi,
+            double* __restrict__ grad) {
+  __shared__ float4 sbuf[kP2PWarps][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int item = blockIdx.x * kP2PWarps + warp;
+  if (item >= nitems) return;  // warp-uniform
+  const P2PItem32 it = items[item];
+  switch (it.lw) {
+    case 5: p2p32_item<1>(body32, it, list_off, list, sbuf[warp], lane, phi, grad); break;
+    case 4: p2p32_item<2>(body32, it, list_off, list, sbuf[warp], lane, phi, grad); break;
+    case 3: p2p32_item<4>(body32, it, list_off, list, sbuf[warp], lane, phi, grad); break;
+    default: p2p32_item<8>(body32, it, list_off, list, sbuf[warp], lane, phi, grad); break;
   }
 }
 
@@ -168,7 +254,7 @@ __global__ void __launch_bounds__(32 * kP2PWarps)
         // dx = x_t - (x_s + offset), as p2p_1toN_256 forms it (kernel.cpp:283-290)
         const double dx = xt.x - (b.x + src.ox), dy = xt.y - (b.y + src.oy), dz = xt.z - (b.z + src.oz);
         const double r2 = dx * dx + dy * dy + dz * dz;
-        const double ir = r2 > 0.0 ? rsqrt(r2) : 0.0;
+        const double ir = r2 > 0.0 ? rsqrt_nr<2>(r2) : 0.0;
         const double qir = b.w * ir;
         P += qir;
         const double q3 = qir * ir * ir;
@@ -189,48 +275,53 @@ __global__ void __launch_bounds__(32 * kP2PWarps)
 
 // ---------------------------------------------------------------------------
 // P2M: check-surface potential of each leaf's bodies (FP64).  Surface points
-// are unit * (2.95 r) + centre (kernel.cpp:336).
+// are unit * (2.95 r) + centre (kernel.cpp:336).  One block per leaf, two
+// surface points per thread, the block sized to the surface (160 threads for
+// the 296 points of P = 8) so that few lanes idle.
 // ---------------------------------------------------------------------------
 constexpr int kSurfThreads = 128;
-constexpr int kSurfPer = 4;
+constexpr int kCheckMaxThreads = 256;
+constexpr int kCheckPer = 2;
 
-__global__ void __launch_bounds__(kSurfThreads)
+template <int NR>
+__global__ void __launch_bounds__(kCheckMaxThreads)
     k_p2m_check(const double4* __restrict__ body64, const LeafInfo* __restrict__ leaves,
                 const double* __restrict__ surf_unit, int ns, double* __restrict__ out) {
-  __shared__ double4 sb[kSurfThreads];
+  __shared__ double4 sb[kCheckMaxThreads];
   const LeafInfo L = leaves[blockIdx.x];
   const double R = L.r * 2.95;
-  const int tid = threadIdx.x;
-  for (int i0 = 0; i0 < ns; i0 += kSurfThreads * kSurfPer) {
-    double yx[kSurfPer], yy[kSurfPer], yz[kSurfPer], acc[kSurfPer];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int i0 = 0; i0 < ns; i0 += nt * kCheckPer) {
+    double yx[kCheckPer], yy[kCheckPer], yz[kCheckPer], acc[kCheckPer];
 #pragma unroll
-    for (int k = 0; k < kSurfPer; ++k) {
-      const int i = i0 + tid + k * kSurfThreads;
+    for (int k = 0; k < kCheckPer; ++k) {
+      const int i = i0 + tid + k * nt;
       const int ii = i < ns ? i : 0;
       yx[k] = surf_unit[3 * ii + 0] * R + L.cx;
       yy[k] = surf_unit[3 * ii + 1] * R + L.cy;
       yz[k] = surf_unit[3 * ii + 2] * R + L.cz;
       acc[k] = 0.0;
     }
-    for (int b0 = 0; b0 < L.bnum; b0 += kSurfThreads) {
-      const int cnt = min(kSurfThreads, L.bnum - b0);
+    for (int b0 = 0; b0 < L.bnum; b0 += nt) {
+      const int cnt = min(nt, L.bnum - b0);
       __syncthreads();
       if (tid < cnt) sb[tid] = body64[L.boff + b0 + tid];
       __syncthreads();
+#pragma unroll 2
       for (int j = 0; j < cnt; ++j) {
         const double4 b = sb[j];
 #pragma unroll
-        for (int k = 0; k < kSurfPer; ++k) {
+        for (int k = 0; k < kCheckPer; ++k) {
           const double dx = yx[k] - b.x, dy = yy[k] - b.y, dz = yz[k] - b.z;
           const double r2 = dx * dx + dy * dy + dz * dz;
-          const double ir = r2 > 0.0 ? rsqrt(r2) : 0.0;
+          const double ir = r2 > 0.0 ? rsqrt_nr<NR>(r2) : 0.0;
           acc[k] += b.w * ir;
         }
       }
     }
 #pragma unroll
-    for (int k = 0; k < kSurfPer; ++k) {
-      const int i = i0 + tid + k * kSurfThreads;
+    for (int k = 0; k < kCheckPer; ++k) {
+      const int i = i0 + tid + k * nt;
       if (i < ns) out[(size_t)blockIdx.x * ns + i] = acc[k];
     }
   }
@@ -239,102 +330,160 @@ __global__ void __launch_bounds__(kSurfThreads)
 // ---------------------------------------------------------------------------
 // L2P: potential and gradient at each leaf's bodies from the downward
 // equivalent density on the 2.95 r surface (kernel.cpp:1461, 1469-1510), FP64.
+// One block per leaf.  A leaf with fewer bodies than threads splits the
+// surface points among G = threads / bnum groups of bnum threads (group g
+// takes points g, g+G, ...) and sums the groups in shared memory, so that a
+// 34-body leaf keeps 102 of 128 threads busy instead of 34.
 // ---------------------------------------------------------------------------
+template <int NR>
 __global__ void __launch_bounds__(kSurfThreads)
     k_l2p_eval(const double4* __restrict__ body64, const LeafInfo* __restrict__ leaves,
                const double* __restrict__ surf_unit, int ns, const double* __restrict__ q_down,
                double* __restrict__ phi, double* __restrict__ grad) {
   extern __shared__ double4 sy[];  // ns entries
+  __shared__ double red[4][kSurfThreads];
   const LeafInfo L = leaves[blockIdx.x];
   const double R = L.r * 2.95;
   for (int i = threadIdx.x; i < ns; i += blockDim.x)
     sy[i] = make_double4(surf_unit[3 * i] * R + L.cx, surf_unit[3 * i + 1] * R + L.cy,
                          surf_unit[3 * i + 2] * R + L.cz, q_down[(size_t)blockIdx.x * ns + i]);
   __syncthreads();
-  for (int t = threadIdx.x; t < L.bnum; t += blockDim.x) {
-    const double4 x = body64[L.boff + t];
+  const int bnum = L.bnum;
+  if (bnum <= 0) return;  // block-uniform
+  const int B = bnum < kSurfThreads ? bnum : kSurfThreads;
+  const int G = kSurfThreads / B;
+  const int grp = threadIdx.x / B, tl = threadIdx.x - grp * B;
+  for (int t0 = 0; t0 < bnum; t0 += B) {
     double p = 0, gx = 0, gy = 0, gz = 0;
-    for (int i = 0; i < ns; ++i) {
-      const double4 y = sy[i];
-      const double dx = x.x - y.x, dy = x.y - y.y, dz = x.z - y.z;
-      const double r2 = dx * dx + dy * dy + dz * dz;
-      const double ir = r2 > 0.0 ? rsqrt(r2) : 0.0;
-      const double qir = y.w * ir;
-      p += qir;
-      const double q3 = qir * ir * ir;
-      gx += q3 * dx;
-      gy += q3 * dy;
-      gz += q3 * dz;
+    const int t = t0 + tl;
+    if (grp < G && t < bnum) {
+      const double4 x = body64[L.boff + t];
+      for (int i = grp; i < ns; i += G) {
+        const double4 y = sy[i];
+        const double dx = x.x - y.x, dy = x.y - y.y, dz = x.z - y.z;
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        const double ir = r2 > 0.0 ? rsqrt_nr<NR>(r2) : 0.0;
+        const double qir = y.w * ir;
+        p += qir;
+        const double q3 = qir * ir * ir;
+        gx += q3 * dx;
+        gy += q3 * dy;
+        gz += q3 * dz;
+      }
     }
-    const int b = L.boff + t;
-    phi[b] = p;
-    grad[3 * b + 0] = -gx;
-    grad[3 * b + 1] = -gy;
-    grad[3 * b + 2] = -gz;
+    if (G > 1) {
+      red[0][threadIdx.x] = p;
+      red[1][threadIdx.x] = gx;
+      red[2][threadIdx.x] = gy;
+      red[3][threadIdx.x] = gz;
+      __syncthreads();
+      if (grp == 0) {
+        for (int g2 = 1; g2 < G; ++g2) {
+          const int o = g2 * B + tl;
+          p += red[0][o];
+          gx += red[1][o];
+          gy += red[2][o];
+          gz += red[3][o];
+        }
+      }
+      __syncthreads();
+    }
+    if (grp == 0 && t < bnum) {
+      const int b = L.boff + t;
+      phi[b] = p;
+      grad[3 * b + 0] = -gx;
+      grad[3 * b + 1] = -gy;
+      grad[3 * b + 2] = -gz;
+    }
   }
 }
 
 // ---------------------------------------------------------------------------
 // Batched FP64 operator application:
 //   C[outrow[r]][n] = beta*C + scale[r] * sum_s sum_j A[inrow[r*S+s]][j] B[g][s][j][n]
-// 64x64 output tiles, 16-deep K steps, 4x4 outputs per thread.
+// 128x64 output tiles, 16-deep K steps, 8x4 outputs per thread; the next K
+// step's A rows (gathered through inrow) and B panel are loaded into
+// registers while the current step is multiplied out of shared memory.
 // ---------------------------------------------------------------------------
-constexpr int kTM = 64, kTN = 64, kTK = 16;
+constexpr int kTM = APPLY_TM, kTN = 64, kTK = 16;
+constexpr int kRPT = kTM / 16;  // output rows per thread
 
-__global__ void __launch_bounds__(256) k_apply_f64(ApplyBatch b) {
+__global__ void __launch_bounds__(256, 2) k_apply_f64(ApplyBatch b) {
   __shared__ double As[kTK][kTM + 1];
   __shared__ double Bs[kTK][kTN];
-  __shared__ int rsrc[kTM];
   const int g = blockIdx.z;
   const int rbeg = b.group_off[g], rend = b.group_off[g + 1];
   const int r0 = rbeg + blockIdx.y * kTM;
   const int c0 = blockIdx.x * kTN;
   if (r0 >= rend) return;  // block-uniform
-  const int ns = b.ns;
-  const double* Bg = b.B + (size_t)g * b.S * ns * ns;
+  const int ns = b.ns, S = b.S;
+  const double* Bg = b.B + (size_t)g * S * ns * ns;
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  double acc[4][4];
+  const int nkt = (ns + kTK - 1) / kTK, total = S * nkt;
+  // this thread loads A rows ty + 16u (the rows it also writes) at k = tx,
+  // and B elements tid + 256u of the 16x64 panel
+  int src[kRPT];
+  double ra[kRPT], rb[4];
+  int s_cur = 0;
+  auto load_src = [&](int s) {
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+    for (int u = 0; u < kRPT; ++u) {
+      const int row = r0 + ty + 16 * u;
+      src[u] = row < rend ? b.inrow[(size_t)row * S + s] : -1;
+    }
+  };
+  auto fetch = [&](int kt) {
+    const int s = kt / nkt, j0 = (kt - s * nkt) * kTK;
+    const int j = j0 + tx;
+#pragma unroll
+    for (int u = 0; u < kRPT; ++u) ra[u] = (src[u] >= 0 && j < ns) ? b.A[(size_t)src[u] * ns + j] : 0.0;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int e = tid + 256 * u;
+      const int jj = j0 + (e >> 6), n = c0 + (e & 63);
+      rb[u] = (jj < ns && n < ns) ? Bg[((size_t)s * ns + jj) * ns + n] : 0.0;
+    }
+  };
+  double acc[kRPT][4];
+#pragma unroll
+  for (int i = 0; i < kRPT; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-  for (int s = 0; s < b.S; ++s) {
+  load_src(0);
+  fetch(0);
+  for (int kt = 0; kt < total; ++kt) {
     __syncthreads();
-    if (tid < kTM) {
-      const int row = r0 + tid;
-      rsrc[tid] = row < rend ? b.inrow[(size_t)row * b.S + s] : -1;
+#pragma unroll
+    for (int u = 0; u < kRPT; ++u) As[tx][ty + 16 * u] = ra[u];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int e = tid + 256 * u;
+      Bs[e >> 6][e & 63] = rb[u];
     }
     __syncthreads();
-    for (int j0 = 0; j0 < ns; j0 += kTK) {
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int e = tid + 256 * u;
-        const int r = e >> 4, k = e & 15;
-        const int src = rsrc[r];
-        const int j = j0 + k;
-        As[k][r] = (src >= 0 && j < ns) ? b.A[(size_t)src * ns + j] : 0.0;
-        const int kk = e >> 6, c = e & 63;
-        const int jj = j0 + kk, n = c0 + c;
-        Bs[kk][c] = (jj < ns && n < ns) ? Bg[((size_t)s * ns + jj) * ns + n] : 0.0;
+    if (kt + 1 < total) {
+      const int s_next = (kt + 1) / nkt;
+      if (s_next != s_cur) {
+        s_cur = s_next;
+        load_src(s_next);
       }
-      __syncthreads();
+      fetch(kt + 1);
+    }
 #pragma unroll
-      for (int k = 0; k < kTK; ++k) {
-        double a[4], bb[4];
+    for (int k = 0; k < kTK; ++k) {
+      double a[kRPT], bb[4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) a[i] = As[k][ty + 16 * i];
+      for (int i = 0; i < kRPT; ++i) a[i] = As[k][ty + 16 * i];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) bb[j] = Bs[k][tx + 16 * j];
+      for (int j = 0; j < 4; ++j) bb[j] = Bs[k][tx + 16 * j];
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < kRPT; ++i)
 #pragma unroll
-          for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], bb[j], acc[i][j]);
-      }
-      __syncthreads();
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], bb[j], acc[i][j]);
     }
   }
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
+  for (int i = 0; i < kRPT; ++i) {
     const int row = r0 + ty + 16 * i;
     if (row >= rend) continue;
     const int o = b.outrow[row];
@@ -479,86 +628,155 @@ __global__ void __launch_bounds__(256)
 
 // Hadamard 8x8 (hadamard_8x8 + c2c_8x8x2_avx, kernel.cpp:1012-1082, c2c.h:201-296):
 //   Pk[f][t][itar] = sum_d sum_isrc G[f][d][isrc][itar] * Q[f][src(t,d)][isrc]
-// One thread per (target, frequency); a block holds one frequency's 26x64
-// kernel coefficients in shared memory, so every coefficient read is a
-// broadcast, and each (target, direction) reads one 64-byte source row.
-// FP32 partial sums per direction are accumulated into FP64.
-constexpr int kHadThreads = 256;
+// A block holds one frequency's 26x64 kernel coefficients in shared memory
+// (every coefficient read is a broadcast) and each thread owns TT targets of
+// that frequency: one coefficient read feeds TT targets, and each (target,
+// direction) reads one 64-byte source row with sector loads.  L1 wavefronts
+// per FMA fall as 1/(4 TT) + 1/16, which is what bounds this kernel.
+// FP32 partial sums over DF directions are accumulated into FP64.
+template <typename T> struct HadCfg;
+template <> struct HadCfg<float> {
+  static constexpr int TT = HAD_TT, DF = HAD_DF, THREADS = 256 / HAD_TT, MINB = HAD_MINB;
+};
+template <> struct HadCfg<double> {
+  static constexpr int TT = 1, DF = 1, THREADS = 256, MINB = 1;
+};
 
 template <typename T>
-__global__ void __launch_bounds__(kHadThreads, sizeof(T) == 4 ? 2 : 1)
+__device__ __forceinline__ void load_row8(const T* qrow, typename Cplx<T>::type (&q)[8]) {
+  constexpr int kPer = 32 / sizeof(T);  // values per 32-byte sector
+#pragma unroll
+  for (int c = 0; c < 16 / kPer; ++c) {
+    T v[kPer];
+    ld_sector(qrow + c * kPer, v);
+#pragma unroll
+    for (int k = 0; k < kPer / 2; ++k) {
+      q[c * kPer / 2 + k].x = v[2 * k];
+      q[c * kPer / 2 + k].y = v[2 * k + 1];
+    }
+  }
+}
+
+template <typename T, int TT>
+__device__ __forceinline__ void had_rows(const typename Cplx<T>::type* __restrict__ Qf, const int (&sd)[TT],
+                                         typename Cplx<T>::type (&q)[TT][8]) {
+#pragma unroll
+  for (int u = 0; u < TT; ++u) {
+    if (sd[u] >= 0) {
+      load_row8<T>(reinterpret_cast<const T*>(Qf + (size_t)sd[u] * 8), q[u]);
+    } else {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) q[u][i].x = q[u][i].y = T(0);
+    }
+  }
+}
+
+template <typename T, int TT>
+__device__ __forceinline__ void had_index(const int* __restrict__ tsrcT, int d, int t0, int nt, int ntar,
+                                          int (&sd)[TT]) {
+#pragma unroll
+  for (int u = 0; u < TT; ++u) {
+    const int t = t0 + u * nt;
+    sd[u] = t < ntar ? tsrcT[d * ntar + t] : -1;
+  }
+}
+
+template <typename T, int TT>
+__device__ __forceinline__ void had_mac(const typename Cplx<T>::type* __restrict__ g, const int (&sd)[TT],
+                                        const typename Cplx<T>::type (&q)[TT][8], T (&pr)[TT][8], T (&pi)[TT][8]) {
+  bool any = false;
+#pragma unroll
+  for (int u = 0; u < TT; ++u) any |= sd[u] >= 0;
+  if (!any) return;
+#pragma unroll
+  for (int isrc = 0; isrc < 8; ++isrc)
+#pragma unroll
+    for (int itar = 0; itar < 8; itar += 2) {
+      const typename Cplx2<T>::type gv = *reinterpret_cast<const typename Cplx2<T>::type*>(g + isrc * 8 + itar);
+#pragma unroll
+      for (int u = 0; u < TT; ++u) {
+        cmad(pr[u][itar], pi[u][itar], gv.x, gv.y, q[u][isrc].x, q[u][isrc].y);
+        cmad(pr[u][itar + 1], pi[u][itar + 1], gv.z, gv.w, q[u][isrc].x, q[u][isrc].y);
+      }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(HadCfg<T>::THREADS, HadCfg<T>::MINB)
     k_m2l_hadamard8(const T* __restrict__ Q, const T* __restrict__ G, const int* __restrict__ tsrcT, int ntar,
                     int nsrc, int Nf, T* __restrict__ Pk) {
   using C2 = typename Cplx<T>::type;
+  constexpr int TT = HadCfg<T>::TT, DF = HadCfg<T>::DF, NT = HadCfg<T>::THREADS;
   __shared__ __align__(32) C2 Gs[26 * 64];
   const int f = blockIdx.y;
   const C2* Gf = reinterpret_cast<const C2*>(G) + (size_t)f * 26 * 64;
-  for (int e = threadIdx.x; e < 26 * 64; e += kHadThreads) Gs[e] = Gf[e];
-  __syncthreads();
-  const int t = blockIdx.x * kHadThreads + threadIdx.x;
-  if (t >= ntar) return;
-  double ar[8], ai[8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) ar[i] = ai[i] = 0.0;
+  for (int e = threadIdx.x; e < 26 * 64; e += NT) Gs[e] = Gf[e];
+  // targets of this thread: t0 + u * NT, u < TT (coalesced tsrcT reads)
+  const int t0 = blockIdx.x * NT * TT + threadIdx.x;
   const C2* Qf = reinterpret_cast<const C2*>(Q) + (size_t)f * nsrc * 8;
-  constexpr int kPer = 32 / sizeof(T);  // values per 32-byte sector
-  // directions in pairs: both source rows are in flight together, and one
-  // FP64 accumulation follows the two FP32 partial sums
-  for (int d0 = 0; d0 < 26; d0 += 2) {
-    int sd[2];
-    sd[0] = tsrcT[d0 * ntar + t];
-    sd[1] = tsrcT[(d0 + 1) * ntar + t];
-    if (sd[0] < 0 && sd[1] < 0) continue;
-    C2 q[2][8];
+  // two-stage pipeline over directions: the source rows of direction d+1
+  // are in flight while direction d is multiplied, and the row indices run
+  // one direction further ahead
+  int ia[TT], ib[TT];
+  C2 qa[TT][8], qb[TT][8];
+  if (t0 < ntar) {
+    had_index<T, TT>(tsrcT, 0, t0, NT, ntar, ia);
+    had_rows<T, TT>(Qf, ia, qa);
+    had_index<T, TT>(tsrcT, 1, t0, NT, ntar, ib);
+  }
+  __syncthreads();
+  if (t0 >= ntar) return;
+  double ar[TT][8], ai[TT][8];
+  T pr[TT][8], pi[TT][8];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      if (sd[h] < 0) {
-#pragma unroll
-        for (int i = 0; i < 8; ++i) q[h][i].x = q[h][i].y = T(0);
-        continue;
-      }
-      const T* qrow = reinterpret_cast<const T*>(Qf + (size_t)sd[h] * 8);
-#pragma unroll
-      for (int c = 0; c < 16 / kPer; ++c) {
-        T v[kPer];
-        ld_sector(qrow + c * kPer, v);
-#pragma unroll
-        for (int k = 0; k < kPer / 2; ++k) {
-          q[h][c * kPer / 2 + k].x = v[2 * k];
-          q[h][c * kPer / 2 + k].y = v[2 * k + 1];
-        }
-      }
-    }
-    T pr[8], pi[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) pr[i] = pi[i] = T(0);
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      if (sd[h] < 0) continue;
-      const C2* g = Gs + (d0 + h) * 64;
-#pragma unroll
-      for (int isrc = 0; isrc < 8; ++isrc)
-#pragma unroll
-        for (int itar = 0; itar < 8; itar += 2) {
-          const typename Cplx2<T>::type gv =
-              *reinterpret_cast<const typename Cplx2<T>::type*>(g + isrc * 8 + itar);
-          cmad(pr[itar], pi[itar], gv.x, gv.y, q[h][isrc].x, q[h][isrc].y);
-          cmad(pr[itar + 1], pi[itar + 1], gv.z, gv.w, q[h][isrc].x, q[h][isrc].y);
-        }
-    }
+  for (int u = 0; u < TT; ++u)
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      ar[i] += (double)pr[i];
-      ai[i] += (double)pi[i];
+      ar[u][i] = ai[u][i] = 0.0;
+      pr[u][i] = pi[u][i] = T(0);
+    }
+  auto flush = [&]() {
+#pragma unroll
+    for (int u = 0; u < TT; ++u)
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        ar[u][i] += (double)pr[u][i];
+        ai[u][i] += (double)pi[u][i];
+        pr[u][i] = pi[u][i] = T(0);
+      }
+  };
+  for (int d = 0; d < 26; d += 2) {
+    int ja[TT];
+    had_rows<T, TT>(Qf, ib, qb);
+    if (d + 2 < 26) had_index<T, TT>(tsrcT, d + 2, t0, NT, ntar, ja);
+    had_mac<T, TT>(Gs + d * 64, ia, qa, pr, pi);
+    if (DF == 1 || (d + 1) % DF == 0) flush();
+    if (d + 2 < 26) {
+#pragma unroll
+      for (int u = 0; u < TT; ++u) ia[u] = ja[u];
+      had_rows<T, TT>(Qf, ia, qa);
+    }
+    int jb[TT];
+    if (d + 3 < 26) had_index<T, TT>(tsrcT, d + 3, t0, NT, ntar, jb);
+    had_mac<T, TT>(Gs + (d + 1) * 64, ib, qb, pr, pi);
+    if ((d + 2) % DF == 0 || d + 2 == 26) flush();
+    if (d + 3 < 26) {
+#pragma unroll
+      for (int u = 0; u < TT; ++u) ib[u] = jb[u];
     }
   }
-  C2* out = reinterpret_cast<C2*>(Pk) + ((size_t)f * ntar + t) * 8;
 #pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    C2 v;
-    v.x = (T)ar[i];
-    v.y = (T)ai[i];
-    out[i] = v;
+  for (int u = 0; u < TT; ++u) {
+    const int t = t0 + u * NT;
+    if (t >= ntar) break;
+    C2* out = reinterpret_cast<C2*>(Pk) + ((size_t)f * ntar + t) * 8;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      C2 v;
+      v.x = (T)ar[u][i];
+      v.y = (T)ai[u][i];
+      out[i] = v;
+    }
   }
 }
 
@@ -766,12 +984,11 @@ cudaError_t launch_prep32(const double4* body64, const int* body_leaf, const Lea
   return cudaGetLastError();
 }
 
-cudaError_t launch_p2p32(const float4* body32, const LeafInfo* leaves, const P2PItem* items, int nitems,
-                         const int* list_off, const P2PSrc32* list, double* phi, double* grad,
-                         cudaStream_t st) {
+cudaError_t launch_p2p32(const float4* body32, const P2PItem32* items, int nitems, const int* list_off,
+                         const P2PSrc32* list, double* phi, double* grad, cudaStream_t st) {
   if (nitems > 0)
-    k_p2p32<<<cdiv(nitems, kP2PWarps), 32 * kP2PWarps, 0, st>>>(body32, leaves, items, nitems, list_off,
-                                                               list, phi, grad);
+    k_p2p32<<<cdiv(nitems, kP2PWarps), 32 * kP2PWarps, 0, st>>>(body32, items, nitems, list_off, list, phi,
+                                                               grad);
   return cudaGetLastError();
 }
 
@@ -785,23 +1002,36 @@ cudaError_t launch_p2p64(const double4* body64, const LeafInfo* leaves, const P2
 }
 
 cudaError_t launch_p2m_check(const double4* body64, const LeafInfo* leaves, int nleaf,
-                             const double* surf_unit, int ns, double* out, cudaStream_t st) {
-  if (nleaf > 0) k_p2m_check<<<nleaf, kSurfThreads, 0, st>>>(body64, leaves, surf_unit, ns, out);
+                             const double* surf_unit, int ns, double* out, cudaStream_t st, int newton) {
+  if (nleaf > 0) {
+    const int per = cdiv(ns, kCheckPer);
+    const int nt = per >= kCheckMaxThreads ? kCheckMaxThreads : cdiv(per, 32) * 32;
+    if (newton == 1)
+      k_p2m_check<1><<<nleaf, nt, 0, st>>>(body64, leaves, surf_unit, ns, out);
+    else
+      k_p2m_check<2><<<nleaf, nt, 0, st>>>(body64, leaves, surf_unit, ns, out);
+  }
+  return cudaGetLastError();
+}
+
+template <int NR>
+static cudaError_t l2p_nr(const double4* body64, const LeafInfo* leaves, int nleaf, const double* surf_unit, int ns,
+                          const double* q_down, double* phi, double* grad, cudaStream_t st) {
+  const size_t sm = sizeof(double4) * ns;
+  if (sm > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_l2p_eval<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+  }
+  k_l2p_eval<NR><<<nleaf, kSurfThreads, sm, st>>>(body64, leaves, surf_unit, ns, q_down, phi, grad);
   return cudaGetLastError();
 }
 
 cudaError_t launch_l2p_eval(const double4* body64, const LeafInfo* leaves, int nleaf,
                             const double* surf_unit, int ns, const double* q_down, double* phi,
-                            double* grad, cudaStream_t st) {
-  if (nleaf > 0) {
-    const size_t sm = sizeof(double4) * ns;
-    if (sm > 48 * 1024) {
-      cudaError_t e = cudaFuncSetAttribute(k_l2p_eval, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      if (e != cudaSuccess) return e;
-    }
-    k_l2p_eval<<<nleaf, kSurfThreads, sm, st>>>(body64, leaves, surf_unit, ns, q_down, phi, grad);
-  }
-  return cudaGetLastError();
+                            double* grad, cudaStream_t st, int newton) {
+  if (nleaf <= 0) return cudaGetLastError();
+  return newton == 1 ? l2p_nr<1>(body64, leaves, nleaf, surf_unit, ns, q_down, phi, grad, st)
+                     : l2p_nr<2>(body64, leaves, nleaf, surf_unit, ns, q_down, phi, grad, st);
 }
 
 cudaError_t launch_apply(const ApplyBatch& b, cudaStream_t st) {
@@ -878,8 +1108,9 @@ template <typename T>
 cudaError_t launch_m2l_hadamard8(const T* Q, const T* G, const int* tsrcT, int ntar, int nsrc, int Nf, T* Pk,
                                  cudaStream_t st) {
   if (ntar > 0) {
-    dim3 grid(cdiv(ntar, kHadThreads), Nf);
-    k_m2l_hadamard8<T><<<grid, kHadThreads, 0, st>>>(Q, G, tsrcT, ntar, nsrc, Nf, Pk);
+    constexpr int NT = HadCfg<T>::THREADS, TT = HadCfg<T>::TT;
+    dim3 grid(cdiv(ntar, NT * TT), Nf);
+    k_m2l_hadamard8<T><<<grid, NT, 0, st>>>(Q, G, tsrcT, ntar, nsrc, Nf, Pk);
   }
   return cudaGetLastError();
 }

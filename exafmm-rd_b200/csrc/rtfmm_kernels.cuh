@@ -16,19 +16,30 @@ struct LeafInfo {
   int boff, bnum;      // bodies in tree order
 };
 
-// P2P work item: a block of targets of one leaf (64 for the FP32 kernel, 32
-// for the FP64 kernel).
+// P2P work item of the FP64 kernel: 32 targets of one leaf.
 struct P2PItem {
   int leaf;   // leaf-table index of the target leaf
   int t0;     // first target (offset inside the leaf)
 };
 
-// One P2P list entry (source leaf) of a target leaf, both precisions.
-struct P2PSrc32 {
+// P2P work item of the FP32 kernel: nt <= W targets of one leaf, W = 1 << lw
+// lanes per target group; the 32/W groups of a warp split every source tile
+// between them, so a leaf's last few targets do not leave most lanes idle.
+struct P2PItem32 {
+  int leaf;   // leaf-table index of the target leaf (its source list)
+  int boff;   // first target body (tree order)
+  int nt;     // targets in this item (1..W)
+  int lw;     // log2 W, W in {4, 8, 16, 32}
+};
+
+// One P2P list entry (source leaf) of a target leaf, FP32 form.  Carries the
+// source's body range so that the kernel reads bodies with one dependent load.
+struct alignas(16) P2PSrc32 {
   float dx, dy, dz;   // c_src + offset - c_tar, for leaf-relative FP32 positions
   int leaf;           // leaf-table index of the source leaf
   int self;           // source == target with zero offset (mask r == 0)
-  int pad[3];
+  int boff, bnum;     // source bodies (tree order)
+  int pad;
 };
 struct P2PSrc64 {
   double ox, oy, oz;  // periodic offset added to the source positions
@@ -52,14 +63,15 @@ struct ApplyBatch {
 // Launch helpers (all asynchronous on `st`; return cudaGetLastError()).
 cudaError_t launch_prep32(const double4* body64, const int* body_leaf, const LeafInfo* leaves,
                           float4* body32, int n, cudaStream_t st);
-cudaError_t launch_p2p32(const float4* body32, const LeafInfo* leaves, const P2PItem* items, int nitems,
-                         const int* list_off, const P2PSrc32* list, double* phi, double* grad,
-                         cudaStream_t st);
+cudaError_t launch_p2p32(const float4* body32, const P2PItem32* items, int nitems, const int* list_off,
+                         const P2PSrc32* list, double* phi, double* grad, cudaStream_t st);
 cudaError_t launch_p2p64(const double4* body64, const LeafInfo* leaves, const P2PItem* items, int nitems,
                          const int* list_off, const P2PSrc64* list, double* phi, double* grad,
                          cudaStream_t st);
+// newton: Newton steps of the FP64 reciprocal square root (1: ~1e-13, for
+// the FP32-mixed form; 2: full FP64)
 cudaError_t launch_p2m_check(const double4* body64, const LeafInfo* leaves, int nleaf,
-                             const double* surf_unit, int ns, double* out, cudaStream_t st);
+                             const double* surf_unit, int ns, double* out, cudaStream_t st, int newton = 2);
 cudaError_t launch_apply(const ApplyBatch& b, cudaStream_t st);
 // q[parent] = sum of Y[child] over the parent's children; `list` holds
 // (parent, coff, cnum) triplets
@@ -87,7 +99,7 @@ cudaError_t launch_m2l_down(const T* Pk, const int* items, const double* tscale,
                             double* p_check, cudaStream_t st);
 cudaError_t launch_l2p_eval(const double4* body64, const LeafInfo* leaves, int nleaf,
                             const double* surf_unit, int ns, const double* q_down, double* phi,
-                            double* grad, cudaStream_t st);
+                            double* grad, cudaStream_t st, int newton = 2);
 cudaError_t launch_dipole(const double4* body64, int n, double* partial /*>= 4*1024*/, cudaStream_t st);
 cudaError_t launch_post(const double* phi_far, const double* grad_far, const double* phi_near,
                         const double* grad_near, const double4* body64, const int64_t* perm, int n,
