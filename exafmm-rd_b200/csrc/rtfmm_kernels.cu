@@ -19,10 +19,13 @@
 
 // FP32 P2P: inner unroll and resident blocks per SM
 #ifndef P2P_UNROLL
-#define P2P_UNROLL 8
+#define P2P_UNROLL 4
 #endif
 #ifndef P2P_MINB
 #define P2P_MINB 6
+#endif
+#ifndef P2P_PACKED
+#define P2P_PACKED 1
 #endif
 // FP32 Hadamard: targets per thread, directions per FP32 partial sum,
 // resident blocks per SM
@@ -35,9 +38,13 @@
 #ifndef HAD_MINB
 #define HAD_MINB 2
 #endif
-// FP64 operator application: output rows per block (64 or 128)
+// FP64 operator application: output rows per block (64 or 128), FP64
+// tensor-core (mma.sync) inner product
 #ifndef APPLY_TM
 #define APPLY_TM 64
+#endif
+#ifndef APPLY_MMA
+#define APPLY_MMA 0
 #endif
 
 namespace rtfmm_b200 {
@@ -136,6 +143,37 @@ __device__ __forceinline__ void p2p32_tile(const float4* __restrict__ s, int k0,
   }
 }
 
+// The same over source pairs with packed FP32x2 arithmetic (sm_100
+// FADD2/FMUL2/FFMA2): the tile is held as 16 pairs, pair k at s[2k] =
+// (-x, -x', -y, -y') and s[2k+1] = (-z, -z', q, q'); lanes of group k0 take
+// pairs k0, k0+G, ...  Per pair the arithmetic and its rounding are those of
+// p2p32_tile; only the sum over sources is split into two interleaved halves.
+template <int G, bool MASK>
+__device__ __forceinline__ void p2p32_tile2(const float4* __restrict__ s, int k0, int npair, float2 px, float2 py,
+                                            float2 pz, float2& p, float2& fx, float2& fy, float2& fz) {
+#pragma unroll kP2PUnroll
+  for (int k = k0; k < npair; k += G) {
+    const float4 u = s[2 * k], v = s[2 * k + 1];
+    const float2 dx = __fadd2_rn(px, make_float2(u.x, u.y));
+    const float2 dy = __fadd2_rn(py, make_float2(u.z, u.w));
+    const float2 dz = __fadd2_rn(pz, make_float2(v.x, v.y));
+    float2 r2 = __fmul2_rn(dz, dz);
+    r2 = __ffma2_rn(dy, dy, r2);
+    r2 = __ffma2_rn(dx, dx, r2);
+    float2 ir = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+    if (MASK) {
+      ir.x = r2.x > 0.f ? ir.x : 0.f;
+      ir.y = r2.y > 0.f ? ir.y : 0.f;
+    }
+    const float2 qir = __fmul2_rn(make_float2(v.z, v.w), ir);
+    p = __fadd2_rn(p, qir);
+    const float2 q3 = __fmul2_rn(__fmul2_rn(qir, ir), ir);
+    fx = __ffma2_rn(q3, dx, fx);
+    fy = __ffma2_rn(q3, dy, fy);
+    fz = __ffma2_rn(q3, dz, fz);
+  }
+}
+
 // One work item: W = 32/G lanes per target group, G groups per warp.
 template <int G>
 __device__ __forceinline__ void p2p32_item(const float4* __restrict__ body32, const P2PItem32& it,
@@ -146,43 +184,75 @@ __device__ __forceinline__ void p2p32_item(const float4* __restrict__ body32, co
   const int grp = lane / W, ti = lane % W;
   const bool active = ti < it.nt;
   const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+  // tile padding: no charge, far from every target (finite 1/r)
+  const float4 pad = make_float4(1e18f, 1e18f, 1e18f, 0.f);
   const float4 xt = active ? body32[it.boff + ti] : zero;
   double P = 0.0, Gx = 0.0, Gy = 0.0, Gz = 0.0;
   int e = list_off[it.leaf];
   const int e1 = list_off[it.leaf + 1];
   P2PSrc32 cur{}, nxt{};
-  float4 stage = zero;
+  float4 stage = pad;
   if (e < e1) {
     cur = list[e];
     if (lane < cur.bnum) stage = body32[cur.boff + lane];
   }
   if (e + 1 < e1) nxt = list[e + 1];
   int c0 = 0;
+#if P2P_PACKED
+  float2 p = make_float2(0.f, 0.f), fx = p, fy = p, fz = p;
+  float* sf = reinterpret_cast<float*>(sw) + 8 * (lane >> 1) + (lane & 1);
+#else
   float p = 0.f, fx = 0.f, fy = 0.f, fz = 0.f;
+#endif
   while (e < e1) {
     const int cnt = min(32, cur.bnum - c0);
     __syncwarp();
+#if P2P_PACKED
+    sf[0] = -stage.x;
+    sf[2] = -stage.y;
+    sf[4] = -stage.z;
+    sf[6] = stage.w;
+#else
     sw[lane] = stage;
+#endif
     __syncwarp();
     // next tile: the rest of this source leaf, else the first of the next
     const bool last = c0 + 32 >= cur.bnum;
-    stage = zero;
+    stage = pad;
     if (!last) {
       if (lane < cur.bnum - c0 - 32) stage = body32[cur.boff + c0 + 32 + lane];
     } else if (e + 1 < e1) {
       if (lane < nxt.bnum) stage = body32[nxt.boff + lane];
     }
     const float px = xt.x - cur.dx, py = xt.y - cur.dy, pz = xt.z - cur.dz;
+#if P2P_PACKED
+    const int npair = (cnt + 1) >> 1;
+    if (cur.self)
+      p2p32_tile2<G, true>(sw, grp, npair, make_float2(px, px), make_float2(py, py), make_float2(pz, pz), p, fx,
+                           fy, fz);
+    else
+      p2p32_tile2<G, false>(sw, grp, npair, make_float2(px, px), make_float2(py, py), make_float2(pz, pz), p, fx,
+                            fy, fz);
+#else
     if (cur.self)
       p2p32_tile<G, true>(sw, grp, cnt, px, py, pz, p, fx, fy, fz);
     else
       p2p32_tile<G, false>(sw, grp, cnt, px, py, pz, p, fx, fy, fz);
+#endif
     if (last) {
+#if P2P_PACKED
+      P += (double)p.x + (double)p.y;
+      Gx += (double)fx.x + (double)fx.y;
+      Gy += (double)fy.x + (double)fy.y;
+      Gz += (double)fz.x + (double)fz.y;
+      p = fx = fy = fz = make_float2(0.f, 0.f);
+#else
       P += (double)p;
       Gx += (double)fx;
       Gy += (double)fy;
       Gz += (double)fz;
       p = fx = fy = fz = 0.f;
+#endif
       ++e;
       c0 = 0;
       cur = nxt;
@@ -444,11 +514,21 @@ __global__ void __launch_bounds__(256, 2) k_apply_f64(ApplyBatch b) {
       rb[u] = (jj < ns && n < ns) ? Bg[((size_t)s * ns + jj) * ns + n] : 0.0;
     }
   };
+#if APPLY_MMA
+  static_assert(kTM == 64, "the tensor-core path tiles 64 rows as 2 x 4 warps");
+  const int lane = tid & 31, wm = (tid >> 5) & 1, wn = tid >> 6;
+  double dacc[4][2][2];
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt) dacc[mt][nt][0] = dacc[mt][nt][1] = 0.0;
+#else
   double acc[kRPT][4];
 #pragma unroll
   for (int i = 0; i < kRPT; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+#endif
   load_src(0);
   fetch(0);
   for (int kt = 0; kt < total; ++kt) {
@@ -469,6 +549,46 @@ __global__ void __launch_bounds__(256, 2) k_apply_f64(ApplyBatch b) {
       }
       fetch(kt + 1);
     }
+#if APPLY_MMA
+    // FP64 tensor-core steps: mma.sync m8n8k4 over this warp's 32x16 block
+    // (4 x 2 tiles of 8x8).  Fragments: A[m][k] at m = lane/4, k = lane%4;
+    // B[k][n] at k = lane%4, n = lane/4; D[m][n] at m = lane/4,
+    // n = 2 (lane%4) + {0, 1}.
+#pragma unroll
+    for (int k4 = 0; k4 < kTK; k4 += 4) {
+      double fa[4], fb[2];
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt) fa[mt] = As[k4 + (lane & 3)][wm * 32 + mt * 8 + (lane >> 2)];
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt) fb[nt] = Bs[k4 + (lane & 3)][wn * 16 + nt * 8 + (lane >> 2)];
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt)
+          asm volatile(
+              "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+              : "+d"(dacc[mt][nt][0]), "+d"(dacc[mt][nt][1])
+              : "d"(fa[mt]), "d"(fb[nt]));
+    }
+  }
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt) {
+    const int row = r0 + wm * 32 + mt * 8 + (lane >> 2);
+    if (row >= rend) continue;
+    const int o = b.outrow[row];
+    const double sc = b.scale ? b.scale[row] : 1.0;
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int n = c0 + wn * 16 + nt * 8 + 2 * (lane & 3) + i;
+        if (n >= ns) continue;
+        double* cp = b.C + (size_t)o * ns + n;
+        *cp = b.beta ? *cp + sc * dacc[mt][nt][i] : sc * dacc[mt][nt][i];
+      }
+  }
+}
+#else
 #pragma unroll
     for (int k = 0; k < kTK; ++k) {
       double a[kRPT], bb[4];
@@ -497,6 +617,7 @@ __global__ void __launch_bounds__(256, 2) k_apply_f64(ApplyBatch b) {
     }
   }
 }
+#endif
 
 // Sibling sum of the per-child M2M products, in crange order
 // (m2m_precompute accumulates child by child, kernel.cpp:398-403).
