@@ -277,20 +277,44 @@ def run_ours(args):
         e2e.append(time.perf_counter() - t0)
     barrier()
 
-    # forward + adjoint through the C ABI (host buffers), both precisions:
-    # the north-star comparison of the mixed and FP64 forms on the full step
+    # forward + adjoint, both precisions: the comparison of the mixed and
+    # FP64 forms on the full step.  Device-resident (CUDA events on the
+    # solver's stream; the adjoint reuses the forward pass's gradient), and
+    # through the host-buffer C ABI (wall clock) beside it.
     wts = np.random.default_rng(4).standard_normal(n)
+    w_dev = torch.from_numpy(wts).cuda()
+    dq_dev = torch.empty(n, dtype=torch.float64, device="cuda")
+    dx_dev = torch.empty((n, 3), dtype=torch.float64, device="cuda")
 
-    def fwd_adj(f):
+    def fwd_adj_dev(f):
+        f.flush_l2()
+        t = f.evaluate_device()
+        return t + f.adjoint_device(w_dev.data_ptr(), dq_dev.data_ptr(), dx_dev.data_ptr())
+
+    def fwd_adj_host(f):
         t0 = time.perf_counter()
         f.evaluate(q)
         f.adjoint(wts)
-        return time.perf_counter() - t0
+        return 1000 * (time.perf_counter() - t0)
 
-    fwd_adj(fm)
-    fwd_adj(f64)
-    fa_m = float(np.mean([fwd_adj(fm) for _ in range(3)]))
-    fa_d = float(np.mean([fwd_adj(f64) for _ in range(3)]))
+    for f in (fm, f64):
+        fwd_adj_dev(f)
+        fwd_adj_host(f)
+    fa_m = float(np.mean([fwd_adj_dev(fm) for _ in range(max(3, args.steps // 2))]))
+    fa_d = float(np.mean([fwd_adj_dev(f64) for _ in range(max(3, args.steps // 2))]))
+    fh_m = float(np.mean([fwd_adj_host(fm) for _ in range(2)]))
+    fh_d = float(np.mean([fwd_adj_host(f64) for _ in range(2)]))
+    # accuracy of the mixed adjoint against the FP64 one
+    fm.evaluate_device()
+    fm.adjoint_device(w_dev.data_ptr(), dq_dev.data_ptr(), dx_dev.data_ptr())
+    dq_m, dx_m = dq_dev.cpu().numpy(), dx_dev.cpu().numpy()
+    f64.evaluate_device()
+    f64.adjoint_device(w_dev.data_ptr(), dq_dev.data_ptr(), dx_dev.data_ptr())
+    dq_d, dx_d = dq_dev.cpu().numpy(), dx_dev.cpu().numpy()
+    ddq = dq_m - dq_d
+    adj_err = {"dLdq_l2": float(np.linalg.norm(ddq) / np.linalg.norm(dq_d)),
+               "dLdq_l2_mean_removed": float(np.linalg.norm(ddq - ddq.mean()) / np.linalg.norm(dq_d - dq_d.mean())),
+               "dLdx_l2": float(np.linalg.norm(dx_m - dx_d) / np.linalg.norm(dx_d))}
 
     t_m = float(np.mean(ms_mixed))
     t_d = float(np.mean(ms64))
@@ -353,8 +377,10 @@ def run_ours(args):
                    "fp64_ms_per_step": t_d, "fp64_value": world * n / (t_d * 1e-3),
                    "mixed_speedup_vs_fp64": t_d / t_m,
                    "mixed_err_vs_fp64": {"l2p": err["l2p"], "l2f": err["l2f"], "l2p_mean_removed": err_mr},
-                   "fwd_adj_ms_mixed": 1000 * fa_m, "fwd_adj_ms_fp64": 1000 * fa_d,
+                   "fwd_adj_ms_mixed": fa_m, "fwd_adj_ms_fp64": fa_d,
                    "fwd_adj_mixed_speedup_vs_fp64": fa_d / fa_m,
+                   "fwd_adj_mixed_err_vs_fp64": adj_err,
+                   "fwd_adj_host_ms_mixed": fh_m, "fwd_adj_host_ms_fp64": fh_d,
                    "stage_ms_overlapped": st_mixed, "stage_ms_serial": stage_serial},
         "roofline": roofline,
         "cpu_baseline": cpu,

@@ -133,6 +133,14 @@ struct rtfmm_fmm {
   double* d_dip = nullptr;
   void* d_flush = nullptr;
   size_t flush_bytes = 0;
+  // adjoint scratch (allocated on first use): tree-order charges, the two
+  // gradient fields, and the host path's staging of w, dL/dq and dL/dx
+  double *d_adj_q = nullptr, *d_adj_gq = nullptr, *d_adj_gw = nullptr;
+  double *d_adj_w = nullptr, *d_adj_dq = nullptr, *d_adj_dx = nullptr;
+  cudaEvent_t ev_adj0 = nullptr, ev_adj1 = nullptr;
+  // d_out_grad holds grad(phi) of the bodies' current charges without the
+  // dipole correction (the last pass was such a forward pass)
+  bool grad_q_valid = false;
   float stage_ms[ST_N] = {};
   int64_t launches = 0;
 };
@@ -160,18 +168,28 @@ int dupload(rtfmm_fmm* f, T** p, const std::vector<T>& h) {
   return RTFMM_OK;
 }
 
+// Frees every device buffer of the handle and forgets the pointers that
+// are allocated lazily (L2 flush, adjoint scratch), so that none dangles.
+void drop_allocs(rtfmm_fmm* f) {
+  for (void* p : f->allocs) cudaFree(p);
+  f->allocs.clear();
+  f->d_flush = nullptr;
+  f->flush_bytes = 0;
+  f->d_adj_q = f->d_adj_gq = f->d_adj_gw = f->d_adj_w = f->d_adj_dq = f->d_adj_dx = nullptr;
+  f->grad_q_valid = false;
+}
+
 void free_device(rtfmm_fmm* f) {
   if (f->dev >= 0) cudaSetDevice(f->dev);
   if (f->h_xin) {
     cudaFreeHost(f->h_xin);
     f->h_xin = nullptr;
   }
-  for (void* p : f->allocs) cudaFree(p);
-  f->allocs.clear();
+  drop_allocs(f);
   if (f->s0) cudaStreamDestroy(f->s0);
   if (f->s1) cudaStreamDestroy(f->s1);
   f->s0 = f->s1 = nullptr;
-  cudaEvent_t* evs[] = {&f->ev_start, &f->ev_near0, &f->ev_near, &f->ev_stop};
+  cudaEvent_t* evs[] = {&f->ev_start, &f->ev_near0, &f->ev_near, &f->ev_stop, &f->ev_adj0, &f->ev_adj1};
   for (auto e : evs)
     if (*e) {
       cudaEventDestroy(*e);
@@ -469,6 +487,8 @@ int ensure_device(rtfmm_fmm* f) {
     CK(cudaEventCreate(&f->ev_near0));
     CK(cudaEventCreate(&f->ev_near));
     CK(cudaEventCreate(&f->ev_stop));
+    CK(cudaEventCreate(&f->ev_adj0));
+    CK(cudaEventCreate(&f->ev_adj1));
     for (int k = 0; k < ST_N; ++k) CK(cudaEventCreate(&f->ev_st[k]));
   } else {
     CK(cudaSetDevice(f->dev));
@@ -482,8 +502,7 @@ int upload_plan(rtfmm_fmm* f) {
   if (rc) return rc;
   // drop buffers of a previous plan, keep streams/events
   CK(cudaDeviceSynchronize());
-  for (void* p : f->allocs) cudaFree(p);
-  f->allocs.clear();
+  drop_allocs(f);
   Plan& p = f->plan;
   const Operators& o = f->ops;
   const int64_t n = p.n;
@@ -791,6 +810,7 @@ int enqueue_pass(rtfmm_fmm* f, bool adjoint = false, bool no_dipole = false) {
   f->launches++;
   CK(cudaEventRecord(f->ev_st[ST_POST], s0));
   CK(cudaEventRecord(f->ev_stop, s0));
+  f->grad_q_valid = !adjoint && dipole == 0 && near && far;
   return RTFMM_OK;
 }
 
@@ -904,6 +924,7 @@ int rtfmm_b200_setup(rtfmm_fmm* f, int64_t n, const double* x, const double* q) 
   }
   f->setup_done = true;
   f->device_ready = false;
+  f->grad_q_valid = false;
   return RTFMM_OK;
 }
 
@@ -921,6 +942,7 @@ int rtfmm_b200_upload(rtfmm_fmm* f) {
       b[i] = make_double4(f->plan.x[3 * i], f->plan.x[3 * i + 1], f->plan.x[3 * i + 2], f->plan.q[i]);
     CK(cudaMemcpy(f->d_body64, b.data(), sizeof(double4) * b.size(), cudaMemcpyHostToDevice));
   }
+  f->grad_q_valid = false;
   return RTFMM_OK;
 }
 
@@ -988,6 +1010,53 @@ int rtfmm_b200_solve(rtfmm_fmm* f, int64_t n, const double* x, const double* q, 
   return rtfmm_b200_evaluate(f, q, phi, grad);
 }
 
+namespace {
+
+int ensure_adj_scratch(rtfmm_fmm* f) {
+  if (f->d_adj_q) return RTFMM_OK;
+  const int64_t n = f->plan.n;
+  int rc = 0;
+  if ((rc = dalloc(f, &f->d_adj_q, n)) || (rc = dalloc(f, &f->d_adj_gq, 3 * n)) ||
+      (rc = dalloc(f, &f->d_adj_gw, 3 * n)) || (rc = dalloc(f, &f->d_adj_w, n)) ||
+      (rc = dalloc(f, &f->d_adj_dq, n)) || (rc = dalloc(f, &f->d_adj_dx, 3 * n)))
+    return rc;
+  return RTFMM_OK;
+}
+
+// The adjoint on device-resident data, all on s0: for L = sum_k w_k phi_k,
+//   dL/dq = K^T w                    (the transposed pass on the weights)
+//   dL/dx = w grad(phi_q) + q grad(psi_w)
+// where psi_w is the field of the weights.  grad(phi_q) is taken from the
+// last forward pass when it is still valid (same charges, no dipole
+// correction), else recomputed.  w, dq, dx are in input order; the bodies
+// keep their charges.
+int adjoint_core(rtfmm_fmm* f, const double* w, double* dq, double* dx) {
+  const int n = (int)f->plan.n;
+  int rc = ensure_adj_scratch(f);
+  if (rc) return rc;
+  cudaStream_t s0 = f->s0;
+  const bool have_gq = f->grad_q_valid;
+  if (have_gq) CK(cudaMemcpyAsync(f->d_adj_gq, f->d_out_grad, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, s0));
+  CK(launch_swap_charges(f->d_body64, w, f->d_perm, n, f->d_adj_q, s0));
+  rc = enqueue_pass(f, true);
+  if (rc) return rc;
+  if (dq) CK(cudaMemcpyAsync(dq, f->d_out_phi, sizeof(double) * n, cudaMemcpyDeviceToDevice, s0));
+  CK(launch_restore_charges(f->d_body64, f->d_adj_q, n, s0));
+  const double* gq = f->d_adj_gq;
+  const double* gw = f->d_out_grad;
+  if (!have_gq) {
+    CK(cudaMemcpyAsync(f->d_adj_gw, f->d_out_grad, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, s0));
+    rc = enqueue_pass(f, false, true);
+    if (rc) return rc;
+    gq = f->d_out_grad;
+    gw = f->d_adj_gw;
+  }
+  if (dx) CK(launch_adj_combine(f->d_perm, w, f->d_adj_q, gq, gw, n, dx, s0));
+  return RTFMM_OK;
+}
+
+}  // namespace
+
 int rtfmm_b200_adjoint(rtfmm_fmm* f, const double* w, double* dLdq, double* dLdx) {
   if (!f) return fail(RTFMM_EINVAL, "null handle");
   if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");
@@ -1000,29 +1069,40 @@ int rtfmm_b200_adjoint(rtfmm_fmm* f, const double* w, double* dLdq, double* dLdx
     if (rc) return rc;
   }
   CK(cudaSetDevice(f->dev));
-  std::vector<double> gw(3 * n), gq(3 * n), pw(n);
-  // 1) transposed chain on the weights: dL/dq and grad(psi_w) at the bodies
-  CK(cudaMemcpyAsync(f->d_xin, f->h_xin, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, f->s0));
-  CK(cudaMemcpyAsync(f->d_qin, w, sizeof(double) * n, cudaMemcpyHostToDevice, f->s0));
-  CK(launch_gather_bodies(f->d_xin, f->d_qin, f->d_perm, (int)n, f->d_body64, f->s0));
-  int rc = enqueue_pass(f, true);
+  int rc = ensure_adj_scratch(f);
   if (rc) return rc;
-  CK(cudaMemcpyAsync(pw.data(), f->d_out_phi, sizeof(double) * n, cudaMemcpyDeviceToHost, f->s0));
-  CK(cudaMemcpyAsync(gw.data(), f->d_out_grad, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, f->s0));
-  // 2) the forward field of the charges, recomputed (nothing kept from the
-  //    forward call): grad(phi_q) at the bodies
+  // the bodies with the set-up charges, as the forward solve had them
+  CK(cudaMemcpyAsync(f->d_xin, f->h_xin, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, f->s0));
   CK(cudaMemcpyAsync(f->d_qin, f->q_in.data(), sizeof(double) * n, cudaMemcpyHostToDevice, f->s0));
   CK(launch_gather_bodies(f->d_xin, f->d_qin, f->d_perm, (int)n, f->d_body64, f->s0));
-  rc = enqueue_pass(f, false, true);
+  f->grad_q_valid = false;
+  CK(cudaMemcpyAsync(f->d_adj_w, w, sizeof(double) * n, cudaMemcpyHostToDevice, f->s0));
+  rc = adjoint_core(f, f->d_adj_w, f->d_adj_dq, f->d_adj_dx);
   if (rc) return rc;
-  CK(cudaMemcpyAsync(gq.data(), f->d_out_grad, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, f->s0));
+  if (dLdq) CK(cudaMemcpyAsync(dLdq, f->d_adj_dq, sizeof(double) * n, cudaMemcpyDeviceToHost, f->s0));
+  if (dLdx) CK(cudaMemcpyAsync(dLdx, f->d_adj_dx, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, f->s0));
   CK(cudaStreamSynchronize(f->s0));
   CK(cudaGetLastError());
-  // dL/dx_i = w_i grad(phi_q)(x_i) + q_i grad(psi_w)(x_i)
-  if (dLdq) std::memcpy(dLdq, pw.data(), sizeof(double) * n);
-  if (dLdx)
-    for (int64_t i = 0; i < n; ++i)
-      for (int k = 0; k < 3; ++k) dLdx[3 * i + k] = w[i] * gq[3 * i + k] + f->q_in[i] * gw[3 * i + k];
+  f->pass_done = true;
+  return RTFMM_OK;
+}
+
+int rtfmm_b200_adjoint_device(rtfmm_fmm* f, const double* w_dev, double* dLdq_dev, double* dLdx_dev, float* ms) {
+  if (!f) return fail(RTFMM_EINVAL, "null handle");
+  if (!f->setup_done || !f->device_ready) return fail(RTFMM_ESTATE, "upload has not run");
+  if (ms) *ms = 0;
+  if (f->plan.n == 0) return RTFMM_OK;
+  if (!w_dev) return fail(RTFMM_EINVAL, "null weights");
+  CK(cudaSetDevice(f->dev));
+  CK(cudaEventRecord(f->ev_adj0, f->s0));
+  int rc = adjoint_core(f, w_dev, dLdq_dev, dLdx_dev);
+  if (rc) return rc;
+  CK(cudaEventRecord(f->ev_adj1, f->s0));
+  CK(cudaEventSynchronize(f->ev_adj1));
+  CK(cudaGetLastError());
+  float t = 0;
+  CK(cudaEventElapsedTime(&t, f->ev_adj0, f->ev_adj1));
+  if (ms) *ms = t;
   f->pass_done = true;
   return RTFMM_OK;
 }

@@ -1053,6 +1053,35 @@ __global__ void k_dipole_final(double* __restrict__ partial) {
   for (int k = 0; k < 3; ++k) partial[3 * kDipBlocks + k] = d[k];
 }
 
+// Adjoint support.  k_swap_charges puts the weights w (input order) into the
+// tree-order bodies and keeps their charges; k_restore_charges puts them
+// back; k_adj_combine forms dL/dx_k = w_k grad(phi_q)_k + q_k grad(psi_w)_k
+// in input order (k = perm[i]).
+__global__ void k_swap_charges(double4* __restrict__ body64, const double* __restrict__ w,
+                               const int64_t* __restrict__ perm, int n, double* __restrict__ qsave) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  qsave[i] = body64[i].w;
+  body64[i].w = w[perm[i]];
+}
+
+__global__ void k_restore_charges(double4* __restrict__ body64, const double* __restrict__ qsave, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  body64[i].w = qsave[i];
+}
+
+__global__ void k_adj_combine(const int64_t* __restrict__ perm, const double* __restrict__ w,
+                              const double* __restrict__ qsave, const double* __restrict__ grad_q,
+                              const double* __restrict__ grad_w, int n, double* __restrict__ dLdx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t k = perm[i];
+  const double wk = w[k], qk = qsave[i];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) dLdx[3 * k + c] = wk * grad_q[3 * k + c] + qk * grad_w[3 * k + c];
+}
+
 __global__ void k_post(const double* __restrict__ phi_far, const double* __restrict__ grad_far,
                        const double* __restrict__ phi_near, const double* __restrict__ grad_near,
                        const double4* __restrict__ body64, const int64_t* __restrict__ perm, int n,
@@ -1273,6 +1302,23 @@ cudaError_t launch_m2l_down(const T* Pk, const int* items, const double* tscale,
 cudaError_t launch_dipole(const double4* body64, int n, double* partial, cudaStream_t st) {
   k_dipole_partial<<<kDipBlocks, 256, 0, st>>>(body64, n, partial);
   k_dipole_final<<<1, 32, 0, st>>>(partial);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_swap_charges(double4* body64, const double* w, const int64_t* perm, int n, double* qsave,
+                                cudaStream_t st) {
+  if (n > 0) k_swap_charges<<<cdiv(n, 256), 256, 0, st>>>(body64, w, perm, n, qsave);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_restore_charges(double4* body64, const double* qsave, int n, cudaStream_t st) {
+  if (n > 0) k_restore_charges<<<cdiv(n, 256), 256, 0, st>>>(body64, qsave, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adj_combine(const int64_t* perm, const double* w, const double* qsave, const double* grad_q,
+                               const double* grad_w, int n, double* dLdx, cudaStream_t st) {
+  if (n > 0) k_adj_combine<<<cdiv(n, 256), 256, 0, st>>>(perm, w, qsave, grad_q, grad_w, n, dLdx);
   return cudaGetLastError();
 }
 

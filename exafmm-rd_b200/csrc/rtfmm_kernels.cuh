@@ -101,6 +101,13 @@ cudaError_t launch_l2p_eval(const double4* body64, const LeafInfo* leaves, int n
                             const double* surf_unit, int ns, const double* q_down, double* phi,
                             double* grad, cudaStream_t st, int newton = 2);
 cudaError_t launch_dipole(const double4* body64, int n, double* partial /*>= 4*1024*/, cudaStream_t st);
+// adjoint: weights into the tree-order bodies (charges kept in qsave), the
+// charges back, and dL/dx = w grad(phi_q) + q grad(psi_w) in input order
+cudaError_t launch_swap_charges(double4* body64, const double* w, const int64_t* perm, int n, double* qsave,
+                                cudaStream_t st);
+cudaError_t launch_restore_charges(double4* body64, const double* qsave, int n, cudaStream_t st);
+cudaError_t launch_adj_combine(const int64_t* perm, const double* w, const double* qsave, const double* grad_q,
+                               const double* grad_w, int n, double* dLdx, cudaStream_t st);
 cudaError_t launch_post(const double* phi_far, const double* grad_far, const double* phi_near,
                         const double* grad_near, const double4* body64, const int64_t* perm, int n,
                         const double* dipole_partial, double coef, int dipole, double out_scale,

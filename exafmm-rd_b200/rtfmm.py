@@ -33,7 +33,8 @@ STAGE_NAMES = ("prep", "P2M", "M2M", "M2L_up", "M2L_hadamard", "M2L_down", "L2L"
 EXPORTS = (
     "rtfmm_b200_default_args", "rtfmm_b200_create", "rtfmm_b200_destroy", "rtfmm_b200_setup",
     "rtfmm_b200_evaluate", "rtfmm_b200_solve", "rtfmm_b200_upload", "rtfmm_b200_evaluate_device",
-    "rtfmm_b200_download", "rtfmm_b200_adjoint", "rtfmm_b200_stage_times", "rtfmm_b200_launch_count",
+    "rtfmm_b200_download", "rtfmm_b200_adjoint", "rtfmm_b200_adjoint_device", "rtfmm_b200_stage_times",
+    "rtfmm_b200_launch_count",
     "rtfmm_b200_flush_l2", "rtfmm_b200_info", "rtfmm_b200_get_cells", "rtfmm_b200_get_perm",
     "rtfmm_b200_get_p2p", "rtfmm_b200_get_m2l", "rtfmm_b200_get_cell_vectors", "rtfmm_b200_get_operator",
     "rtfmm_b200_last_error", "rtfmm_b200_version", "rtfmm_b200_p2m_noalloc",
@@ -81,6 +82,7 @@ def lib():
         "rtfmm_b200_evaluate_device": (ctypes.c_int, [_vp, _fp]),
         "rtfmm_b200_download": (ctypes.c_int, [_vp, _dp, _dp]),
         "rtfmm_b200_adjoint": (ctypes.c_int, [_vp, _dp, _dp, _dp]),
+        "rtfmm_b200_adjoint_device": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_float)]),
         "rtfmm_b200_stage_times": (ctypes.c_int, [_vp, _dp, ctypes.c_int]),
         "rtfmm_b200_launch_count": (ctypes.c_int, [_vp, _lp]),
         "rtfmm_b200_flush_l2": (ctypes.c_int, [_vp]),
@@ -247,6 +249,15 @@ class LaplaceFMM:
         dx = np.empty((self.n, 3))
         _check(lib().rtfmm_b200_adjoint(self._h, _ptr(w), _ptr(dq), _ptr(dx)))
         return dq, dx
+
+    def adjoint_device(self, w_ptr, dq_ptr, dx_ptr):
+        """Adjoint on device memory: integer device addresses (e.g. a torch
+        tensor's data_ptr()) of w (n), dL/dq (n) and dL/dx (n, 3), input
+        order, float64.  Returns the device time in ms."""
+        ms = ctypes.c_float(0)
+        _check(lib().rtfmm_b200_adjoint_device(self._h, _vp(w_ptr), _vp(dq_ptr or None), _vp(dx_ptr or None),
+                                               ctypes.byref(ms)))
+        return ms.value
 
     # -- introspection ------------------------------------------------------------
     def info(self):

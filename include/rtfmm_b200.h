@@ -134,6 +134,21 @@ int rtfmm_b200_download(rtfmm_fmm* fmm, double* phi, double* grad);
  */
 int rtfmm_b200_adjoint(rtfmm_fmm* fmm, const double* w, double* dLdq, double* dLdx);
 
+/*
+ * The adjoint on device memory (no reference counterpart): w_dev (n),
+ * dLdq_dev (n) and dLdx_dev (n*3) are device pointers on the handle's
+ * device, in input order (the outputs may be NULL).  It works on the bodies
+ * and charges the device holds (those of the last upload, evaluate or solve)
+ * and needs rtfmm_b200_upload (or an evaluate) first.  When the last pass
+ * was a forward pass of these charges without the dipole correction, its
+ * gradient is reused and the call runs one transposed pass; otherwise it
+ * runs two.  Weights are not checked for NaN/Inf.  *ms (may be NULL)
+ * receives the device time of the call; it returns when the results are
+ * complete.  Afterwards rtfmm_b200_download returns intermediate fields.
+ */
+int rtfmm_b200_adjoint_device(rtfmm_fmm* fmm, const double* w_dev, double* dLdq_dev, double* dLdx_dev,
+                              float* ms);
+
 /* Per-stage device times of the last pass, in ms, in this order:
  * prep, P2M, M2M, M2L_up, M2L_hadamard, M2L_down, L2L, L2P, P2P, post.
  * Writes min(cap, 10) values; returns the number of stages. */

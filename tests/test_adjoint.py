@@ -126,3 +126,32 @@ def test_autograd_harness(pkg):
     dq, dx = f.adjoint(w.numpy())
     assert np.allclose(qt.grad.numpy(), dq, rtol=0, atol=1e-12 * np.abs(dq).max())
     assert np.allclose(xt.grad.numpy(), dx, rtol=0, atol=1e-12 * np.abs(dx).max())
+
+
+@pytest.mark.parametrize("precision,dipole", [(0, 0), (1, 0), (0, 1)])
+def test_device_adjoint_matches_host_adjoint(pkg, precision, dipole):
+    """rtfmm_b200_adjoint_device on device buffers gives the host adjoint's
+    dL/dq and dL/dx: after a forward pass without the dipole correction it
+    reuses that pass's gradient, otherwise (dipole on, or a second call) it
+    recomputes it."""
+    import torch
+    x, q = uniform01(3000, 11)
+    w = np.random.default_rng(12).standard_normal(len(q))
+    a = pkg.Argument(P=6, ncrit=32, images=3, cycle=1.0, x=(0.5, 0.5, 0.5), dipole_correction=dipole,
+                     divide_4pi=1, precision=precision)
+    ref = pkg.LaplaceFMM(x, q, a)
+    ref.setup()
+    dq_ref, dx_ref = ref.adjoint(w)
+    f = pkg.LaplaceFMM(x, q, a)
+    f.setup()
+    f.upload()
+    f.evaluate_device()
+    wt = torch.from_numpy(w).cuda()
+    for call in range(2):
+        dq = torch.full((len(q),), float("nan"), dtype=torch.float64, device="cuda")
+        dx = torch.full((len(q), 3), float("nan"), dtype=torch.float64, device="cuda")
+        ms = f.adjoint_device(wt.data_ptr(), dq.data_ptr(), dx.data_ptr())
+        assert ms > 0
+        dqn, dxn = dq.cpu().numpy(), dx.cpu().numpy()
+        assert np.linalg.norm(dqn - dq_ref) <= 1e-12 * np.linalg.norm(dq_ref), call
+        assert np.linalg.norm(dxn - dx_ref) <= 1e-12 * np.linalg.norm(dx_ref), call
