@@ -46,6 +46,10 @@
 #ifndef APPLY_MMA
 #define APPLY_MMA 0
 #endif
+// FP64 operator application on the cp.async + mma.sync kernel
+#ifndef APPLY_TC
+#define APPLY_TC 1
+#endif
 
 namespace rtfmm_b200 {
 
@@ -619,6 +623,137 @@ __global__ void __launch_bounds__(256, 2) k_apply_f64(ApplyBatch b) {
 }
 #endif
 
+// ---------------------------------------------------------------------------
+// The same batched application on the FP64 tensor path: 64x64 output tiles
+// per 128-thread block (2 x 2 warps of 32x32, each 4 x 4 mma.sync m8n8k4
+// f64 tiles), A rows (gathered through inrow) and the B panel moved into
+// shared memory by cp.async through a three-stage ring, so that the loads of
+// K step t+2 are in flight while step t is multiplied.  Products and sums
+// are IEEE FP64 as in the SIMT kernel; only the summation order differs.
+// Every 16-byte copy is in bounds or zero-filled (ns is even: 6(P-1)^2+2).
+// ---------------------------------------------------------------------------
+constexpr int kGM = 64, kGN = 64, kGK = 16, kGStages = 3, kGThreads = 128;
+constexpr int kAPitch = kGK + 4;  // doubles per A row in shared memory (conflict-free fragments)
+constexpr int kBPitch = kGN + 4;  // doubles per B row
+constexpr int kAStage = kGM * kAPitch, kBStage = kGK * kBPitch;
+[[maybe_unused]] constexpr size_t kGSmem = sizeof(double) * kGStages * (kAStage + kBStage);
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  const int nbytes = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sa), "l"(gmem), "r"(nbytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+__device__ __forceinline__ void dmma8x8x4(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(kGThreads) k_apply_f64_tc(ApplyBatch b) {
+  extern __shared__ __align__(16) double gsm[];
+  double* As = gsm;
+  double* Bs = gsm + kGStages * kAStage;
+  const int g = blockIdx.z;
+  const int rbeg = b.group_off[g], rend = b.group_off[g + 1];
+  const int r0 = rbeg + blockIdx.y * kGM;
+  const int c0 = blockIdx.x * kGN;
+  if (r0 >= rend) return;  // block-uniform
+  const int ns = b.ns, S = b.S;
+  const double* Bg = b.B + (size_t)g * S * ns * ns;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp & 1, wn = warp >> 1;
+  const int nkt = (ns + kGK - 1) / kGK, total = S * nkt;
+  // copies of this thread: A chunk e = tid + 128u -> row e/8, doubles 2(e%8)..+1;
+  // B chunk e -> K row e/32, columns 2(e%32)..+1
+  int srow[4];
+  int s_cur = -1;
+  auto issue = [&](int kt) {
+    const int s = kt / nkt, j0 = (kt - s * nkt) * kGK;
+    if (s != s_cur) {
+      s_cur = s;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int row = r0 + ((tid + kGThreads * u) >> 3);
+        srow[u] = row < rend ? b.inrow[(size_t)row * S + s] : -1;
+      }
+    }
+    double* as = As + (kt % kGStages) * kAStage;
+    double* bs = Bs + (kt % kGStages) * kBStage;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int e = tid + kGThreads * u;
+      const int r = e >> 3, ch = e & 7, j = j0 + 2 * ch;
+      const bool ok = srow[u] >= 0 && j < ns;
+      cp_async16(as + r * kAPitch + 2 * ch, ok ? b.A + (size_t)srow[u] * ns + j : b.A, ok);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int e = tid + kGThreads * u;
+      const int kr = e >> 5, ch = e & 31, jj = j0 + kr, n = c0 + 2 * ch;
+      const bool ok = jj < ns && n < ns;
+      cp_async16(bs + kr * kBPitch + 2 * ch, ok ? Bg + ((size_t)s * ns + jj) * ns + n : Bg, ok);
+    }
+  };
+  double acc[4][4][2];
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) acc[mt][nt][0] = acc[mt][nt][1] = 0.0;
+#pragma unroll
+  for (int st = 0; st < kGStages - 1; ++st) {
+    if (st < total) issue(st);
+    cp_async_commit();
+  }
+  for (int kt = 0; kt < total; ++kt) {
+    cp_async_wait<kGStages - 2>();
+    __syncthreads();  // step kt is in shared memory; step kt-1's buffer is free
+    if (kt + kGStages - 1 < total) issue(kt + kGStages - 1);
+    cp_async_commit();
+    const double* as = As + (kt % kGStages) * kAStage + (wm * 32 + (lane >> 2)) * kAPitch + (lane & 3);
+    const double* bs = Bs + (kt % kGStages) * kBStage + (lane & 3) * kBPitch + wn * 32 + (lane >> 2);
+#pragma unroll
+    for (int k4 = 0; k4 < kGK; k4 += 4) {
+      double fa[4], fb[4];
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt) fa[mt] = as[mt * 8 * kAPitch + k4];
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) fb[nt] = bs[k4 * kBPitch + nt * 8];
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) dmma8x8x4(acc[mt][nt], fa[mt], fb[nt]);
+    }
+  }
+  cp_async_wait<0>();
+  // D fragment: row lane/4, columns 2 (lane%4) + {0, 1} of each 8x8 tile
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt) {
+    const int row = r0 + wm * 32 + mt * 8 + (lane >> 2);
+    if (row >= rend) continue;
+    const int o = b.outrow[row];
+    const double sc = b.scale ? b.scale[row] : 1.0;
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+      const int n = c0 + wn * 32 + nt * 8 + 2 * (lane & 3);
+      if (n >= ns) continue;  // n even, ns even: n + 1 < ns as well
+      double2* cp = reinterpret_cast<double2*>(b.C + (size_t)o * ns + n);
+      double2 v = make_double2(sc * acc[mt][nt][0], sc * acc[mt][nt][1]);
+      if (b.beta) {
+        const double2 c = *cp;
+        v.x += c.x;
+        v.y += c.y;
+      }
+      *cp = v;
+    }
+  }
+}
+
 // Sibling sum of the per-child M2M products, in crange order
 // (m2m_precompute accumulates child by child, kernel.cpp:398-403).
 __global__ void k_sum_children(const int* __restrict__ list, int nparents, const double* __restrict__ Y, int ns,
@@ -1186,8 +1321,24 @@ cudaError_t launch_l2p_eval(const double4* body64, const LeafInfo* leaves, int n
 
 cudaError_t launch_apply(const ApplyBatch& b, cudaStream_t st) {
   if (b.max_rows > 0 && b.groups > 0) {
+#if APPLY_TC
+    if (b.ns % 2 != 0) return cudaErrorInvalidValue;  // 16-byte copies need an even ns
+    // the shared-memory opt-in is per function and device
+    static bool attr_set[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+      e = cudaFuncSetAttribute(k_apply_f64_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGSmem);
+      if (e != cudaSuccess) return e;
+      if (dev >= 0 && dev < 64) attr_set[dev] = true;
+    }
+    dim3 grid(cdiv(b.ns, kGN), cdiv(b.max_rows, kGM), b.groups);
+    k_apply_f64_tc<<<grid, kGThreads, kGSmem, st>>>(b);
+#else
     dim3 grid(cdiv(b.ns, kTN), cdiv(b.max_rows, kTM), b.groups);
     k_apply_f64<<<grid, 256, 0, st>>>(b);
+#endif
   }
   return cudaGetLastError();
 }
