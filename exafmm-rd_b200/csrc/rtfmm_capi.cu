@@ -65,6 +65,10 @@ struct ApplyCall {
 //   adjoint image levels: the transposes swap roles, so the upward step uses
 //   M2M_img[13] (the transpose of the forward L2L_img) and the downward step
 //   the transposed 27-image sum
+// Largest P at which the FP32-mixed form runs the 8x8 FFT-M2L in FP32 (its
+// gradient error stays below 1e-5 on uniform inputs up to P = 8; 3e-5 at 10).
+constexpr int kM2L32MaxP = 8;
+
 enum BSel { B_P2M1 = 0, B_P2M2, B_L2P1, B_L2P2, B_M2MT, B_M2M, B_IMGSUMT, B_IMG13, B_ADJ_IMG_UP, B_ADJ_IMG_DOWN,
             B_NUM };
 
@@ -141,6 +145,8 @@ struct rtfmm_fmm {
   // d_out_grad holds grad(phi) of the bodies' current charges without the
   // dipole correction (the last pass was such a forward pass)
   bool grad_q_valid = false;
+  // the 8x8 FFT-M2L (up, Hadamard, down) runs in FP32: the mixed form at P <= 8
+  bool m2l32 = false;
   float stage_ms[ST_N] = {};
   int64_t launches = 0;
 };
@@ -596,7 +602,8 @@ int upload_plan(rtfmm_fmm* f) {
   for (int t = 0; t < f->nT8; ++t)
     for (int d = 0; d < 26; ++d) tsrcT[(size_t)d * f->nT8 + t] = f->tsrc8[(size_t)t * 26 + d];
   RC(dupload(f, &f->d_tsrc8, tsrcT));
-  if (mixed) {
+  f->m2l32 = mixed && o.P <= kM2L32MaxP;
+  if (f->m2l32) {
     std::vector<float> g(g64.size());
     for (size_t i = 0; i < g.size(); ++i) g[i] = (float)g64[i];
     float* gp;
@@ -621,8 +628,8 @@ int upload_plan(rtfmm_fmm* f) {
   RC(dalloc(f, &f->d_Q27, (size_t)f->nS27 * 8 * Nf * 2));
   RC(dalloc(f, &f->d_Pk27, (size_t)f->nT27 * 8 * Nf * 2));
   // M2L up/down blocks: groups of sp child slots (sized to shared memory)
-  f->sp_up8 = mixed ? m2l_up_slots<float>(o.P) : m2l_up_slots<double>(o.P);
-  f->sp_down8 = mixed ? m2l_down_slots<float>(o.P) : m2l_down_slots<double>(o.P);
+  f->sp_up8 = f->m2l32 ? m2l_up_slots<float>(o.P) : m2l_up_slots<double>(o.P);
+  f->sp_down8 = f->m2l32 ? m2l_down_slots<float>(o.P) : m2l_down_slots<double>(o.P);
   f->sp_up27 = m2l_up_slots<double>(o.P);
   f->sp_down27 = m2l_down_slots<double>(o.P);
   auto group = [](const std::vector<int>& slots, int sp, bool keep_empty, std::vector<int>& items) {
@@ -743,7 +750,7 @@ int enqueue_pass(rtfmm_fmm* f, bool adjoint = false, bool no_dipole = false) {
     CK(cudaEventRecord(f->ev_st[ST_M2M], s0));
     const int nup8 = (int)f->up8_items.size() / 10, nup27 = (int)f->up27_items.size() / 10;
     const int ndn8 = (int)f->down8_items.size() / 10, ndn27 = (int)f->down27_items.size() / 10;
-    if (mixed) {
+    if (f->m2l32) {
       CK(launch_m2l_up<float>(f->d_qeq, f->d_up8, nup8, f->d_surf_ijk, f->d_twiddle, P, ns, f->nS8, f->sp_up8,
                               (float*)f->d_Q8, s0));
     } else {
@@ -754,7 +761,7 @@ int enqueue_pass(rtfmm_fmm* f, bool adjoint = false, bool no_dipole = false) {
                              f->sp_up27, f->d_Q27, s0));
     f->launches += (nup8 > 0) + (nup27 > 0);
     CK(cudaEventRecord(f->ev_st[ST_UP], s0));
-    if (mixed) {
+    if (f->m2l32) {
       CK(launch_m2l_hadamard8<float>((const float*)f->d_Q8, (const float*)f->d_G8, f->d_tsrc8, f->nT8, f->nS8,
                                      Nf, (float*)f->d_Pk8, s0));
     } else {
@@ -764,7 +771,7 @@ int enqueue_pass(rtfmm_fmm* f, bool adjoint = false, bool no_dipole = false) {
     CK(launch_m2l_hadamard27(f->d_Q27, f->d_G27, f->d_tsrc27, f->nT27, f->nS27, Nf, f->d_Pk27, s0));
     f->launches += (f->nT8 > 0) + (f->nT27 > 0);
     CK(cudaEventRecord(f->ev_st[ST_HAD], s0));
-    if (mixed) {
+    if (f->m2l32) {
       CK(launch_m2l_down<float>((const float*)f->d_Pk8, f->d_down8, f->d_tscale8, ndn8, f->d_surf_ijk,
                                 f->d_twiddle, P, ns, f->nT8, f->sp_down8, f->d_pchk, s0));
     } else {

@@ -27,6 +27,9 @@
 #ifndef P2P_PACKED
 #define P2P_PACKED 1
 #endif
+#ifndef P2P_WARPS
+#define P2P_WARPS 4
+#endif
 // FP32 Hadamard: targets per thread, directions per FP32 partial sum,
 // resident blocks per SM
 #ifndef HAD_TT
@@ -124,7 +127,7 @@ __global__ void k_prep32(const double4* __restrict__ body64, const int* __restri
 // next tile's bodies and the next list entry loaded while the current tile is
 // computed.  FP32 partial sums per source leaf are accumulated into FP64.
 // ---------------------------------------------------------------------------
-constexpr int kP2PWarps = 4;
+constexpr int kP2PWarps = P2P_WARPS;
 constexpr int kP2PUnroll = P2P_UNROLL;
 
 // Lanes of group `k0` (of G groups) take the tile's sources k0, k0+G, ...

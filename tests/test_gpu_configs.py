@@ -1,0 +1,134 @@
+"""GPU parity on the workload's configurations at their full sizes.
+
+The oracle finishes in seconds only up to a few thousand bodies, so the two
+large configurations are checked through properties that do not depend on
+size:
+
+  C1   N=8192 uniform in [0,1)^3, P=6, ncrit=64, images=3, seed 1: against
+       the oracle, both precisions.
+  P10  N=4000 uniform, P=10, ncrit=64, images=3: against the oracle (the
+       P=10 operators: 488 surface points, a 19^3 convolution grid).
+  C3   N=2^22 in 64 Gaussian blobs (sigma 0.02, wrapped), P=10, ncrit=128,
+       images=3 (deep adaptive tree): FP32-mixed against FP64 (3e-5), and
+       linearity in the charges in FP64 on the same tree.
+  C5   200^3 rock-salt lattice (spacing a = 1/200, q = (-1)^(i+j+k)), P=10,
+       ncrit=256, images=4.  Unjittered, the periodic potential at every site
+       is -M q_i / a up to a constant, M = 1.747564594633182 the NaCl
+       Madelung constant, and the field vanishes by symmetry.  Jittered by
+       U(+-0.1 a), FP32-mixed against FP64.
+
+Tolerances are relative L2 (the reference's compare metric) unless stated.
+At P=10 the check-to-equivalent operator's condition number (1.3e16)
+exceeds 1/eps: two FP64 implementations agree only to ~1e-7 there (the
+reference and the oracle differ by 7e-8 in the gradient on the same input),
+so the FP64 tolerance is 1e-7 at P=10 and 1e-9 below.  In the mixed form
+the gradient error is set by FP32 P2P on the closest pairs: the relative L2
+metric is dominated by the few closest pairs, whose coordinate difference
+carries 2^-24 of the leaf size; on the dense blobs of C3 that is 1.8e-5.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+MADELUNG_NACL = 1.747564594633182
+
+
+def uniform01(n, seed):
+    rng = np.random.default_rng(seed)
+    x = rng.random((n, 3))
+    q = rng.random(n) * 2 - 1
+    return x, q - q.mean()
+
+
+def blobs(n, nblob, sigma, seed):
+    rng = np.random.default_rng(seed)
+    c = rng.random((nblob, 3))
+    x = np.mod(c[rng.integers(0, nblob, n)] + sigma * rng.standard_normal((n, 3)), 1.0)
+    q = np.where(rng.random(n) < 0.5, -1.0, 1.0)
+    return x, q - q.mean()
+
+
+def rock_salt(n, jitter, seed):
+    a = 1.0 / n
+    g = (np.arange(n) + 0.5) * a
+    X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
+    x = np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1)
+    if jitter:
+        x = np.mod(x + np.random.default_rng(seed).uniform(-jitter * a, jitter * a, x.shape), 1.0)
+    i, j, k = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    q = np.where((i + j + k).ravel() % 2 == 0, 1.0, -1.0)
+    return x, q
+
+
+def l2(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b)))
+
+
+def args(pkg, P, ncrit, images, precision, div4pi=1):
+    return pkg.Argument(P=P, ncrit=ncrit, images=images, cycle=1.0, x=(0.5, 0.5, 0.5), dipole_correction=0,
+                        divide_4pi=div4pi, precision=precision)
+
+
+def solve(pkg, x, q, a):
+    f = pkg.LaplaceFMM(x, q, a)
+    phi, grad = f.solve()
+    return f, phi, grad
+
+
+@pytest.mark.parametrize("name,n,P,ncrit,seed", [("C1", 8192, 6, 64, 1), ("P10", 4000, 10, 64, 7)])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_against_oracle(pkg, oracle, name, n, P, ncrit, seed, precision):
+    x, q = uniform01(n, seed)
+    f, phi, grad = solve(pkg, x, q, args(pkg, P, ncrit, 3, precision))
+    f.close()
+    F = oracle.FMM(x, q, P, ncrit, 3, 1.0, center=(0.5, 0.5, 0.5), dipole_correction=0, divide_4pi=1)
+    rphi, rgrad = F.solve()
+    eg = l2(grad, rgrad)
+    emr = l2(phi - phi.mean(), rphi - rphi.mean())
+    if precision == 0:
+        tol = 1e-7 if P >= 10 else 1e-9
+        assert eg < tol and emr < 10 * tol and l2(phi, rphi) < 1e-5, (eg, emr)
+    else:
+        assert eg < 1e-5 and l2(phi, rphi) < 1e-5, (eg, l2(phi, rphi))
+
+
+def test_c3_blobs_mixed_vs_fp64_and_linearity(pkg):
+    x, q = blobs(1 << 22, 64, 0.02, 3)
+    fd, phi_d, grad_d = solve(pkg, x, q, args(pkg, 10, 128, 3, 0))
+    fm, phi_m, grad_m = solve(pkg, x, q, args(pkg, 10, 128, 3, 1))
+    fm.close()
+    assert l2(grad_m, grad_d) < 3e-5, l2(grad_m, grad_d)
+    assert l2(phi_m - phi_m.mean(), phi_d - phi_d.mean()) < 1e-5
+    # linearity on the same tree: phi(q + 2 q2) = phi(q) + 2 phi(q2)
+    q2 = np.random.default_rng(13).standard_normal(len(q))
+    q2 -= q2.mean()
+    phi2, grad2 = fd.evaluate(q2)
+    phi3, grad3 = fd.evaluate(q + 2 * q2)
+    fd.close()
+    assert l2(grad3, grad_d + 2 * grad2) < 1e-11
+    assert l2(phi3 - phi3.mean(), (phi_d + 2 * phi2) - (phi_d + 2 * phi2).mean()) < 1e-9
+
+
+@pytest.mark.parametrize("precision,tol_phi,tol_grad", [(0, 1e-8, 1e-5), (1, 2e-6, 1e-4)])
+def test_c5_lattice_madelung(pkg, precision, tol_phi, tol_grad):
+    n = 200
+    a = 1.0 / n
+    x, q = rock_salt(n, 0.0, 5)
+    f, phi, grad = solve(pkg, x, q, args(pkg, 10, 256, 4, precision, div4pi=0))
+    f.close()
+    exact = -MADELUNG_NACL * q / a
+    # the constant is the lattice sum's shape term; q has zero mean
+    assert abs(float(np.mean(q * phi)) * a + MADELUNG_NACL) / MADELUNG_NACL < tol_phi
+    assert l2(phi - phi.mean(), exact) < 10 * tol_phi
+    assert float(np.abs(grad).max()) * a * a / MADELUNG_NACL < tol_grad
+
+
+def test_c5_jittered_mixed_vs_fp64(pkg):
+    x, q = rock_salt(200, 0.1, 5)
+    fd, phi_d, grad_d = solve(pkg, x, q, args(pkg, 10, 256, 4, 0))
+    fd.close()
+    fm, phi_m, grad_m = solve(pkg, x, q, args(pkg, 10, 256, 4, 1))
+    fm.close()
+    assert l2(grad_m, grad_d) < 1e-5, l2(grad_m, grad_d)
+    assert l2(phi_m - phi_m.mean(), phi_d - phi_d.mean()) < 1e-5

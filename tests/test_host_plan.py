@@ -124,7 +124,7 @@ def test_kernel_spectra_match_oracle(pkg, oracle, P):
     assert np.abs(got - ref).max() / scale < 1e-13
 
 
-@pytest.mark.parametrize("P", [4, 6, 8])
+@pytest.mark.parametrize("P", [4, 6, 8, 10])
 def test_m2m_reproduces_child_potential(pkg, oracle, P):
     """The parent equivalent density from M2M reproduces the child's field on
     the parent check surface (the defining property of the operator,
@@ -146,7 +146,27 @@ def test_m2m_reproduces_child_potential(pkg, oracle, P):
         qc = rng.standard_normal(ns)
         target = G @ qc
         err = np.linalg.norm(A @ (m2m[o] @ qc) - target) / np.linalg.norm(target)
-        assert err < {4: 1e-12, 6: 1e-10, 8: 1e-8}[P]
+        assert err < {4: 1e-12, 6: 1e-10, 8: 1e-8, 10: 1e-9}[P]
+
+
+@pytest.mark.parametrize("P", [8, 10])
+def test_svd_factors_are_orthonormal(pkg, oracle, P):
+    """U and V of the check-to-equivalent operator are orthonormal to working
+    precision, as an orthogonal factorisation (the reference's dgesvd,
+    mathfunc.cpp:81-110) returns them, also at P = 10 where the operator's
+    condition number (1.3e16) exceeds 1/eps: U = A V / s alone loses
+    orthogonality in the columns of the smallest singular values."""
+    x, q = uniform(200, 3)
+    f = pkg.LaplaceFMM(x, q, pkg.Argument(P=P, ncrit=64, images=1, cycle=1.0))
+    f.setup()
+    ns = oracle.surface_point_num(P)
+    U = f.operator(4, ns * ns).reshape(ns, ns)
+    VS = f.operator(5, ns * ns).reshape(ns, ns)
+    sinv = np.linalg.norm(VS, axis=0)
+    keep = sinv > 0
+    V = VS[:, keep] / sinv[keep]
+    assert np.abs(U.T @ U - np.eye(ns)).max() < 1e-13
+    assert np.abs(V.T @ V - np.eye(int(keep.sum()))).max() < 1e-13
 
 
 def test_errors(pkg):

@@ -90,3 +90,24 @@ def test_fmm_gradient_error_vs_ewald_is_the_published_order(oracle):
     phi, grad = oracle.solve(g["x"], g["q"], 6, 64, 3, 1.0, dipole_correction=1, divide_4pi=1)
     e = l2(grad, g["ewald_grad"])
     assert 1e-5 < e < 1e-4, e
+
+
+def test_oracle_rock_salt_madelung(oracle):
+    """Physics known answer for the periodic top: on an unjittered rock-salt
+    lattice (spacing a, q = (-1)^(i+j+k)) the periodic 1/r potential at every
+    site is -M q_i / a up to a constant, M = 1.747564594633182 the NaCl
+    Madelung constant, and the field vanishes."""
+    M = 1.747564594633182
+    n = 8
+    a = 1.0 / n
+    g = (np.arange(n) + 0.5) * a
+    X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
+    x = np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1)
+    i, j, k = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    q = np.where((i + j + k).ravel() % 2 == 0, 1.0, -1.0)
+    F = oracle.FMM(x, q, 6, 64, 3, 1.0, center=(0.5, 0.5, 0.5), dipole_correction=0, divide_4pi=0)
+    phi, grad = F.solve()
+    assert abs(float(np.mean(q * phi)) * a + M) / M < 1e-7
+    pm = phi - phi.mean()
+    assert np.linalg.norm(pm + M * q / a) / np.linalg.norm(M * q / a) < 1e-6
+    assert np.abs(grad).max() * a * a / M < 1e-6
