@@ -17,6 +17,11 @@
 
 #include <cuda_runtime.h>
 
+// FP64 pair kernels: seed the reciprocal square root with the FP64 (1) or
+// FP32 (0) hardware approximation
+#ifndef RSQ_SEED64
+#define RSQ_SEED64 1
+#endif
 // FP32 P2P: inner unroll and resident blocks per SM
 #ifndef P2P_UNROLL
 #define P2P_UNROLL 4
@@ -83,16 +88,23 @@ __device__ __forceinline__ float rsqrt_approx(float x) {
   return y;
 }
 
-// 1/sqrt(x) in FP64 by Newton-Raphson from the FP32 hardware approximation:
-// y <- y (3/2 - x y^2 / 2).  The approximation is good to about 2^-22, so
-// one step gives ~1e-13 and two give full double precision.  Arguments
-// outside the normal FP32 range (pairs closer than ~1e-19 or farther than
-// ~1e19) take the FP64 library function instead.
+// 1/sqrt(x) in FP64 by Newton-Raphson, y <- y (3/2 - x y^2 / 2), from a
+// hardware seed.  The PTX FP64 approximation (rsqrt.approx.ftz.f64, one
+// special-function op) is good to 9.1e-7 relative; one step gives 1.3e-12 and
+// two give 3.3e-16 (maxima measured against CUDA's rsqrt over 1e-30..1e30).
+// The FP32 approximation (1.5e-7, but two conversions on the same pipe as the
+// seed) gives 3.2e-14 and 3.3e-16, for arguments in the normal FP32 range.
+// x must be positive and normal (pairs closer than 1e-154 are not supported).
 template <int NR>
 __device__ __forceinline__ double rsqrt_nr(double x) {
+#if RSQ_SEED64
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+#else
   const float xf = (float)x;
   if (!(xf >= 1.2e-38f && xf <= 3.0e38f)) return rsqrt(x);
   double y = (double)rsqrt_approx(xf);
+#endif
   const double h = 0.5 * x;
 #pragma unroll
   for (int i = 0; i < NR; ++i) y = y * fma(-h * y, y, 1.5);
