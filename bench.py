@@ -384,7 +384,7 @@ def run_ours(args):
                    "stage_ms_overlapped": st_mixed, "stage_ms_serial": stage_serial},
         "roofline": roofline,
         "cpu_baseline": cpu,
-        "e2e": {"value": world * n / t_e, "unit": "particles/s", "h2d_bytes_per_step": 8 * n + 24 * n,
+        "e2e": {"value": world * n / t_e, "unit": "particles/s", "h2d_bytes_per_step": 8 * n,
                 "d2h_bytes_per_step": 8 * n + 24 * n, "ms_per_step": 1000 * t_e},
         "gpu_launches": launches,
         "clocks": clocks,

@@ -145,6 +145,9 @@ struct rtfmm_fmm {
   // d_out_grad holds grad(phi) of the bodies' current charges without the
   // dipole correction (the last pass was such a forward pass)
   bool grad_q_valid = false;
+  // d_body64 holds this set-up's positions (tree order); an evaluate then
+  // only moves the charges
+  bool pos_on_device = false;
   // the 8x8 FFT-M2L (up, Hadamard, down) runs in FP32: the mixed form at P <= 8
   bool m2l32 = false;
   float stage_ms[ST_N] = {};
@@ -183,6 +186,7 @@ void drop_allocs(rtfmm_fmm* f) {
   f->flush_bytes = 0;
   f->d_adj_q = f->d_adj_gq = f->d_adj_gw = f->d_adj_w = f->d_adj_dq = f->d_adj_dx = nullptr;
   f->grad_q_valid = false;
+  f->pos_on_device = false;
 }
 
 void free_device(rtfmm_fmm* f) {
@@ -932,6 +936,7 @@ int rtfmm_b200_setup(rtfmm_fmm* f, int64_t n, const double* x, const double* q) 
   f->setup_done = true;
   f->device_ready = false;
   f->grad_q_valid = false;
+  f->pos_on_device = false;
   return RTFMM_OK;
 }
 
@@ -950,6 +955,7 @@ int rtfmm_b200_upload(rtfmm_fmm* f) {
     CK(cudaMemcpy(f->d_body64, b.data(), sizeof(double4) * b.size(), cudaMemcpyHostToDevice));
   }
   f->grad_q_valid = false;
+  f->pos_on_device = true;
   return RTFMM_OK;
 }
 
@@ -994,10 +1000,16 @@ int rtfmm_b200_evaluate(rtfmm_fmm* f, const double* q, double* phi, double* grad
     if (rc) return rc;
   }
   CK(cudaSetDevice(f->dev));
-  // host -> device (input order), then gather into tree order on the device
-  CK(cudaMemcpyAsync(f->d_xin, f->h_xin, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, f->s0));
+  // host -> device (input order), then into tree order on the device; the
+  // positions move only on the first call after set-up
   CK(cudaMemcpyAsync(f->d_qin, q ? q : f->q_in.data(), sizeof(double) * n, cudaMemcpyHostToDevice, f->s0));
-  CK(launch_gather_bodies(f->d_xin, f->d_qin, f->d_perm, (int)n, f->d_body64, f->s0));
+  if (f->pos_on_device) {
+    CK(launch_set_charges(f->d_body64, f->d_qin, f->d_perm, (int)n, f->s0));
+  } else {
+    CK(cudaMemcpyAsync(f->d_xin, f->h_xin, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, f->s0));
+    CK(launch_gather_bodies(f->d_xin, f->d_qin, f->d_perm, (int)n, f->d_body64, f->s0));
+    f->pos_on_device = true;
+  }
   int rc = enqueue_pass(f);
   if (rc) return rc;
   f->launches++;
@@ -1083,6 +1095,7 @@ int rtfmm_b200_adjoint(rtfmm_fmm* f, const double* w, double* dLdq, double* dLdx
   CK(cudaMemcpyAsync(f->d_qin, f->q_in.data(), sizeof(double) * n, cudaMemcpyHostToDevice, f->s0));
   CK(launch_gather_bodies(f->d_xin, f->d_qin, f->d_perm, (int)n, f->d_body64, f->s0));
   f->grad_q_valid = false;
+  f->pos_on_device = true;
   CK(cudaMemcpyAsync(f->d_adj_w, w, sizeof(double) * n, cudaMemcpyHostToDevice, f->s0));
   rc = adjoint_core(f, f->d_adj_w, f->d_adj_dq, f->d_adj_dx);
   if (rc) return rc;

@@ -46,6 +46,10 @@
 #ifndef HAD_MINB
 #define HAD_MINB 2
 #endif
+// FP32 Hadamard: FP64 accumulators in shared memory (1) or registers (0)
+#ifndef HAD_ACC_SMEM
+#define HAD_ACC_SMEM 0
+#endif
 // FP64 operator application: output rows per block (64 or 128), FP64
 // tensor-core (mma.sync) inner product
 #ifndef APPLY_TM
@@ -908,9 +912,11 @@ __global__ void __launch_bounds__(256)
 template <typename T> struct HadCfg;
 template <> struct HadCfg<float> {
   static constexpr int TT = HAD_TT, DF = HAD_DF, THREADS = 256 / HAD_TT, MINB = HAD_MINB;
+  static constexpr bool ACC_SMEM = HAD_ACC_SMEM;
 };
 template <> struct HadCfg<double> {
   static constexpr int TT = 1, DF = 1, THREADS = 256, MINB = 1;
+  static constexpr bool ACC_SMEM = false;
 };
 
 template <typename T>
@@ -997,22 +1003,38 @@ __global__ void __launch_bounds__(HadCfg<T>::THREADS, HadCfg<T>::MINB)
   }
   __syncthreads();
   if (t0 >= ntar) return;
-  double ar[TT][8], ai[TT][8];
   T pr[TT][8], pi[TT][8];
 #pragma unroll
   for (int u = 0; u < TT; ++u)
 #pragma unroll
+    for (int i = 0; i < 8; ++i) pr[u][i] = pi[u][i] = T(0);
+  // FP64 accumulators: registers, or one shared-memory column per thread
+  constexpr bool kAccS = HadCfg<T>::ACC_SMEM;
+  __shared__ double accs[kAccS ? TT * 16 : 1][NT];
+  double ar[TT][8], ai[TT][8];
+#pragma unroll
+  for (int u = 0; u < TT; ++u)
+#pragma unroll
     for (int i = 0; i < 8; ++i) {
-      ar[u][i] = ai[u][i] = 0.0;
-      pr[u][i] = pi[u][i] = T(0);
+      if constexpr (kAccS) {
+        accs[u * 16 + 2 * i][threadIdx.x] = 0.0;
+        accs[u * 16 + 2 * i + 1][threadIdx.x] = 0.0;
+      } else {
+        ar[u][i] = ai[u][i] = 0.0;
+      }
     }
   auto flush = [&]() {
 #pragma unroll
     for (int u = 0; u < TT; ++u)
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
-        ar[u][i] += (double)pr[u][i];
-        ai[u][i] += (double)pi[u][i];
+        if constexpr (kAccS) {
+          accs[u * 16 + 2 * i][threadIdx.x] += (double)pr[u][i];
+          accs[u * 16 + 2 * i + 1][threadIdx.x] += (double)pi[u][i];
+        } else {
+          ar[u][i] += (double)pr[u][i];
+          ai[u][i] += (double)pi[u][i];
+        }
         pr[u][i] = pi[u][i] = T(0);
       }
   };
@@ -1044,8 +1066,13 @@ __global__ void __launch_bounds__(HadCfg<T>::THREADS, HadCfg<T>::MINB)
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
       C2 v;
-      v.x = (T)ar[u][i];
-      v.y = (T)ai[u][i];
+      if constexpr (kAccS) {
+        v.x = (T)accs[u * 16 + 2 * i][threadIdx.x];
+        v.y = (T)accs[u * 16 + 2 * i + 1][threadIdx.x];
+      } else {
+        v.x = (T)ar[u][i];
+        v.y = (T)ai[u][i];
+      }
       out[i] = v;
     }
   }
@@ -1213,6 +1240,15 @@ __global__ void k_swap_charges(double4* __restrict__ body64, const double* __res
   if (i >= n) return;
   qsave[i] = body64[i].w;
   body64[i].w = w[perm[i]];
+}
+
+// New charges (input order) for bodies whose positions are already on the
+// device in tree order.
+__global__ void k_set_charges(double4* __restrict__ body64, const double* __restrict__ q,
+                              const int64_t* __restrict__ perm, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  body64[i].w = q[perm[i]];
 }
 
 __global__ void k_restore_charges(double4* __restrict__ body64, const double* __restrict__ qsave, int n) {
@@ -1474,6 +1510,11 @@ cudaError_t launch_dipole(const double4* body64, int n, double* partial, cudaStr
 cudaError_t launch_swap_charges(double4* body64, const double* w, const int64_t* perm, int n, double* qsave,
                                 cudaStream_t st) {
   if (n > 0) k_swap_charges<<<cdiv(n, 256), 256, 0, st>>>(body64, w, perm, n, qsave);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_set_charges(double4* body64, const double* q, const int64_t* perm, int n, cudaStream_t st) {
+  if (n > 0) k_set_charges<<<cdiv(n, 256), 256, 0, st>>>(body64, q, perm, n);
   return cudaGetLastError();
 }
 

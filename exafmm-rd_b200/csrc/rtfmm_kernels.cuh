@@ -106,6 +106,8 @@ cudaError_t launch_dipole(const double4* body64, int n, double* partial /*>= 4*1
 cudaError_t launch_swap_charges(double4* body64, const double* w, const int64_t* perm, int n, double* qsave,
                                 cudaStream_t st);
 cudaError_t launch_restore_charges(double4* body64, const double* qsave, int n, cudaStream_t st);
+// new charges (input order) into bodies whose positions are on the device
+cudaError_t launch_set_charges(double4* body64, const double* q, const int64_t* perm, int n, cudaStream_t st);
 cudaError_t launch_adj_combine(const int64_t* perm, const double* w, const double* qsave, const double* grad_q,
                                const double* grad_w, int n, double* dLdx, cudaStream_t st);
 cudaError_t launch_post(const double* phi_far, const double* grad_far, const double* phi_near,

@@ -100,8 +100,9 @@ int rtfmm_b200_destroy(rtfmm_fmm* fmm);
 int rtfmm_b200_setup(rtfmm_fmm* fmm, int64_t n, const double* x, const double* q);
 
 /*
- * The evaluation pass with host buffers: copies q (and the positions the
- * tree was built on) to the device, runs P2M, M2M, M2L, L2L, L2P and P2P
+ * The evaluation pass with host buffers: copies q (and, on the first call
+ * after setup, the positions the tree was built on; they then stay on the
+ * device) to the device, runs P2M, M2M, M2L, L2L, L2P and P2P
  * (the hot block, 3dpp/src/fmm.cpp:51-60), then the dipole correction, the
  * 1/(4 pi) scaling and the re-sort (fmm.cpp:75-80) on the device, and copies
  * phi (n) and grad (n*3) back.  q may be NULL to reuse the charges given to
