@@ -38,17 +38,17 @@
 // FP32 Hadamard: targets per thread, directions per FP32 partial sum,
 // resident blocks per SM
 #ifndef HAD_TT
-#define HAD_TT 1
+#define HAD_TT 2
 #endif
 #ifndef HAD_DF
-#define HAD_DF 2
+#define HAD_DF 8
 #endif
 #ifndef HAD_MINB
-#define HAD_MINB 2
+#define HAD_MINB 4
 #endif
 // FP32 Hadamard: FP64 accumulators in shared memory (1) or registers (0)
 #ifndef HAD_ACC_SMEM
-#define HAD_ACC_SMEM 0
+#define HAD_ACC_SMEM 1
 #endif
 // FP64 operator application: output rows per block (64 or 128), FP64
 // tensor-core (mma.sync) inner product
