@@ -65,6 +65,10 @@ struct ApplyCall {
 //   adjoint image levels: the transposes swap roles, so the upward step uses
 //   M2M_img[13] (the transpose of the forward L2L_img) and the downward step
 //   the transposed 27-image sum
+#ifndef STREAM_PRIO
+#define STREAM_PRIO 1
+#endif
+
 // Largest P at which the FP32-mixed form runs the 8x8 FFT-M2L in FP32 (its
 // gradient error stays below 1e-5 on uniform inputs up to P = 8; 3e-5 at 10).
 constexpr int kM2L32MaxP = 8;
@@ -491,8 +495,18 @@ int ensure_device(rtfmm_fmm* f) {
     free_device(f);
     CK(cudaSetDevice(f->args.device));
     f->dev = f->args.device;
+    // the far field (a chain of dependent kernels, s0) at the highest
+    // priority, P2P (one large independent kernel, s1) at the lowest, so that
+    // pending P2P blocks fill the SMs the far-field chain leaves idle
+    int prio_lo = 0, prio_hi = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+#if STREAM_PRIO
+    CK(cudaStreamCreateWithPriority(&f->s0, cudaStreamNonBlocking, prio_hi));
+    CK(cudaStreamCreateWithPriority(&f->s1, cudaStreamNonBlocking, prio_lo));
+#else
     CK(cudaStreamCreateWithFlags(&f->s0, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&f->s1, cudaStreamNonBlocking));
+#endif
     CK(cudaEventCreate(&f->ev_start));
     CK(cudaEventCreate(&f->ev_near0));
     CK(cudaEventCreate(&f->ev_near));
