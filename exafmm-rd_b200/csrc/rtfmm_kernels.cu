@@ -35,6 +35,9 @@
 #ifndef P2P_WARPS
 #define P2P_WARPS 4
 #endif
+#ifndef P2P_TILE
+#define P2P_TILE 32
+#endif
 // FP32 Hadamard: targets per thread, directions per FP32 partial sum,
 // resident blocks per SM
 #ifndef HAD_TT
@@ -145,6 +148,7 @@ __global__ void k_prep32(const double4* __restrict__ body64, const int* __restri
 // ---------------------------------------------------------------------------
 constexpr int kP2PWarps = P2P_WARPS;
 constexpr int kP2PUnroll = P2P_UNROLL;
+constexpr int kP2PTile = P2P_TILE;  // sources staged per tile (32 or 64)
 
 // Lanes of group `k0` (of G groups) take the tile's sources k0, k0+G, ...
 template <int G, bool MASK>
@@ -166,35 +170,42 @@ __device__ __forceinline__ void p2p32_tile(const float4* __restrict__ s, int k0,
   }
 }
 
+// One source pair k of a packed tile (layout below) against this lane's target.
+template <bool MASK>
+__device__ __forceinline__ void p2p32_pair2(const float4* __restrict__ s, int k, float2 px, float2 py, float2 pz,
+                                            float2& p, float2& fx, float2& fy, float2& fz) {
+  const float4 u = s[2 * k], v = s[2 * k + 1];
+  const float2 dx = __fadd2_rn(px, make_float2(u.x, u.y));
+  const float2 dy = __fadd2_rn(py, make_float2(u.z, u.w));
+  const float2 dz = __fadd2_rn(pz, make_float2(v.x, v.y));
+  float2 r2 = __fmul2_rn(dz, dz);
+  r2 = __ffma2_rn(dy, dy, r2);
+  r2 = __ffma2_rn(dx, dx, r2);
+  float2 ir = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+  if (MASK) {
+    ir.x = r2.x > 0.f ? ir.x : 0.f;
+    ir.y = r2.y > 0.f ? ir.y : 0.f;
+  }
+  const float2 qir = __fmul2_rn(make_float2(v.z, v.w), ir);
+  p = __fadd2_rn(p, qir);
+  const float2 q3 = __fmul2_rn(__fmul2_rn(qir, ir), ir);
+  fx = __ffma2_rn(q3, dx, fx);
+  fy = __ffma2_rn(q3, dy, fy);
+  fz = __ffma2_rn(q3, dz, fz);
+}
+
 // The same over source pairs with packed FP32x2 arithmetic (sm_100
 // FADD2/FMUL2/FFMA2): the tile is held as 16 pairs, pair k at s[2k] =
 // (-x, -x', -y, -y') and s[2k+1] = (-z, -z', q, q'); lanes of group k0 take
 // pairs k0, k0+G, ...  Per pair the arithmetic and its rounding are those of
 // p2p32_tile; only the sum over sources is split into two interleaved halves.
+// All 16 pairs of a tile are written (padding carries no charge and sits far
+// away); running the padding too, in fixed blocks, was measured slower.
 template <int G, bool MASK>
 __device__ __forceinline__ void p2p32_tile2(const float4* __restrict__ s, int k0, int npair, float2 px, float2 py,
                                             float2 pz, float2& p, float2& fx, float2& fy, float2& fz) {
 #pragma unroll kP2PUnroll
-  for (int k = k0; k < npair; k += G) {
-    const float4 u = s[2 * k], v = s[2 * k + 1];
-    const float2 dx = __fadd2_rn(px, make_float2(u.x, u.y));
-    const float2 dy = __fadd2_rn(py, make_float2(u.z, u.w));
-    const float2 dz = __fadd2_rn(pz, make_float2(v.x, v.y));
-    float2 r2 = __fmul2_rn(dz, dz);
-    r2 = __ffma2_rn(dy, dy, r2);
-    r2 = __ffma2_rn(dx, dx, r2);
-    float2 ir = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
-    if (MASK) {
-      ir.x = r2.x > 0.f ? ir.x : 0.f;
-      ir.y = r2.y > 0.f ? ir.y : 0.f;
-    }
-    const float2 qir = __fmul2_rn(make_float2(v.z, v.w), ir);
-    p = __fadd2_rn(p, qir);
-    const float2 q3 = __fmul2_rn(__fmul2_rn(qir, ir), ir);
-    fx = __ffma2_rn(q3, dx, fx);
-    fy = __ffma2_rn(q3, dy, fy);
-    fz = __ffma2_rn(q3, dz, fz);
-  }
+  for (int k = k0; k < npair; k += G) p2p32_pair2<MASK>(s, k, px, py, pz, p, fx, fy, fz);
 }
 
 // One work item: W = 32/G lanes per target group, G groups per warp.
@@ -214,10 +225,16 @@ __device__ __forceinline__ void p2p32_item(const float4* __restrict__ body32, co
   int e = list_off[it.leaf];
   const int e1 = list_off[it.leaf + 1];
   P2PSrc32 cur{}, nxt{};
-  float4 stage = pad;
+  // this lane stages sources c0 + lane + 32 h of the tile, h < kP2PTile / 32
+  constexpr int NH = kP2PTile / 32;
+  float4 stage[NH];
+#pragma unroll
+  for (int h = 0; h < NH; ++h) stage[h] = pad;
   if (e < e1) {
     cur = list[e];
-    if (lane < cur.bnum) stage = body32[cur.boff + lane];
+#pragma unroll
+    for (int h = 0; h < NH; ++h)
+      if (lane + 32 * h < cur.bnum) stage[h] = body32[cur.boff + lane + 32 * h];
   }
   if (e + 1 < e1) nxt = list[e + 1];
   int c0 = 0;
@@ -225,27 +242,34 @@ __device__ __forceinline__ void p2p32_item(const float4* __restrict__ body32, co
   float2 p = make_float2(0.f, 0.f), fx = p, fy = p, fz = p;
   float* sf = reinterpret_cast<float*>(sw) + 8 * (lane >> 1) + (lane & 1);
 #else
+  static_assert(kP2PTile == 32, "the scalar P2P form stages 32 sources");
   float p = 0.f, fx = 0.f, fy = 0.f, fz = 0.f;
 #endif
   while (e < e1) {
-    const int cnt = min(32, cur.bnum - c0);
+    const int cnt = min(kP2PTile, cur.bnum - c0);
     __syncwarp();
 #if P2P_PACKED
-    sf[0] = -stage.x;
-    sf[2] = -stage.y;
-    sf[4] = -stage.z;
-    sf[6] = stage.w;
+#pragma unroll
+    for (int h = 0; h < NH; ++h) {
+      sf[128 * h + 0] = -stage[h].x;
+      sf[128 * h + 2] = -stage[h].y;
+      sf[128 * h + 4] = -stage[h].z;
+      sf[128 * h + 6] = stage[h].w;
+    }
 #else
-    sw[lane] = stage;
+    sw[lane] = stage[0];
 #endif
     __syncwarp();
     // next tile: the rest of this source leaf, else the first of the next
-    const bool last = c0 + 32 >= cur.bnum;
-    stage = pad;
-    if (!last) {
-      if (lane < cur.bnum - c0 - 32) stage = body32[cur.boff + c0 + 32 + lane];
-    } else if (e + 1 < e1) {
-      if (lane < nxt.bnum) stage = body32[nxt.boff + lane];
+    const bool last = c0 + kP2PTile >= cur.bnum;
+#pragma unroll
+    for (int h = 0; h < NH; ++h) {
+      stage[h] = pad;
+      if (!last) {
+        if (lane + 32 * h < cur.bnum - c0 - kP2PTile) stage[h] = body32[cur.boff + c0 + kP2PTile + lane + 32 * h];
+      } else if (e + 1 < e1) {
+        if (lane + 32 * h < nxt.bnum) stage[h] = body32[nxt.boff + lane + 32 * h];
+      }
     }
     const float px = xt.x - cur.dx, py = xt.y - cur.dy, pz = xt.z - cur.dz;
 #if P2P_PACKED
@@ -281,7 +305,7 @@ __device__ __forceinline__ void p2p32_item(const float4* __restrict__ body32, co
       cur = nxt;
       if (e + 1 < e1) nxt = list[e + 1];
     } else {
-      c0 += 32;
+      c0 += kP2PTile;
     }
   }
   // sum the source groups (lanes ti, ti + W, ...)
@@ -305,7 +329,7 @@ __global__ void __launch_bounds__(32 * kP2PWarps, P2P_MINB)
     k_p2p32(const float4* __restrict__ body32, const P2PItem32* __restrict__ items, int nitems,
             const int* __restrict__ list_off, const P2PSrc32* __restrict__ list, double* __restrict__ phi,
             double* __restrict__ grad) {
-  __shared__ float4 sbuf[kP2PWarps][32];
+  __shared__ float4 sbuf[kP2PWarps][kP2PTile];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int item = blockIdx.x * kP2PWarps + warp;
   if (item >= nitems) return;  // warp-uniform

@@ -38,6 +38,7 @@ EXPORTS = (
     "rtfmm_b200_flush_l2", "rtfmm_b200_info", "rtfmm_b200_get_cells", "rtfmm_b200_get_perm",
     "rtfmm_b200_get_p2p", "rtfmm_b200_get_m2l", "rtfmm_b200_get_cell_vectors", "rtfmm_b200_get_operator",
     "rtfmm_b200_last_error", "rtfmm_b200_version", "rtfmm_b200_p2m_noalloc",
+    "rtfmm_b200_ewald_sampled", "rtfmm_b200_direct_sampled",
 )
 
 
@@ -83,6 +84,10 @@ def lib():
         "rtfmm_b200_download": (ctypes.c_int, [_vp, _dp, _dp]),
         "rtfmm_b200_adjoint": (ctypes.c_int, [_vp, _dp, _dp, _dp]),
         "rtfmm_b200_adjoint_device": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_float)]),
+        "rtfmm_b200_ewald_sampled": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, _dp, _dp, ctypes.c_double,
+                                                    ctypes.c_int, ctypes.c_int64, _lp, _dp, _dp]),
+        "rtfmm_b200_direct_sampled": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, _dp, _dp, ctypes.c_int64, _lp,
+                                                     _dp, _dp]),
         "rtfmm_b200_stage_times": (ctypes.c_int, [_vp, _dp, ctypes.c_int]),
         "rtfmm_b200_launch_count": (ctypes.c_int, [_vp, _lp]),
         "rtfmm_b200_flush_l2": (ctypes.c_int, [_vp]),
@@ -328,6 +333,32 @@ def generate_random_bodies(n, r, offset=(0.0, 0.0, 0.0), seed=5, zero_netcharge=
     if zero_netcharge and n:
         q = q - (sum(q.tolist()) / n)
     return x, q
+
+
+def ewald_sampled(x, q, cycle, targets, ksize=11, device=0):
+    """Ewald sum on sampled targets, FP64 on the GPU (EwaldSolver,
+    3dpp/src/ewald.cpp): (phi, grad) at bodies ``targets``, no 1/(4 pi)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    t = np.ascontiguousarray(targets, dtype=np.int64)
+    phi = np.empty(len(t))
+    grad = np.empty((len(t), 3))
+    _check(lib().rtfmm_b200_ewald_sampled(device, len(q), _ptr(x), _ptr(q), float(cycle), int(ksize), len(t),
+                                          _ptr(t, _lp), _ptr(phi), _ptr(grad)))
+    return phi, grad
+
+
+def direct_sampled(x, q, targets, device=0):
+    """Free-space direct sum on sampled targets, FP64 on the GPU: (phi, grad)
+    at bodies ``targets``, no 1/(4 pi)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    t = np.ascontiguousarray(targets, dtype=np.int64)
+    phi = np.empty(len(t))
+    grad = np.empty((len(t), 3))
+    _check(lib().rtfmm_b200_direct_sampled(device, len(q), _ptr(x), _ptr(q), len(t), _ptr(t, _lp), _ptr(phi),
+                                           _ptr(grad)))
+    return phi, grad
 
 
 def compare(p1, f1, q1, p2, f2, q2):

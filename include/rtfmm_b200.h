@@ -153,6 +153,27 @@ int rtfmm_b200_adjoint(rtfmm_fmm* fmm, const double* w, double* dLdq, double* dL
 int rtfmm_b200_adjoint_device(rtfmm_fmm* fmm, const double* w_dev, double* dLdq_dev, double* dLdx_dev,
                               float* ms);
 
+/*
+ * Accuracy references on sampled targets, FP64 on the GPU (device `device`),
+ * for sizes where a CPU sum would take hours.  x is n*3, q is n (host),
+ * targets holds nt body indices; phi (nt) and grad (nt*3) receive the
+ * potential and its gradient at those bodies, without 1/(4 pi) and without
+ * a dipole term.  Both allocate and free their own device memory.
+ *
+ * rtfmm_b200_ewald_sampled replaces EwaldSolver (3dpp/include/ewald.h,
+ * 3dpp/src/ewald.cpp): alpha = ksize/cycle, real-space sum over r < cycle/2,
+ * reciprocal sum over the (2 ksize + 1)^3 - 1 integer waves, self term;
+ * ksize in [1, 16] (the reference's default is 11).  The real-space image of
+ * a pair is the per-particle minimum image (the converged sum); the
+ * reference takes one image per pair of leaf cells, which can drop pairs
+ * that are close across the periodic boundary.  rtfmm_b200_direct_sampled is
+ * the free-space direct sum over all bodies.
+ */
+int rtfmm_b200_ewald_sampled(int device, int64_t n, const double* x, const double* q, double cycle, int ksize,
+                             int64_t nt, const int64_t* targets, double* phi, double* grad);
+int rtfmm_b200_direct_sampled(int device, int64_t n, const double* x, const double* q, int64_t nt,
+                              const int64_t* targets, double* phi, double* grad);
+
 /* Per-stage device times of the last pass, in ms, in this order:
  * prep, P2M, M2M, M2L_up, M2L_hadamard, M2L_down, L2L, L2P, P2P, post.
  * Writes min(cap, 10) values; returns the number of stages. */
