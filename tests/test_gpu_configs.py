@@ -9,13 +9,15 @@ size:
   P10  N=4000 uniform, P=10, ncrit=64, images=3: against the oracle (the
        P=10 operators: 488 surface points, a 19^3 convolution grid).
   C3   N=2^22 in 64 Gaussian blobs (sigma 0.02, wrapped), P=10, ncrit=128,
-       images=3 (deep adaptive tree): FP32-mixed against FP64 (3e-5), and
-       linearity in the charges in FP64 on the same tree.
+       images=3 (deep adaptive tree): FP32-mixed against FP64 (3e-5),
+       FP64 against the converged Ewald sum on sampled bodies, and linearity
+       in the charges in FP64 on the same tree.
   C5   200^3 rock-salt lattice (spacing a = 1/200, q = (-1)^(i+j+k)), P=10,
        ncrit=256, images=4.  Unjittered, the periodic potential at every site
        is -M q_i / a up to a constant, M = 1.747564594633182 the NaCl
        Madelung constant, and the field vanishes by symmetry.  Jittered by
-       U(+-0.1 a), FP32-mixed against FP64.
+       U(+-0.1 a), FP32-mixed against FP64 and both against the converged
+       Ewald sum on sampled bodies.
 
 Tolerances are relative L2 (the reference's compare metric) unless stated.
 At P=10 the check-to-equivalent operator's condition number (1.3e16)
@@ -100,6 +102,7 @@ def test_c3_blobs_mixed_vs_fp64_and_linearity(pkg):
     fm.close()
     assert l2(grad_m, grad_d) < 3e-5, l2(grad_m, grad_d)
     assert l2(phi_m - phi_m.mean(), phi_d - phi_d.mean()) < 1e-5
+    assert ewald_grad_error(pkg, x, q, grad_d) < 1e-4
     # linearity on the same tree: phi(q + 2 q2) = phi(q) + 2 phi(q2)
     q2 = np.random.default_rng(13).standard_normal(len(q))
     q2 -= q2.mean()
@@ -124,6 +127,15 @@ def test_c5_lattice_madelung(pkg, precision, tol_phi, tol_grad):
     assert float(np.abs(grad).max()) * a * a / MADELUNG_NACL < tol_grad
 
 
+def ewald_grad_error(pkg, x, q, grad, nsample=512, seed=9):
+    """Relative L2 error of an FMM gradient (1/(4 pi) scaled, no dipole
+    correction) against the converged Ewald sum on sampled bodies."""
+    t = np.random.default_rng(seed).choice(len(q), nsample, replace=False)
+    _, egrad = pkg.ewald_sampled(x, q, 1.0, t, ksize=11)
+    corr = 4 * np.pi / 3 * (q @ x)  # the dipole term of the Ewald (tin-foil) sum, L = 1
+    return l2(4 * np.pi * grad[t] - corr, egrad)
+
+
 def test_c5_jittered_mixed_vs_fp64(pkg):
     x, q = rock_salt(200, 0.1, 5)
     fd, phi_d, grad_d = solve(pkg, x, q, args(pkg, 10, 256, 4, 0))
@@ -132,3 +144,6 @@ def test_c5_jittered_mixed_vs_fp64(pkg):
     fm.close()
     assert l2(grad_m, grad_d) < 1e-5, l2(grad_m, grad_d)
     assert l2(phi_m - phi_m.mean(), phi_d - phi_d.mean()) < 1e-5
+    # against the converged Ewald sum (measured 3.7e-7 FP64, 2.0e-6 mixed)
+    assert ewald_grad_error(pkg, x, q, grad_d) < 2e-6
+    assert ewald_grad_error(pkg, x, q, grad_m) < 1e-5
