@@ -271,7 +271,7 @@ void build_tables(rtfmm_fmm* f) {
     return v;
   };
   std::vector<std::vector<P2PEntry>> leaf_lists(f->leaves.size());
-  for (auto& kv : p.p2p) {
+  for (const auto& kv : p.p2p) {
     const std::vector<int> tl = leaves_under(kv.first);
     for (const P2PEntry& e : kv.second) {
       const std::vector<int>& sl = leaves_under(e.src);
@@ -434,7 +434,7 @@ void build_tables(rtfmm_fmm* f) {
   // FFT-M2L lists (m2l_fft_precompute_t, kernel.cpp:1153-1245)
   std::map<int, int> s8, s27;
   std::vector<int> t8cells, t27cells;
-  for (auto& kv : p.m2l) {
+  for (const auto& kv : p.m2l) {
     bool single = false, normal = false;
     for (const M2LEntry& e : kv.second) (e.single ? single : normal) = true;
     if (normal) t8cells.push_back(kv.first);
@@ -1219,7 +1219,7 @@ int rtfmm_b200_get_p2p(rtfmm_fmm* f, int32_t* ints, double* off) {
   if (!f) return fail(RTFMM_EINVAL, "null handle");
   if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");
   size_t e = 0;
-  for (auto& kv : f->plan.p2p)
+  for (const auto& kv : f->plan.p2p)
     for (const P2PEntry& s : kv.second) {
       if (ints) {
         ints[2 * e] = kv.first;
@@ -1236,7 +1236,7 @@ int rtfmm_b200_get_m2l(rtfmm_fmm* f, int32_t* ints, double* off) {
   if (!f) return fail(RTFMM_EINVAL, "null handle");
   if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");
   size_t e = 0;
-  for (auto& kv : f->plan.m2l)
+  for (const auto& kv : f->plan.m2l)
     for (const M2LEntry& s : kv.second) {
       if (ints) {
         ints[3 * e] = kv.first;

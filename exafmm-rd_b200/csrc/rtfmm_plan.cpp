@@ -5,6 +5,7 @@
 #include "rtfmm_plan.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <unordered_map>
@@ -34,6 +35,52 @@ static V3 child_center(const V3& xp, double rp, int octant) {
   return c;
 }
 
+// Splits one cell's bodies into its octants: a stable counting partition of
+// perm[b0, b0+nb) by the octant code 4(x>cx)+2(y>cy)+(z>cz).  Large cells are
+// partitioned by all threads (per-thread counts over contiguous chunks, so the
+// result is the same stable order); small ones by the calling thread.
+static void split_cell(const double* xin, const Cell& cell, std::vector<int64_t>& perm, std::vector<int64_t>& tmp,
+                       std::vector<uint8_t>& code, int count[8], bool parallel) {
+  const int64_t b0 = cell.boff, nb = cell.bnum;
+  auto octant = [&](int64_t i) {
+    const double* p = xin + 3 * perm[b0 + i];
+    return ((p[0] > cell.x[0]) << 2) + ((p[1] > cell.x[1]) << 1) + (p[2] > cell.x[2]);
+  };
+  int nt = 1;
+#ifdef _OPENMP
+  if (parallel) nt = std::max(1, std::min(omp_get_max_threads(), (int)(nb / 16384)));
+#endif
+  std::vector<int64_t> cnt((size_t)nt * 8, 0), off((size_t)nt * 8, 0);
+#pragma omp parallel for num_threads(nt) schedule(static, 1) if (nt > 1)
+  for (int t = 0; t < nt; ++t) {
+    const int64_t i0 = nb * t / nt, i1 = nb * (t + 1) / nt;
+    for (int64_t i = i0; i < i1; ++i) {
+      const int o = octant(i);
+      code[b0 + i] = (uint8_t)o;
+      cnt[(size_t)t * 8 + o]++;
+    }
+  }
+  int64_t run = 0;
+  for (int o = 0; o < 8; ++o) {
+    int64_t c = 0;
+    for (int t = 0; t < nt; ++t) {
+      off[(size_t)t * 8 + o] = run + c;
+      c += cnt[(size_t)t * 8 + o];
+    }
+    count[o] = (int)c;
+    run += c;
+  }
+#pragma omp parallel for num_threads(nt) schedule(static, 1) if (nt > 1)
+  for (int t = 0; t < nt; ++t) {
+    const int64_t i0 = nb * t / nt, i1 = nb * (t + 1) / nt;
+    int64_t fill[8];
+    for (int o = 0; o < 8; ++o) fill[o] = off[(size_t)t * 8 + o];
+    for (int64_t i = i0; i < i1; ++i) tmp[b0 + fill[code[b0 + i]]++] = perm[b0 + i];
+  }
+#pragma omp parallel for num_threads(nt) schedule(static) if (nt > 1)
+  for (int64_t i = 0; i < nb; ++i) perm[b0 + i] = tmp[b0 + i];
+}
+
 std::string build_tree(Plan& plan, const double* xin, const double* qin) {
   const int64_t n = plan.n;
   const Args& a = plan.args;
@@ -54,51 +101,65 @@ std::string build_tree(Plan& plan, const double* xin, const double* qin) {
   root.boff = 0;
   root.bnum = (int)n;
   plan.cells.push_back(root);
-  size_t head = 0;
-  while (head < plan.cells.size()) {
-    int c = (int)head++;
-    Cell cell = plan.cells[c];
-    if (cell.bnum <= a.ncrit) continue;
-    if (cell.depth >= kMaxDepth)
-      return "octree deeper than 40 levels: more than ncrit bodies share a position";
-    const int b0 = cell.boff, nb = cell.bnum;
-    int count[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int i = 0; i < nb; ++i) {
-      const double* p = xin + 3 * plan.perm[b0 + i];
-      int o = ((p[0] > cell.x[0]) << 2) + ((p[1] > cell.x[1]) << 1) + (p[2] > cell.x[2]);
-      code[b0 + i] = (uint8_t)o;
-      count[o]++;
+  // Breadth-first, one level at a time: the cells of a level split their own
+  // body ranges independently (in parallel), then their children are appended
+  // in cell order, octants in order -- the queue order of the reference's
+  // breadth-first build, so cells and the body permutation are the same.
+  size_t lev0 = 0, lev1 = 1;
+  const int64_t big = 1 << 18;
+  while (lev0 < lev1) {
+    const int nl = (int)(lev1 - lev0);
+    std::vector<std::array<int, 8>> counts(nl);
+    int deep = 0;
+    for (int k = 0; k < nl; ++k) {
+      const Cell& c = plan.cells[lev0 + k];
+      if (c.bnum > a.ncrit && c.depth >= kMaxDepth) deep = 1;
     }
-    int start[8], nchild = 0, s = 0;
-    for (int o = 0; o < 8; ++o) {
-      start[o] = s;
-      s += count[o];
-      if (count[o] > 0) nchild++;
+    if (deep) return "octree deeper than 40 levels: more than ncrit bodies share a position";
+    // large cells: every thread on one cell; the rest: one cell per thread
+    for (int k = 0; k < nl; ++k) {
+      const Cell& c = plan.cells[lev0 + k];
+      if (c.bnum > a.ncrit && c.bnum >= big) split_cell(xin, c, plan.perm, tmp, code, counts[k].data(), true);
     }
-    int fill[8];
-    std::memcpy(fill, start, sizeof(fill));
-    for (int i = 0; i < nb; ++i) tmp[fill[code[b0 + i]]++] = plan.perm[b0 + i];
-    std::memcpy(&plan.perm[b0], tmp.data(), sizeof(int64_t) * nb);
-    const int insert = (int)plan.cells.size();
-    plan.cells[c].coff = insert;
-    plan.cells[c].cnum = nchild;
-    for (int o = 0; o < 8; ++o) {
-      if (count[o] == 0) continue;
-      Cell ch;
-      ch.octant = o;
-      ch.depth = cell.depth + 1;
-      ch.r = cell.r / 2;
-      ch.x = child_center(cell.x, cell.r, o);
-      ch.coff = 0;
-      ch.cnum = 0;
-      ch.boff = b0 + start[o];
-      ch.bnum = count[o];
-      plan.cells.push_back(ch);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int k = 0; k < nl; ++k) {
+      const Cell& c = plan.cells[lev0 + k];
+      if (c.bnum > a.ncrit && c.bnum < big) split_cell(xin, c, plan.perm, tmp, code, counts[k].data(), false);
     }
+    for (int k = 0; k < nl; ++k) {
+      const int ci = (int)(lev0 + k);
+      const Cell cell = plan.cells[ci];
+      if (cell.bnum <= a.ncrit) continue;
+      const int* count = counts[k].data();
+      int nchild = 0, s = 0;
+      const int insert = (int)plan.cells.size();
+      for (int o = 0; o < 8; ++o) {
+        if (count[o] == 0) {
+          continue;
+        }
+        Cell ch;
+        ch.octant = o;
+        ch.depth = cell.depth + 1;
+        ch.r = cell.r / 2;
+        ch.x = child_center(cell.x, cell.r, o);
+        ch.coff = 0;
+        ch.cnum = 0;
+        ch.boff = cell.boff + s;
+        ch.bnum = count[o];
+        plan.cells.push_back(ch);
+        s += count[o];
+        nchild++;
+      }
+      plan.cells[ci].coff = insert;
+      plan.cells[ci].cnum = nchild;
+    }
+    lev0 = lev1;
+    lev1 = plan.cells.size();
   }
   plan.ntree = (int)plan.cells.size();
   plan.x.resize(3 * n);
   plan.q.resize(n);
+#pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < n; ++i) {
     const int64_t k = plan.perm[i];
     plan.x[3 * i + 0] = xin[3 * k + 0];
@@ -135,40 +196,30 @@ struct Walker {
   }
   bool leaf(int c) const { return p.cells[c].cnum == 0; }
 
-  // horizontal_origin (traverser.cpp:70-148) with an explicit stack; children
+  // horizontal_origin (traverser.cpp:70-148) as a stack of frames; children
   // are visited in the reference's recursion order.  M2P/P2L cases become P2P
   // (traverser.cpp:75-86); M2L pairs of the dual walk are counted only (the
   // M2L of the pass uses the parent map).
-  void horizontal_origin(int tc0, int sc0, int tcp0, int scp0, const V3& off) {
-    struct Frame { int tc, sc, tcp, scp; };
-    std::vector<Frame> stack;
-    stack.push_back({tc0, sc0, tcp0, scp0});
-    while (!stack.empty()) {
-      Frame f = stack.back();
-      stack.pop_back();
-      int divide = 0;
-      const Cell& T = p.cells[f.tc];
-      const Cell& S = p.cells[f.sc];
-      if (!adjacent(f.tc, f.sc, off)) {
-        if (adjacent(f.tc, f.scp, off) && leaf(f.tc) && p.cells[f.scp].depth >= T.depth) {
-          p.p2p[f.tc].push_back({f.sc, off});
-        } else if (adjacent(f.tcp, f.sc, off) && leaf(f.sc) && p.cells[f.tcp].depth >= S.depth) {
-          p.p2p[f.tc].push_back({f.sc, off});
-        } else if (neighbour(f.tcp, f.scp, off)) {
-          // an M2L pair of the dual walk; served by the parent map
-        } else {
-          if (leaf(f.tc) && leaf(f.sc)) {
-          } else if (!leaf(f.tc) && leaf(f.sc)) {
-            divide = 1;
-          } else if (leaf(f.tc) && !leaf(f.sc)) {
-            divide = 2;
-          } else {
-            divide = T.r >= S.r ? 1 : 2;
-          }
-        }
+  struct Frame {
+    int tc, sc, tcp, scp;
+  };
+  // One frame: returns 1 and sets *hit for a P2P pair, or writes the child
+  // frames in visiting order to kids (returning -count), or returns 0.
+  int step(const Frame& f, const V3& off, int* hit, Frame* kids) const {
+    int divide = 0;
+    const Cell& T = p.cells[f.tc];
+    const Cell& S = p.cells[f.sc];
+    if (!adjacent(f.tc, f.sc, off)) {
+      if (adjacent(f.tc, f.scp, off) && leaf(f.tc) && p.cells[f.scp].depth >= T.depth) {
+        *hit = f.sc;
+        return 1;
+      } else if (adjacent(f.tcp, f.sc, off) && leaf(f.sc) && p.cells[f.tcp].depth >= S.depth) {
+        *hit = f.sc;
+        return 1;
+      } else if (neighbour(f.tcp, f.scp, off)) {
+        // an M2L pair of the dual walk; served by the parent map
       } else {
         if (leaf(f.tc) && leaf(f.sc)) {
-          p.p2p[f.tc].push_back({f.sc, off});
         } else if (!leaf(f.tc) && leaf(f.sc)) {
           divide = 1;
         } else if (leaf(f.tc) && !leaf(f.sc)) {
@@ -177,12 +228,91 @@ struct Walker {
           divide = T.r >= S.r ? 1 : 2;
         }
       }
-      if (divide == 1) {
-        for (int i = T.cnum - 1; i >= 0; --i) stack.push_back({T.coff + i, f.sc, f.tc, f.scp});
-      } else if (divide == 2) {
-        for (int i = S.cnum - 1; i >= 0; --i) stack.push_back({f.tc, S.coff + i, f.tcp, f.sc});
+    } else {
+      if (leaf(f.tc) && leaf(f.sc)) {
+        *hit = f.sc;
+        return 1;
+      } else if (!leaf(f.tc) && leaf(f.sc)) {
+        divide = 1;
+      } else if (leaf(f.tc) && !leaf(f.sc)) {
+        divide = 2;
+      } else {
+        divide = T.r >= S.r ? 1 : 2;
       }
     }
+    if (divide == 1) {
+      for (int i = 0; i < T.cnum; ++i) kids[i] = {T.coff + i, f.sc, f.tc, f.scp};
+      return -T.cnum;
+    }
+    if (divide == 2) {
+      for (int i = 0; i < S.cnum; ++i) kids[i] = {f.tc, S.coff + i, f.tcp, f.sc};
+      return -S.cnum;
+    }
+    return 0;
+  }
+
+  // The walk below one frame, its P2P pairs (target, source) appended in the
+  // order the recursion emits them.
+  void walk(const Frame& f0, const V3& off, std::vector<std::pair<int, int>>& out) const {
+    std::vector<Frame> stack;
+    stack.push_back(f0);
+    Frame kids[8];
+    while (!stack.empty()) {
+      const Frame f = stack.back();
+      stack.pop_back();
+      int hit = -1;
+      const int r = step(f, off, &hit, kids);
+      if (r == 1) {
+        out.push_back({f.tc, hit});
+      } else if (r < 0) {
+        for (int i = -r - 1; i >= 0; --i) stack.push_back(kids[i]);
+      }
+    }
+  }
+
+  // The walks of all root frames (one per periodic offset), split into the
+  // subtrees of their first frames and run in parallel.  A frame either emits
+  // one pair or divides, so the output of a walk is the concatenation of its
+  // subtrees' outputs in visiting order; they are merged in that order, and
+  // the lists are the ones the sequential recursion builds.
+  void walks(const std::vector<Frame>& roots, const std::vector<V3>& offs) {
+    struct Item {
+      Frame f;
+      int walk;
+      int hit;  // >= 0: an emitted pair, no frame
+    };
+    std::vector<Item> items;
+    for (size_t w = 0; w < roots.size(); ++w) items.push_back({roots[w], (int)w, -1});
+    Frame kids[8];
+    for (int round = 0; round < 6 && items.size() < 4096; ++round) {
+      std::vector<Item> next;
+      next.reserve(items.size() * 8);
+      for (const Item& it : items) {
+        if (it.hit >= 0) {
+          next.push_back(it);
+          continue;
+        }
+        int hit = -1;
+        const int r = step(it.f, offs[(size_t)it.walk], &hit, kids);
+        if (r == 1) {
+          next.push_back({it.f, it.walk, hit});
+        } else if (r < 0) {
+          for (int i = 0; i < -r; ++i) next.push_back({kids[i], it.walk, -1});
+        }
+      }
+      items.swap(next);
+    }
+    std::vector<std::vector<std::pair<int, int>>> outs(items.size());
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int i = 0; i < (int)items.size(); ++i) {
+      const Item& it = items[(size_t)i];
+      if (it.hit >= 0)
+        outs[(size_t)i].push_back({it.f.tc, it.hit});
+      else
+        walk(it.f, offs[(size_t)it.walk], outs[(size_t)i]);
+    }
+    for (size_t i = 0; i < items.size(); ++i)
+      for (const auto& pr : outs[i]) p.p2p[pr.first].push_back({pr.second, offs[(size_t)items[i].walk]});
   }
 };
 
@@ -197,7 +327,7 @@ void traverse(Plan& plan) {
   // The depth -1 super-cell exists before the tree-level M2L parent map is
   // built (traverser.cpp:30-35); deeper image cells are added afterwards.
   if (a.images == 0) {
-    w.horizontal_origin(0, 0, 0, 0, V3{0, 0, 0});
+    w.walks({{0, 0, 0, 0}}, {V3{0, 0, 0}});
   } else {
     Cell c;
     c.octant = 13;
@@ -210,12 +340,15 @@ void traverse(Plan& plan) {
     c.bnum = plan.cells[0].bnum;
     plan.cells.push_back(c);
     const int cidx = (int)plan.cells.size() - 1;
+    std::vector<Walker::Frame> roots;
+    std::vector<V3> offs;
     for (int pz = -1; pz <= 1; ++pz)
       for (int py = -1; py <= 1; ++py)
         for (int px = -1; px <= 1; ++px) {
-          V3 off{px * cycle, py * cycle, pz * cycle};
-          w.horizontal_origin(0, 0, cidx, cidx, off);
+          roots.push_back({0, 0, cidx, cidx});
+          offs.push_back(V3{px * cycle, py * cycle, pz * cycle});
         }
+    w.walks(roots, offs);
   }
 
   // M2L parent map over the tree cells (make_M2L_parent_map and the
@@ -305,9 +438,9 @@ void traverse(Plan& plan) {
     plan.dmax = std::max(plan.dmax, c.depth);
   }
   plan.n_p2p = 0;
-  for (auto& kv : plan.p2p) plan.n_p2p += (int64_t)kv.second.size();
+  for (const auto& kv : plan.p2p) plan.n_p2p += (int64_t)kv.second.size();
   plan.n_m2l = 0;
-  for (auto& kv : plan.m2l) plan.n_m2l += (int64_t)kv.second.size();
+  for (const auto& kv : plan.m2l) plan.n_m2l += (int64_t)kv.second.size();
 }
 
 // ---------------------------------------------------------------------------

@@ -55,6 +55,52 @@ struct Operators {
   std::vector<int> surf_ijk;       // ns x 3 lattice coordinates (x,y,z)
 };
 
+// Per-cell lists indexed by cell: a vector of vectors that reads like the
+// map it replaces (lists[c] grows the index; iteration visits the cells with
+// a non-empty list in cell order as (first = cell, second = list)).
+template <typename E>
+struct CellLists {
+  std::vector<std::vector<E>> v;
+  std::vector<E>& operator[](int c) {
+    if (c >= (int)v.size()) v.resize((size_t)c + 1);
+    return v[(size_t)c];
+  }
+  const std::vector<E>& at(int c) const {
+    static const std::vector<E> empty;
+    return c < (int)v.size() ? v[(size_t)c] : empty;
+  }
+  void clear() { v.clear(); }
+  size_t size() const {  // cells with a non-empty list
+    size_t k = 0;
+    for (const auto& l : v) k += !l.empty();
+    return k;
+  }
+  struct Item {
+    int first;
+    const std::vector<E>& second;
+  };
+  struct Iter {
+    const CellLists* L;
+    int i;
+    void skip() {
+      while (i < (int)L->v.size() && L->v[(size_t)i].empty()) ++i;
+    }
+    Item operator*() const { return {i, L->v[(size_t)i]}; }
+    Iter& operator++() {
+      ++i;
+      skip();
+      return *this;
+    }
+    bool operator!=(const Iter& o) const { return i != o.i; }
+  };
+  Iter begin() const {
+    Iter it{this, 0};
+    it.skip();
+    return it;
+  }
+  Iter end() const { return Iter{this, (int)v.size()}; }
+};
+
 struct Args {
   int P = 4, ncrit = 16, images = 0;
   double cycle = 6.283185307179586;
@@ -73,8 +119,8 @@ struct Plan {
   std::vector<Cell> cells;         // tree cells, then image cells
   int ntree = 0;                   // cells before the image super-cells
   int dmin = 0, dmax = 0;
-  std::map<int, std::vector<P2PEntry>> p2p;
-  std::map<int, std::vector<M2LEntry>> m2l;
+  CellLists<P2PEntry> p2p;  // by target cell
+  CellLists<M2LEntry> m2l;  // by target parent
   int64_t n_p2p = 0, n_m2l = 0;
 };
 

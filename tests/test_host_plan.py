@@ -83,6 +83,14 @@ def test_tree_and_lists_match_oracle(pkg, oracle, kind, n, ncrit, images):
         assert tuple(reals[c, 1:]) == tuple(C.x[c])
     assert np.array_equal(f.perm(), F.perm)
     assert lists_of(f) == oracle_lists(F)
+    # each target's P2P list in the reference's recursion order (the order
+    # of the FP64 sums), also when the walk is split across threads
+    pi, po = f.p2p_lists()
+    got = {}
+    for (t, s_), o in zip(pi, po):
+        got.setdefault(int(t), []).append((int(s_), tuple(np.round(o, 12))))
+    want = {t: [(s_, tuple(np.round(off, 12))) for (s_, off) in l] for t, l in F.trav.p2p.items() if l}
+    assert got == want
 
 
 def test_m2l_parent_map_is_symmetric(pkg):
