@@ -279,14 +279,22 @@ void build_tables(rtfmm_fmm* f) {
         for (int sc : sl) leaf_lists[leaf_of_cell[t]].push_back({sc, e.off});
     }
   }
-  f->list_off.assign(f->leaves.size() + 1, 0);
-  f->list32.clear();
-  f->list64.clear();
-  f->items.clear();
-  f->items2.clear();
-  for (int l = 0; l < (int)f->leaves.size(); ++l) {
-    f->list_off[l] = (int)f->list32.size();
+  // CSR offsets and item offsets first, then every leaf's entries in parallel
+  const int nlf = (int)f->leaves.size();
+  f->list_off.assign(nlf + 1, 0);
+  std::vector<int> item_off(nlf + 1, 0);
+  for (int l = 0; l < nlf; ++l) {
+    f->list_off[l + 1] = f->list_off[l] + (int)leaf_lists[l].size();
+    item_off[l + 1] = item_off[l] + (f->leaves[l].bnum + 31) / 32;
+  }
+  f->list32.assign(f->list_off[nlf], P2PSrc32{});
+  f->list64.assign(f->list_off[nlf], P2PSrc64{});
+  f->items.assign(item_off[nlf], P2PItem{});
+  f->items2.assign(item_off[nlf], P2PItem32{});
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int l = 0; l < nlf; ++l) {
     const int c = f->leaves[l].cell;
+    int k = f->list_off[l];
     for (const P2PEntry& e : leaf_lists[l]) {
       const int sl = leaf_of_cell[e.src];
       const Cell& S = p.cells[e.src];
@@ -300,26 +308,27 @@ void build_tables(rtfmm_fmm* f) {
       a.boff = f->leaves[sl].boff;
       a.bnum = f->leaves[sl].bnum;
       a.pad = 0;
-      f->list32.push_back(a);
+      f->list32[k] = a;
       P2PSrc64 b;
       b.ox = e.off[0];
       b.oy = e.off[1];
       b.oz = e.off[2];
       b.leaf = sl;
       b.self = a.self;
-      f->list64.push_back(b);
+      f->list64[k] = b;
+      ++k;
     }
-    for (int t0 = 0; t0 < f->leaves[l].bnum; t0 += 32) f->items.push_back({l, t0});
     // FP32 items: 32 targets each; the last <= 16 targets of a leaf take a
     // narrower group (W = 16, 8 or 4 lanes) and split the sources 32/W ways
-    for (int t0 = 0; t0 < f->leaves[l].bnum; t0 += 32) {
+    int j = item_off[l];
+    for (int t0 = 0; t0 < f->leaves[l].bnum; t0 += 32, ++j) {
+      f->items[j] = {l, t0};
       const int rem = std::min(32, f->leaves[l].bnum - t0);
       int lw = 5;
       while (lw > 2 && rem <= (1 << (lw - 1))) --lw;
-      f->items2.push_back({l, f->leaves[l].boff + t0, rem, lw});
+      f->items2[j] = {l, f->leaves[l].boff + t0, rem, lw};
     }
   }
-  f->list_off[f->leaves.size()] = (int)f->list32.size();
 
   // batched operator applications
   f->idx_pool.clear();
