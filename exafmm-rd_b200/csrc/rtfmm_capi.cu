@@ -93,8 +93,7 @@ struct rtfmm_fmm {
   // host plan tables
   std::vector<LeafInfo> leaves;
   std::vector<int> body_leaf;
-  std::vector<P2PItem> items;    // 32 targets per item (FP64 P2P)
-  std::vector<P2PItem32> items2; // FP32 P2P items (target groups)
+  std::vector<P2PItem32> items2; // P2P work items (target groups), both precisions
   std::vector<int> list_off;
   std::vector<P2PSrc32> list32;
   std::vector<P2PSrc64> list64;
@@ -123,7 +122,6 @@ struct rtfmm_fmm {
   double *d_qeq = nullptr, *d_pchk = nullptr, *d_leafvec = nullptr, *d_leafvec2 = nullptr, *d_y = nullptr;
   double *d_far_phi = nullptr, *d_far_grad = nullptr, *d_near_phi = nullptr, *d_near_grad = nullptr;
   double *d_out_phi = nullptr, *d_out_grad = nullptr;
-  P2PItem* d_items = nullptr;
   P2PItem32* d_items2 = nullptr;
   int* d_list_off = nullptr;
   P2PSrc32* d_list32 = nullptr;
@@ -289,7 +287,6 @@ void build_tables(rtfmm_fmm* f) {
   }
   f->list32.assign(f->list_off[nlf], P2PSrc32{});
   f->list64.assign(f->list_off[nlf], P2PSrc64{});
-  f->items.assign(item_off[nlf], P2PItem{});
   f->items2.assign(item_off[nlf], P2PItem32{});
 #pragma omp parallel for schedule(dynamic, 64)
   for (int l = 0; l < nlf; ++l) {
@@ -315,6 +312,8 @@ void build_tables(rtfmm_fmm* f) {
       b.oz = e.off[2];
       b.leaf = sl;
       b.self = a.self;
+      b.boff = a.boff;
+      b.bnum = a.bnum;
       f->list64[k] = b;
       ++k;
     }
@@ -322,7 +321,6 @@ void build_tables(rtfmm_fmm* f) {
     // narrower group (W = 16, 8 or 4 lanes) and split the sources 32/W ways
     int j = item_off[l];
     for (int t0 = 0; t0 < f->leaves[l].bnum; t0 += 32, ++j) {
-      f->items[j] = {l, t0};
       const int rem = std::min(32, f->leaves[l].bnum - t0);
       int lw = 5;
       while (lw > 2 && rem <= (1 << (lw - 1))) --lw;
@@ -565,7 +563,6 @@ int upload_plan(rtfmm_fmm* f) {
   RC(dalloc(f, &f->d_near_grad, 3 * n));
   RC(dalloc(f, &f->d_out_phi, n));
   RC(dalloc(f, &f->d_out_grad, 3 * n));
-  RC(dupload(f, &f->d_items, f->items));
   RC(dupload(f, &f->d_items2, f->items2));
   RC(dupload(f, &f->d_list_off, f->list_off));
   RC(dupload(f, &f->d_list32, f->list32));
@@ -749,7 +746,7 @@ int enqueue_pass(rtfmm_fmm* f, bool adjoint = false, bool no_dipole = false) {
                       f->d_near_phi, f->d_near_grad, s1));
       f->launches += 1;
     } else {
-      CK(launch_p2p64(f->d_body64, f->d_leaves, f->d_items, (int)f->items.size(), f->d_list_off, f->d_list64,
+      CK(launch_p2p64(f->d_body64, f->d_items2, (int)f->items2.size(), f->d_list_off, f->d_list64,
                       f->d_near_phi, f->d_near_grad, s1));
       f->launches += 1;
     }

@@ -342,51 +342,95 @@ __global__ void __launch_bounds__(32 * kP2PWarps, P2P_MINB)
   }
 }
 
+// FP64 P2P, the same work items as the FP32 kernel (lane groups for a leaf's
+// last targets, next tile and list entry loaded during the current tile);
+// per pair the reference's arithmetic (dx = x_t - (x_s + offset),
+// kernel.cpp:283-290) in FP64 with the Newton-refined reciprocal square root.
+template <int G>
+__device__ __forceinline__ void p2p64_item(const double4* __restrict__ body64, const P2PItem32& it,
+                                           const int* __restrict__ list_off, const P2PSrc64* __restrict__ list,
+                                           double4* __restrict__ sw, int lane, double* __restrict__ phi,
+                                           double* __restrict__ grad) {
+  constexpr int W = 32 / G;
+  const int grp = lane / W, ti = lane % W;
+  const bool active = ti < it.nt;
+  const double4 zero = make_double4(0.0, 0.0, 0.0, 0.0);
+  const double4 xt = active ? body64[it.boff + ti] : zero;
+  double P = 0.0, Gx = 0.0, Gy = 0.0, Gz = 0.0;
+  int e = list_off[it.leaf];
+  const int e1 = list_off[it.leaf + 1];
+  P2PSrc64 cur{}, nxt{};
+  double4 stage = zero;
+  if (e < e1) {
+    cur = list[e];
+    if (lane < cur.bnum) stage = body64[cur.boff + lane];
+  }
+  if (e + 1 < e1) nxt = list[e + 1];
+  int c0 = 0;
+  while (e < e1) {
+    const int cnt = min(32, cur.bnum - c0);
+    __syncwarp();
+    sw[lane] = stage;
+    __syncwarp();
+    const bool last = c0 + 32 >= cur.bnum;
+    stage = zero;
+    if (!last) {
+      if (lane < cur.bnum - c0 - 32) stage = body64[cur.boff + c0 + 32 + lane];
+    } else if (e + 1 < e1) {
+      if (lane < nxt.bnum) stage = body64[nxt.boff + lane];
+    }
+#pragma unroll 4
+    for (int k = grp; k < cnt; k += G) {
+      const double4 b = sw[k];
+      const double dx = xt.x - (b.x + cur.ox), dy = xt.y - (b.y + cur.oy), dz = xt.z - (b.z + cur.oz);
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      const double ir = r2 > 0.0 ? rsqrt_nr<2>(r2) : 0.0;
+      const double qir = b.w * ir;
+      P += qir;
+      const double q3 = qir * ir * ir;
+      Gx += q3 * dx;
+      Gy += q3 * dy;
+      Gz += q3 * dz;
+    }
+    if (last) {
+      ++e;
+      c0 = 0;
+      cur = nxt;
+      if (e + 1 < e1) nxt = list[e + 1];
+    } else {
+      c0 += 32;
+    }
+  }
+#pragma unroll
+  for (int o = W; o < 32; o <<= 1) {
+    P += __shfl_xor_sync(0xffffffffu, P, o);
+    Gx += __shfl_xor_sync(0xffffffffu, Gx, o);
+    Gy += __shfl_xor_sync(0xffffffffu, Gy, o);
+    Gz += __shfl_xor_sync(0xffffffffu, Gz, o);
+  }
+  if (active && grp == 0) {
+    const int bi = it.boff + ti;
+    phi[bi] = P;
+    grad[3 * bi + 0] = -Gx;
+    grad[3 * bi + 1] = -Gy;
+    grad[3 * bi + 2] = -Gz;
+  }
+}
+
 __global__ void __launch_bounds__(32 * kP2PWarps)
-    k_p2p64(const double4* __restrict__ body64, const LeafInfo* __restrict__ leaves,
-            const P2PItem* __restrict__ items, int nitems, const int* __restrict__ list_off,
-            const P2PSrc64* __restrict__ list, double* __restrict__ phi, double* __restrict__ grad) {
+    k_p2p64(const double4* __restrict__ body64, const P2PItem32* __restrict__ items, int nitems,
+            const int* __restrict__ list_off, const P2PSrc64* __restrict__ list, double* __restrict__ phi,
+            double* __restrict__ grad) {
   __shared__ double4 sbuf[kP2PWarps][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int item = blockIdx.x * kP2PWarps + warp;
-  if (item >= nitems) return;
-  const P2PItem it = items[item];
-  const LeafInfo T = leaves[it.leaf];
-  const int t = it.t0 + lane;
-  const bool active = t < T.bnum;
-  const double4 xt = active ? body64[T.boff + t] : make_double4(0, 0, 0, 0);
-  double P = 0.0, Gx = 0.0, Gy = 0.0, Gz = 0.0;
-  const int e1 = list_off[it.leaf + 1];
-  for (int e = list_off[it.leaf]; e < e1; ++e) {
-    const P2PSrc64 src = list[e];
-    const LeafInfo S = leaves[src.leaf];
-    for (int c0 = 0; c0 < S.bnum; c0 += 32) {
-      const int cnt = min(32, S.bnum - c0);
-      __syncwarp();
-      if (lane < cnt) sbuf[warp][lane] = body64[S.boff + c0 + lane];
-      __syncwarp();
-#pragma unroll 4
-      for (int k = 0; k < cnt; ++k) {
-        const double4 b = sbuf[warp][k];
-        // dx = x_t - (x_s + offset), as p2p_1toN_256 forms it (kernel.cpp:283-290)
-        const double dx = xt.x - (b.x + src.ox), dy = xt.y - (b.y + src.oy), dz = xt.z - (b.z + src.oz);
-        const double r2 = dx * dx + dy * dy + dz * dz;
-        const double ir = r2 > 0.0 ? rsqrt_nr<2>(r2) : 0.0;
-        const double qir = b.w * ir;
-        P += qir;
-        const double q3 = qir * ir * ir;
-        Gx += q3 * dx;
-        Gy += q3 * dy;
-        Gz += q3 * dz;
-      }
-    }
-  }
-  if (active) {
-    const int b = T.boff + t;
-    phi[b] = P;
-    grad[3 * b + 0] = -Gx;
-    grad[3 * b + 1] = -Gy;
-    grad[3 * b + 2] = -Gz;
+  if (item >= nitems) return;  // warp-uniform
+  const P2PItem32 it = items[item];
+  switch (it.lw) {
+    case 5: p2p64_item<1>(body64, it, list_off, list, sbuf[warp], lane, phi, grad); break;
+    case 4: p2p64_item<2>(body64, it, list_off, list, sbuf[warp], lane, phi, grad); break;
+    case 3: p2p64_item<4>(body64, it, list_off, list, sbuf[warp], lane, phi, grad); break;
+    default: p2p64_item<8>(body64, it, list_off, list, sbuf[warp], lane, phi, grad); break;
   }
 }
 
@@ -1352,12 +1396,11 @@ cudaError_t launch_p2p32(const float4* body32, const P2PItem32* items, int nitem
   return cudaGetLastError();
 }
 
-cudaError_t launch_p2p64(const double4* body64, const LeafInfo* leaves, const P2PItem* items, int nitems,
-                         const int* list_off, const P2PSrc64* list, double* phi, double* grad,
-                         cudaStream_t st) {
+cudaError_t launch_p2p64(const double4* body64, const P2PItem32* items, int nitems, const int* list_off,
+                         const P2PSrc64* list, double* phi, double* grad, cudaStream_t st) {
   if (nitems > 0)
-    k_p2p64<<<cdiv(nitems, kP2PWarps), 32 * kP2PWarps, 0, st>>>(body64, leaves, items, nitems, list_off,
-                                                               list, phi, grad);
+    k_p2p64<<<cdiv(nitems, kP2PWarps), 32 * kP2PWarps, 0, st>>>(body64, items, nitems, list_off, list, phi,
+                                                               grad);
   return cudaGetLastError();
 }
 

@@ -16,13 +16,7 @@ struct LeafInfo {
   int boff, bnum;      // bodies in tree order
 };
 
-// P2P work item of the FP64 kernel: 32 targets of one leaf.
-struct P2PItem {
-  int leaf;   // leaf-table index of the target leaf
-  int t0;     // first target (offset inside the leaf)
-};
-
-// P2P work item of the FP32 kernel: nt <= W targets of one leaf, W = 1 << lw
+// P2P work item: nt <= W targets of one leaf, W = 1 << lw
 // lanes per target group; the 32/W groups of a warp split every source tile
 // between them, so a leaf's last few targets do not leave most lanes idle.
 struct P2PItem32 {
@@ -32,8 +26,9 @@ struct P2PItem32 {
   int lw;     // log2 W, W in {4, 8, 16, 32}
 };
 
-// One P2P list entry (source leaf) of a target leaf, FP32 form.  Carries the
-// source's body range so that the kernel reads bodies with one dependent load.
+// One P2P list entry (source leaf) of a target leaf, FP32 form.  Both forms
+// carry the source's body range so that the kernels read bodies with one
+// dependent load.
 struct alignas(16) P2PSrc32 {
   float dx, dy, dz;   // c_src + offset - c_tar, for leaf-relative FP32 positions
   int leaf;           // leaf-table index of the source leaf
@@ -45,6 +40,7 @@ struct P2PSrc64 {
   double ox, oy, oz;  // periodic offset added to the source positions
   int leaf;
   int self;
+  int boff, bnum;     // source bodies (tree order)
 };
 
 // Batched FP64 operator application (see k_apply_f64).
@@ -65,9 +61,8 @@ cudaError_t launch_prep32(const double4* body64, const int* body_leaf, const Lea
                           float4* body32, int n, cudaStream_t st);
 cudaError_t launch_p2p32(const float4* body32, const P2PItem32* items, int nitems, const int* list_off,
                          const P2PSrc32* list, double* phi, double* grad, cudaStream_t st);
-cudaError_t launch_p2p64(const double4* body64, const LeafInfo* leaves, const P2PItem* items, int nitems,
-                         const int* list_off, const P2PSrc64* list, double* phi, double* grad,
-                         cudaStream_t st);
+cudaError_t launch_p2p64(const double4* body64, const P2PItem32* items, int nitems, const int* list_off,
+                         const P2PSrc64* list, double* phi, double* grad, cudaStream_t st);
 // newton: Newton steps of the FP64 reciprocal square root (1: ~1e-13, for
 // the FP32-mixed form; 2: full FP64)
 cudaError_t launch_p2m_check(const double4* body64, const LeafInfo* leaves, int nleaf,
