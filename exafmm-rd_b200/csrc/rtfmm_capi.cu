@@ -998,6 +998,30 @@ int rtfmm_b200_evaluate_device(rtfmm_fmm* f, float* ms) {
   return RTFMM_OK;
 }
 
+int rtfmm_b200_forward_device(rtfmm_fmm* f, const double* q_dev, double* phi_dev, double* grad_dev, float* ms) {
+  if (!f) return fail(RTFMM_EINVAL, "null handle");
+  if (!f->setup_done || !f->device_ready || !f->pos_on_device)
+    return fail(RTFMM_ESTATE, "upload (or an evaluate) has not run");
+  if (ms) *ms = 0;
+  const int64_t n = f->plan.n;
+  if (n == 0) return RTFMM_OK;
+  CK(cudaSetDevice(f->dev));
+  if (q_dev) CK(launch_set_charges(f->d_body64, q_dev, f->d_perm, (int)n, f->s0));
+  int rc = enqueue_pass(f);
+  if (rc) return rc;
+  if (phi_dev) CK(cudaMemcpyAsync(phi_dev, f->d_out_phi, sizeof(double) * n, cudaMemcpyDeviceToDevice, f->s0));
+  if (grad_dev)
+    CK(cudaMemcpyAsync(grad_dev, f->d_out_grad, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, f->s0));
+  float t = 0;
+  rc = collect_times(f, &t);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(f->s0));
+  CK(cudaGetLastError());
+  if (ms) *ms = t;
+  f->pass_done = true;
+  return RTFMM_OK;
+}
+
 int rtfmm_b200_download(rtfmm_fmm* f, double* phi, double* grad) {
   if (!f) return fail(RTFMM_EINVAL, "null handle");
   if (!f->pass_done) return fail(RTFMM_ESTATE, "no pass has run");

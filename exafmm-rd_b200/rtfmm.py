@@ -33,7 +33,8 @@ STAGE_NAMES = ("prep", "P2M", "M2M", "M2L_up", "M2L_hadamard", "M2L_down", "L2L"
 EXPORTS = (
     "rtfmm_b200_default_args", "rtfmm_b200_create", "rtfmm_b200_destroy", "rtfmm_b200_setup",
     "rtfmm_b200_evaluate", "rtfmm_b200_solve", "rtfmm_b200_upload", "rtfmm_b200_evaluate_device",
-    "rtfmm_b200_download", "rtfmm_b200_adjoint", "rtfmm_b200_adjoint_device", "rtfmm_b200_stage_times",
+    "rtfmm_b200_download", "rtfmm_b200_forward_device", "rtfmm_b200_adjoint", "rtfmm_b200_adjoint_device",
+    "rtfmm_b200_stage_times",
     "rtfmm_b200_launch_count",
     "rtfmm_b200_flush_l2", "rtfmm_b200_info", "rtfmm_b200_get_cells", "rtfmm_b200_get_perm",
     "rtfmm_b200_get_p2p", "rtfmm_b200_get_m2l", "rtfmm_b200_get_cell_vectors", "rtfmm_b200_get_operator",
@@ -84,6 +85,7 @@ def lib():
         "rtfmm_b200_download": (ctypes.c_int, [_vp, _dp, _dp]),
         "rtfmm_b200_adjoint": (ctypes.c_int, [_vp, _dp, _dp, _dp]),
         "rtfmm_b200_adjoint_device": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_float)]),
+        "rtfmm_b200_forward_device": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_float)]),
         "rtfmm_b200_ewald_sampled": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, _dp, _dp, ctypes.c_double,
                                                     ctypes.c_int, ctypes.c_int64, _lp, _dp, _dp]),
         "rtfmm_b200_direct_sampled": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, _dp, _dp, ctypes.c_int64, _lp,
@@ -254,6 +256,15 @@ class LaplaceFMM:
         dx = np.empty((self.n, 3))
         _check(lib().rtfmm_b200_adjoint(self._h, _ptr(w), _ptr(dq), _ptr(dx)))
         return dq, dx
+
+    def forward_device(self, q_ptr, phi_ptr, grad_ptr):
+        """The pass on device memory: integer device addresses of q (n, or 0
+        to keep the charges on the device), phi (n) and grad (n, 3), input
+        order, float64.  Returns the pass time in ms."""
+        ms = ctypes.c_float(0)
+        _check(lib().rtfmm_b200_forward_device(self._h, _vp(q_ptr or None), _vp(phi_ptr or None),
+                                               _vp(grad_ptr or None), ctypes.byref(ms)))
+        return ms.value
 
     def adjoint_device(self, w_ptr, dq_ptr, dx_ptr):
         """Adjoint on device memory: integer device addresses (e.g. a torch

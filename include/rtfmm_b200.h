@@ -123,6 +123,18 @@ int rtfmm_b200_solve(rtfmm_fmm* fmm, int64_t n, const double* x, const double* q
 int rtfmm_b200_upload(rtfmm_fmm* fmm);
 int rtfmm_b200_evaluate_device(rtfmm_fmm* fmm, float* ms);
 
+/*
+ * The evaluation pass on device buffers: q_dev (n charges, input order; NULL
+ * keeps the bodies' current charges) replaces the charges of the bodies on
+ * the device, and phi_dev (n) / grad_dev (n*3), device pointers in input
+ * order (either may be NULL), receive the results.  Needs rtfmm_b200_upload
+ * (or an evaluate) first; charges are not checked for NaN/Inf.  *ms (may be
+ * NULL) receives the pass time; returns when the results are complete.
+ * Together with rtfmm_b200_adjoint_device this is a forward/backward step
+ * without host copies.
+ */
+int rtfmm_b200_forward_device(rtfmm_fmm* fmm, const double* q_dev, double* phi_dev, double* grad_dev, float* ms);
+
 /* Copies the outputs of the last device pass to the host (input order). */
 int rtfmm_b200_download(rtfmm_fmm* fmm, double* phi, double* grad);
 

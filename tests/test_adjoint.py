@@ -155,3 +155,45 @@ def test_device_adjoint_matches_host_adjoint(pkg, precision, dipole):
         dqn, dxn = dq.cpu().numpy(), dx.cpu().numpy()
         assert np.linalg.norm(dqn - dq_ref) <= 1e-12 * np.linalg.norm(dq_ref), call
         assert np.linalg.norm(dxn - dx_ref) <= 1e-12 * np.linalg.norm(dx_ref), call
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_forward_device_matches_host_solve(pkg, precision):
+    """rtfmm_b200_forward_device with new charges on the device equals a host
+    solve with those charges (same tree, same kernels)."""
+    import torch
+    x, q = uniform01(3000, 13)
+    q2 = np.random.default_rng(14).standard_normal(len(q))
+    q2 -= q2.mean()
+    a = args(pkg, 6, 32, 3, precision)
+    f = pkg.LaplaceFMM(x, q, a)
+    f.setup()
+    f.upload()
+    qd = torch.from_numpy(q2).cuda()
+    phi = torch.full((len(q),), float("nan"), dtype=torch.float64, device="cuda")
+    grad = torch.full((len(q), 3), float("nan"), dtype=torch.float64, device="cuda")
+    assert f.forward_device(qd.data_ptr(), phi.data_ptr(), grad.data_ptr()) > 0
+    ref = pkg.LaplaceFMM(x, q2, a)
+    rphi, rgrad = ref.solve()
+    assert np.allclose(phi.cpu().numpy(), rphi, rtol=0, atol=1e-13 * np.abs(rphi).max())
+    assert np.allclose(grad.cpu().numpy(), rgrad, rtol=0, atol=1e-13 * np.abs(rgrad).max())
+
+
+def test_autograd_harness_on_cuda_tensors(pkg):
+    """The autograd harness on CUDA tensors (device forward, device adjoint
+    reusing the forward gradient) gives the host path's gradients."""
+    import torch
+    from fmm_autograd import fmm_potential
+    x, q = uniform01(1500, 15)
+    a = args(pkg, 5, 32, 1, 0)
+    w = torch.tensor(np.random.default_rng(16).standard_normal(len(q)))
+    xt = torch.tensor(x, device="cuda", requires_grad=True)
+    qt = torch.tensor(q, device="cuda", requires_grad=True)
+    phi = fmm_potential(xt, qt, pkg, a)
+    (phi * w.cuda()).sum().backward()
+    f = pkg.LaplaceFMM(x, q, a)
+    rphi, _ = f.solve()
+    dq, dx = f.adjoint(w.numpy())
+    assert np.allclose(phi.detach().cpu().numpy(), rphi, rtol=0, atol=1e-12 * np.abs(rphi).max())
+    assert np.allclose(qt.grad.cpu().numpy(), dq, rtol=0, atol=1e-12 * np.abs(dq).max())
+    assert np.allclose(xt.grad.cpu().numpy(), dx, rtol=0, atol=1e-12 * np.abs(dx).max())
