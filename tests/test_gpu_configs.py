@@ -147,3 +147,18 @@ def test_c5_jittered_mixed_vs_fp64(pkg):
     # against the converged Ewald sum (measured 3.7e-7 FP64, 2.0e-6 mixed)
     assert ewald_grad_error(pkg, x, q, grad_d) < 2e-6
     assert ewald_grad_error(pkg, x, q, grad_m) < 1e-5
+
+
+@pytest.mark.parametrize("P,ncrit,images", [(7, 40, 2), (12, 64, 1), (6, 1000, 3), (3, 16, 2)])
+def test_other_orders_and_leaf_sizes(pkg, oracle, P, ncrit, images):
+    """Expansion orders without a compile-time specialisation of the M2L
+    transforms (3, 7, 12) and leaves far larger than a warp (ncrit=1000),
+    FP64 against the oracle."""
+    x, q = uniform01(2000, 20 + P)
+    f, phi, grad = solve(pkg, x, q, args(pkg, P, ncrit, images, 0))
+    f.close()
+    F = oracle.FMM(x, q, P, ncrit, images, 1.0, center=(0.5, 0.5, 0.5), dipole_correction=0, divide_4pi=1)
+    rphi, rgrad = F.solve()
+    tol = 1e-7 if P >= 10 else 1e-9
+    assert l2(grad, rgrad) < tol, l2(grad, rgrad)
+    assert l2(phi - phi.mean(), rphi - rphi.mean()) < 10 * tol
