@@ -2,12 +2,15 @@
 //
 // Stage map (reference function -> kernel here):
 //   p2p_1toN_256          (3dpp/src/kernel.cpp:258-311)   k_p2p32 / k_p2p64
-//   p2m_precompute        (kernel.cpp:332-371)            k_p2m_check + k_apply_f64
-//   m2m_precompute / img  (kernel.cpp:395-404, 434-442)   k_apply_f64 per level
+//   p2m_precompute        (kernel.cpp:332-371)            k_p2m_check + k_apply_f64_tc
+//   m2m_precompute / img  (kernel.cpp:395-404, 434-442)   k_apply_f64_tc per level
 //   m2l_fft_precompute_t  (kernel.cpp:1140-1397)          k_m2l_up, k_m2l_hadamard8,
 //     hadamard_8x8 / 1x27 (kernel.cpp:1012-1138)          k_m2l_hadamard27, k_m2l_down
-//   l2l_precompute / img  (kernel.cpp:1419-1435)          k_apply_f64 per level
-//   l2p_precompute        (kernel.cpp:1458-1511)          k_apply_f64 + k_l2p_eval
+//   l2l_precompute / img  (kernel.cpp:1419-1435)          k_apply_f64_tc per level
+//   l2p_precompute        (kernel.cpp:1458-1511)          k_apply_f64_tc + k_l2p_eval
+// (k_apply_f64 is the SIMT form of the operator GEMM, built with APPLY_TC=0.)
+// The adjoint adds k_swap_charges, k_restore_charges, k_adj_combine; the
+// device-buffer forward k_set_charges.
 //   dipole_correction, scale_bodies, sort_bodies_by_idx
 //                         (kernel.cpp:1580-1596, body.cpp:88-96,177-190)  k_dipole_*, k_post
 //
