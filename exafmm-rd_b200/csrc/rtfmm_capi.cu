@@ -6,6 +6,7 @@
 //   stream s1 (near field): P2P, concurrently with the far field
 //
 // This is LaplaceFMM::solve (3dpp/src/fmm.cpp:13-81) split at its hot block.
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <algorithm>
@@ -65,6 +66,12 @@ struct ApplyCall {
 //   adjoint image levels: the transposes swap roles, so the upward step uses
 //   M2M_img[13] (the transpose of the forward L2L_img) and the downward step
 //   the transposed 27-image sum
+#ifndef USE_PASS_GRAPH
+#define USE_PASS_GRAPH 0
+#endif
+#ifndef GRAPH_NODE_PRIO
+#define GRAPH_NODE_PRIO 1
+#endif
 #ifndef STREAM_PRIO
 #define STREAM_PRIO 1
 #endif
@@ -150,6 +157,13 @@ struct rtfmm_fmm {
   // d_body64 holds this set-up's positions (tree order); an evaluate then
   // only moves the charges
   bool pos_on_device = false;
+  // host set-up wall times of the last setup (s): tree, lists, operators
+  // (0 when cached), device tables, whole call
+  double setup_s[5] = {0, 0, 0, 0, 0};
+  // the pass captured as a CUDA graph (evaluate_device / forward_device with
+  // all stages overlapped), rebuilt when the tables are
+  cudaGraphExec_t pass_graph = nullptr;
+  cudaEvent_t ev_g0 = nullptr, ev_g1 = nullptr;
   // the 8x8 FFT-M2L (up, Hadamard, down) runs in FP32: the mixed form at P <= 8
   bool m2l32 = false;
   float stage_ms[ST_N] = {};
@@ -181,7 +195,15 @@ int dupload(rtfmm_fmm* f, T** p, const std::vector<T>& h) {
 
 // Frees every device buffer of the handle and forgets the pointers that
 // are allocated lazily (L2 flush, adjoint scratch), so that none dangles.
+void drop_graph(rtfmm_fmm* f) {
+  if (f->pass_graph) {
+    cudaGraphExecDestroy(f->pass_graph);
+    f->pass_graph = nullptr;
+  }
+}
+
 void drop_allocs(rtfmm_fmm* f) {
+  drop_graph(f);
   for (void* p : f->allocs) cudaFree(p);
   f->allocs.clear();
   f->d_flush = nullptr;
@@ -201,7 +223,8 @@ void free_device(rtfmm_fmm* f) {
   if (f->s0) cudaStreamDestroy(f->s0);
   if (f->s1) cudaStreamDestroy(f->s1);
   f->s0 = f->s1 = nullptr;
-  cudaEvent_t* evs[] = {&f->ev_start, &f->ev_near0, &f->ev_near, &f->ev_stop, &f->ev_adj0, &f->ev_adj1};
+  cudaEvent_t* evs[] = {&f->ev_start, &f->ev_near0, &f->ev_near, &f->ev_stop, &f->ev_adj0, &f->ev_adj1,
+                        &f->ev_g0, &f->ev_g1};
   for (auto e : evs)
     if (*e) {
       cudaEventDestroy(*e);
@@ -215,18 +238,24 @@ void free_device(rtfmm_fmm* f) {
   f->device_ready = false;
 }
 
+double wall_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 bool finite_all(const double* a, int64_t n) {
   for (int64_t i = 0; i < n; ++i)
     if (!std::isfinite(a[i])) return false;
   return true;
 }
 
+// Longest root-to-leaf path of the octree (its depth limit is 40).
+constexpr int kMaxPath = 48;
+
 // Host tables for the device pass, derived from the plan.
 void build_tables(rtfmm_fmm* f) {
   Plan& p = f->plan;
   const Operators& o = f->ops;
   const int ns = o.ns;
-  std::vector<int> leaf_of_cell(p.cells.size(), -1);
   f->leaves.clear();
   for (int c = 0; c < p.ntree; ++c) {
     const Cell& cl = p.cells[c];
@@ -240,10 +269,10 @@ void build_tables(rtfmm_fmm* f) {
     L.cell = c;
     L.boff = cl.boff;
     L.bnum = cl.bnum;
-    leaf_of_cell[c] = (int)f->leaves.size();
     f->leaves.push_back(L);
   }
   f->body_leaf.assign(p.n, 0);
+#pragma omp parallel for schedule(dynamic, 64)
   for (int l = 0; l < (int)f->leaves.size(); ++l)
     for (int b = 0; b < f->leaves[l].bnum; ++b) f->body_leaf[f->leaves[l].boff + b] = l;
 
@@ -253,37 +282,59 @@ void build_tables(rtfmm_fmm* f) {
   // (p2p_1toN_256, kernel.cpp:276-301).  Such a pair is expanded here into
   // the leaf pairs beneath it (same bodies, same sum), so that every list
   // entry is leaf to leaf and FP32 positions can stay leaf-relative.
-  std::vector<std::vector<int>> under(p.ntree);
-  std::function<const std::vector<int>&(int)> leaves_under = [&](int c) -> const std::vector<int>& {
-    std::vector<int>& v = under[c];
-    if (!v.empty()) return v;
-    const Cell& cl = p.cells[c];
-    if (cl.cnum == 0) {
-      v.push_back(c);
-    } else {
-      for (int k = 0; k < cl.cnum; ++k) {
-        const std::vector<int>& w = leaves_under(cl.coff + k);
-        v.insert(v.end(), w.begin(), w.end());
-      }
-    }
-    return v;
-  };
-  std::vector<std::vector<P2PEntry>> leaf_lists(f->leaves.size());
-  for (const auto& kv : p.p2p) {
-    const std::vector<int> tl = leaves_under(kv.first);
-    for (const P2PEntry& e : kv.second) {
-      const std::vector<int>& sl = leaves_under(e.src);
-      for (int t : tl)
-        for (int sc : sl) leaf_lists[leaf_of_cell[t]].push_back({sc, e.off});
-    }
-  }
-  // CSR offsets and item offsets first, then every leaf's entries in parallel
+  //
+  // A target leaf's list is: for every cell on its root-to-leaf path that
+  // has a P2P list (ascending cell index, the order the lists are keyed by),
+  // each entry in list order, expanded into the source's leaves in
+  // depth-first order.  The leaves under a cell are the ones whose bodies
+  // lie in the cell's body range: a contiguous run of the leaves sorted by
+  // their first body.  Each leaf's list is counted, then filled, in
+  // parallel.
   const int nlf = (int)f->leaves.size();
+  std::vector<int> parent(p.ntree, -1);
+  for (int c = 0; c < p.ntree; ++c)
+    for (int k = 0; k < p.cells[c].cnum; ++k)
+      if (p.cells[c].coff + k < p.ntree) parent[p.cells[c].coff + k] = c;
+  std::vector<int> dfs(nlf), dfs_pos(nlf);
+  for (int l = 0; l < nlf; ++l) dfs[l] = l;
+  std::sort(dfs.begin(), dfs.end(), [&](int a, int b) { return f->leaves[a].boff < f->leaves[b].boff; });
+  for (int i = 0; i < nlf; ++i) dfs_pos[dfs[i]] = i;
+  auto leaf_run = [&](int c, int* lo, int* hi) {
+    const Cell& cl = p.cells[c];
+    if (cl.bnum == 0) {  // an empty root leaf (no bodies): itself
+      *lo = 0;
+      *hi = nlf;
+      return;
+    }
+    *lo = dfs_pos[f->body_leaf[cl.boff]];
+    *hi = dfs_pos[f->body_leaf[cl.boff + cl.bnum - 1]] + 1;
+  };
+  auto path_lists = [&](int c, int* path) {  // cells root..c with a P2P list
+    int k = 0;
+    for (int a = c; a >= 0; a = parent[a])
+      if (!p.p2p.at(a).empty()) path[k++] = a;
+    std::reverse(path, path + k);
+    return k;
+  };
   f->list_off.assign(nlf + 1, 0);
   std::vector<int> item_off(nlf + 1, 0);
+#pragma omp parallel for schedule(dynamic, 64)
   for (int l = 0; l < nlf; ++l) {
-    f->list_off[l + 1] = f->list_off[l] + (int)leaf_lists[l].size();
-    item_off[l + 1] = item_off[l] + (f->leaves[l].bnum + 31) / 32;
+    int path[kMaxPath];
+    const int np = path_lists(f->leaves[l].cell, path);
+    int64_t cnt = 0;
+    for (int i = 0; i < np; ++i)
+      for (const P2PEntry& e : p.p2p.at(path[i])) {
+        int lo, hi;
+        leaf_run(e.src, &lo, &hi);
+        cnt += hi - lo;
+      }
+    f->list_off[l + 1] = (int)cnt;
+    item_off[l + 1] = (f->leaves[l].bnum + 31) / 32;
+  }
+  for (int l = 0; l < nlf; ++l) {
+    f->list_off[l + 1] += f->list_off[l];
+    item_off[l + 1] += item_off[l];
   }
   f->list32.assign(f->list_off[nlf], P2PSrc32{});
   f->list64.assign(f->list_off[nlf], P2PSrc64{});
@@ -291,32 +342,39 @@ void build_tables(rtfmm_fmm* f) {
 #pragma omp parallel for schedule(dynamic, 64)
   for (int l = 0; l < nlf; ++l) {
     const int c = f->leaves[l].cell;
+    const Cell& T = p.cells[c];
+    int path[kMaxPath];
+    const int np = path_lists(c, path);
     int k = f->list_off[l];
-    for (const P2PEntry& e : leaf_lists[l]) {
-      const int sl = leaf_of_cell[e.src];
-      const Cell& S = p.cells[e.src];
-      const Cell& T = p.cells[c];
-      P2PSrc32 a;
-      a.dx = (float)(S.x[0] + e.off[0] - T.x[0]);
-      a.dy = (float)(S.x[1] + e.off[1] - T.x[1]);
-      a.dz = (float)(S.x[2] + e.off[2] - T.x[2]);
-      a.leaf = sl;
-      a.self = (e.src == c && e.off[0] == 0 && e.off[1] == 0 && e.off[2] == 0) ? 1 : 0;
-      a.boff = f->leaves[sl].boff;
-      a.bnum = f->leaves[sl].bnum;
-      a.pad = 0;
-      f->list32[k] = a;
-      P2PSrc64 b;
-      b.ox = e.off[0];
-      b.oy = e.off[1];
-      b.oz = e.off[2];
-      b.leaf = sl;
-      b.self = a.self;
-      b.boff = a.boff;
-      b.bnum = a.bnum;
-      f->list64[k] = b;
-      ++k;
-    }
+    for (int i = 0; i < np; ++i)
+      for (const P2PEntry& e : p.p2p.at(path[i])) {
+        int lo, hi;
+        leaf_run(e.src, &lo, &hi);
+        for (int r = lo; r < hi; ++r) {
+          const int sl = dfs[r];
+          const Cell& S = p.cells[f->leaves[sl].cell];
+          P2PSrc32 a;
+          a.dx = (float)(S.x[0] + e.off[0] - T.x[0]);
+          a.dy = (float)(S.x[1] + e.off[1] - T.x[1]);
+          a.dz = (float)(S.x[2] + e.off[2] - T.x[2]);
+          a.leaf = sl;
+          a.self = (f->leaves[sl].cell == c && e.off[0] == 0 && e.off[1] == 0 && e.off[2] == 0) ? 1 : 0;
+          a.boff = f->leaves[sl].boff;
+          a.bnum = f->leaves[sl].bnum;
+          a.pad = 0;
+          f->list32[k] = a;
+          P2PSrc64 b;
+          b.ox = e.off[0];
+          b.oy = e.off[1];
+          b.oz = e.off[2];
+          b.leaf = sl;
+          b.self = a.self;
+          b.boff = a.boff;
+          b.bnum = a.bnum;
+          f->list64[k] = b;
+          ++k;
+        }
+      }
     // FP32 items: 32 targets each; the last <= 16 targets of a leaf take a
     // narrower group (W = 16, 8 or 4 lanes) and split the sources 32/W ways
     int j = item_off[l];
@@ -520,6 +578,8 @@ int ensure_device(rtfmm_fmm* f) {
     CK(cudaEventCreate(&f->ev_stop));
     CK(cudaEventCreate(&f->ev_adj0));
     CK(cudaEventCreate(&f->ev_adj1));
+    CK(cudaEventCreate(&f->ev_g0));
+    CK(cudaEventCreate(&f->ev_g1));
     for (int k = 0; k < ST_N; ++k) CK(cudaEventCreate(&f->ev_st[k]));
   } else {
     CK(cudaSetDevice(f->dev));
@@ -866,6 +926,40 @@ int collect_times(rtfmm_fmm* f, float* total) {
   return RTFMM_OK;
 }
 
+// The forward pass as a CUDA graph: captured once per set of device tables
+// (the launches, their arguments and the two-stream fork/join are fixed by
+// the plan), then replayed with one launch.  Stage times are not recorded in
+// this mode (the timing events inside the capture become plain dependencies);
+// *ms is the replay's time.
+int run_pass_graph(rtfmm_fmm* f, float* ms) {
+  if (!f->pass_graph) {
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(f->s0, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_pass(f);
+    cudaError_t e = cudaStreamEndCapture(f->s0, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) return fail(RTFMM_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    // kernel nodes keep the priority of the stream they were captured from
+    e = cudaGraphInstantiateWithFlags(&f->pass_graph, g, GRAPH_NODE_PRIO ? cudaGraphInstantiateFlagUseNodePriority : 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      f->pass_graph = nullptr;
+      return fail(RTFMM_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    }
+  }
+  CK(cudaEventRecord(f->ev_g0, f->s0));
+  CK(cudaGraphLaunch(f->pass_graph, f->s0));
+  CK(cudaEventRecord(f->ev_g1, f->s0));
+  CK(cudaEventSynchronize(f->ev_g1));
+  float t = 0;
+  CK(cudaEventElapsedTime(&t, f->ev_g0, f->ev_g1));
+  if (ms) *ms = t;
+  return RTFMM_OK;
+}
+
 }  // namespace
 
 namespace rtfmm_b200 {
@@ -930,6 +1024,7 @@ int rtfmm_b200_setup(rtfmm_fmm* f, int64_t n, const double* x, const double* q) 
   if (!f) return fail(RTFMM_EINVAL, "null handle");
   if (n < 0 || n > (int64_t)1 << 30) return fail(RTFMM_EINVAL, "n out of range");
   if (n > 0 && (!x || !q)) return fail(RTFMM_EINVAL, "null body arrays");
+  const double t0 = wall_s();
   if (!finite_all(x, 3 * n) || !finite_all(q, n)) return fail(RTFMM_EINVAL, "non-finite body position or charge");
   try {
     f->setup_done = false;
@@ -939,15 +1034,26 @@ int rtfmm_b200_setup(rtfmm_fmm* f, int64_t n, const double* x, const double* q) 
     f->plan.n = n;
     f->x_in.assign(x, x + 3 * n);
     f->q_in.assign(q, q + n);
+    double* st = f->setup_s;
+    for (int k = 0; k < 5; ++k) st[k] = 0;
+    double t = wall_s();
     std::string err = build_tree(f->plan, x, q);
     if (!err.empty()) return fail(RTFMM_EINVAL, err);
+    st[0] = wall_s() - t;
+    t = wall_s();
     traverse(f->plan);
+    st[1] = wall_s() - t;
     if (!f->ops_valid || f->ops.P != f->args.P || f->ops.images != f->args.images ||
         f->ops.r0 != f->plan.r0) {
+      t = wall_s();
       build_operators(f->ops, f->args.P, f->plan.r0, f->args.images);
       f->ops_valid = true;
+      st[2] = wall_s() - t;
     }
+    t = wall_s();
     build_tables(f);
+    st[3] = wall_s() - t;
+    st[4] = wall_s() - t0;
   } catch (const std::bad_alloc&) {
     return fail(RTFMM_ENOMEM, "host allocation failed during set-up");
   } catch (const std::exception& e) {
@@ -987,11 +1093,16 @@ int rtfmm_b200_evaluate_device(rtfmm_fmm* f, float* ms) {
     if (ms) *ms = 0;
     return RTFMM_OK;
   }
-  int rc = enqueue_pass(f);
-  if (rc) return rc;
   float t = 0;
-  rc = collect_times(f, &t);
-  if (rc) return rc;
+  if (USE_PASS_GRAPH && !(f->args.stages & RTFMM_STAGE_SERIAL)) {
+    int rc = run_pass_graph(f, &t);
+    if (rc) return rc;
+  } else {
+    int rc = enqueue_pass(f);
+    if (rc) return rc;
+    rc = collect_times(f, &t);
+    if (rc) return rc;
+  }
   CK(cudaGetLastError());
   if (ms) *ms = t;
   f->pass_done = true;
@@ -1194,6 +1305,13 @@ int rtfmm_b200_flush_l2(rtfmm_fmm* f) {
   }
   CK(cudaMemsetAsync(f->d_flush, f->launches & 0xff, f->flush_bytes, f->s0));
   CK(cudaStreamSynchronize(f->s0));
+  return RTFMM_OK;
+}
+
+int rtfmm_b200_setup_times(rtfmm_fmm* f, double* s, int cap) {
+  if (!f || !s) return fail(RTFMM_EINVAL, "null argument");
+  if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");
+  for (int k = 0; k < 5 && k < cap; ++k) s[k] = f->setup_s[k];
   return RTFMM_OK;
 }
 

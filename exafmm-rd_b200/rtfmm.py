@@ -36,7 +36,7 @@ EXPORTS = (
     "rtfmm_b200_download", "rtfmm_b200_forward_device", "rtfmm_b200_adjoint", "rtfmm_b200_adjoint_device",
     "rtfmm_b200_stage_times",
     "rtfmm_b200_launch_count",
-    "rtfmm_b200_flush_l2", "rtfmm_b200_info", "rtfmm_b200_get_cells", "rtfmm_b200_get_perm",
+    "rtfmm_b200_flush_l2", "rtfmm_b200_setup_times", "rtfmm_b200_info", "rtfmm_b200_get_cells", "rtfmm_b200_get_perm",
     "rtfmm_b200_get_p2p", "rtfmm_b200_get_m2l", "rtfmm_b200_get_cell_vectors", "rtfmm_b200_get_operator",
     "rtfmm_b200_last_error", "rtfmm_b200_version", "rtfmm_b200_p2m_noalloc",
     "rtfmm_b200_ewald_sampled", "rtfmm_b200_direct_sampled",
@@ -94,6 +94,7 @@ def lib():
         "rtfmm_b200_launch_count": (ctypes.c_int, [_vp, _lp]),
         "rtfmm_b200_flush_l2": (ctypes.c_int, [_vp]),
         "rtfmm_b200_info": (ctypes.c_int, [_vp, _lp, ctypes.c_int]),
+        "rtfmm_b200_setup_times": (ctypes.c_int, [_vp, _dp, ctypes.c_int]),
         "rtfmm_b200_get_cells": (ctypes.c_int, [_vp, _ip, _dp]),
         "rtfmm_b200_get_perm": (ctypes.c_int, [_vp, _lp]),
         "rtfmm_b200_get_p2p": (ctypes.c_int, [_vp, _ip, _dp]),
@@ -276,6 +277,13 @@ class LaplaceFMM:
         return ms.value
 
     # -- introspection ------------------------------------------------------------
+    def setup_times(self):
+        """Wall seconds of the last setup's phases: tree, lists, operators
+        (0 when cached), device tables, total."""
+        v = np.zeros(5)
+        _check(lib().rtfmm_b200_setup_times(self._h, _ptr(v), 5))
+        return dict(zip(("tree", "lists", "operators", "tables", "total"), v.tolist()))
+
     def info(self):
         v = np.zeros(12, dtype=np.int64)
         lib().rtfmm_b200_info(self._h, _ptr(v, _lp), 12)

@@ -200,6 +200,13 @@ int rtfmm_b200_flush_l2(rtfmm_fmm* fmm);
 
 /* ---- introspection (host data after setup; used by parity tests) ---- */
 
+/* Host set-up wall times of the last rtfmm_b200_setup, in seconds:
+ * s[0] octree, s[1] interaction lists, s[2] operator tables (0 when the
+ * handle's cached tables were reused), s[3] device tables, s[4] the whole
+ * call.  The reference times the same phases separately from the
+ * evaluation (3dpp/src/fmm.cpp:13-50).  Writes min(cap, 5) values. */
+int rtfmm_b200_setup_times(rtfmm_fmm* fmm, double* s, int cap);
+
 /* Tree and list sizes.  info[0..11] = ncell (incl. image cells), nleaf,
  * depth_min, depth_max, n_p2p_entries, n_m2l_parents, n_m2l_entries,
  * num_surf, P2P body pairs (sum over list entries of n_target * n_source),
