@@ -11,9 +11,9 @@ directory name is not a Python identifier, so load it by path:
         submodule_search_locations=[os.path.join(root, "exafmm-rd_b200")])
     pkg = importlib.util.module_from_spec(spec); spec.loader.exec_module(pkg)
 """
-from .rtfmm import (FP32_MIXED, FP64, STAGE_ALL, STAGE_FAR, STAGE_NAMES, STAGE_NEAR, STAGE_SERIAL, Argument, LaplaceFMM,
-                    RtfmmError, compare, direct_sampled, ewald_sampled, generate_random_bodies, lib)
+from .rtfmm import (FP32_MIXED, FP64, STAGE_ALL, STAGE_FAR, STAGE_NAMES, STAGE_NEAR, STAGE_SERIAL, STAGE_TIMED,
+                    Argument, LaplaceFMM, RtfmmError, compare, direct_sampled, ewald_sampled, generate_random_bodies, lib)
 
 __all__ = ["Argument", "LaplaceFMM", "RtfmmError", "compare", "direct_sampled", "ewald_sampled",
            "generate_random_bodies", "lib", "FP64",
-           "FP32_MIXED", "STAGE_ALL", "STAGE_FAR", "STAGE_NEAR", "STAGE_NAMES", "STAGE_SERIAL"]
+           "FP32_MIXED", "STAGE_ALL", "STAGE_FAR", "STAGE_NEAR", "STAGE_NAMES", "STAGE_SERIAL", "STAGE_TIMED"]

@@ -67,10 +67,7 @@ struct ApplyCall {
 //   M2M_img[13] (the transpose of the forward L2L_img) and the downward step
 //   the transposed 27-image sum
 #ifndef USE_PASS_GRAPH
-#define USE_PASS_GRAPH 0
-#endif
-#ifndef GRAPH_NODE_PRIO
-#define GRAPH_NODE_PRIO 1
+#define USE_PASS_GRAPH 1
 #endif
 #ifndef STREAM_PRIO
 #define STREAM_PRIO 1
@@ -160,9 +157,10 @@ struct rtfmm_fmm {
   // host set-up wall times of the last setup (s): tree, lists, operators
   // (0 when cached), device tables, whole call
   double setup_s[5] = {0, 0, 0, 0, 0};
-  // the pass captured as a CUDA graph (evaluate_device / forward_device with
-  // all stages overlapped), rebuilt when the tables are
+  // the forward pass captured as a CUDA graph (launch_pass), dropped with
+  // the device tables
   cudaGraphExec_t pass_graph = nullptr;
+  bool graph_grad_q_valid = false;
   cudaEvent_t ev_g0 = nullptr, ev_g1 = nullptr;
   // the 8x8 FFT-M2L (up, Hadamard, down) runs in FP32: the mixed form at P <= 8
   bool m2l32 = false;
@@ -926,12 +924,21 @@ int collect_times(rtfmm_fmm* f, float* total) {
   return RTFMM_OK;
 }
 
-// The forward pass as a CUDA graph: captured once per set of device tables
-// (the launches, their arguments and the two-stream fork/join are fixed by
-// the plan), then replayed with one launch.  Stage times are not recorded in
-// this mode (the timing events inside the capture become plain dependencies);
-// *ms is the replay's time.
-int run_pass_graph(rtfmm_fmm* f, float* ms) {
+// The forward pass as a CUDA graph: captured on first use per set of device
+// tables (the launches, their arguments and the two-stream fork/join are
+// fixed by the plan; charges, positions and outputs live in the handle's
+// buffers), then replayed with one launch.  Kernel nodes keep the priority
+// of the stream they were captured from, so the far-field chain still
+// preempts P2P.  Per-stage events are not recorded in a replay: the stage
+// timing and serial diagnostics (RTFMM_STAGE_TIMED, RTFMM_STAGE_SERIAL)
+// issue the launches directly.
+bool use_graph(const rtfmm_fmm* f) {
+  return USE_PASS_GRAPH && !(f->args.stages & (RTFMM_STAGE_SERIAL | RTFMM_STAGE_TIMED));
+}
+
+// Enqueues one forward pass on s0 (graph replay or direct launches).
+int launch_pass(rtfmm_fmm* f) {
+  if (!use_graph(f)) return enqueue_pass(f);
   if (!f->pass_graph) {
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(f->s0, cudaStreamCaptureModeThreadLocal));
@@ -942,21 +949,29 @@ int run_pass_graph(rtfmm_fmm* f, float* ms) {
       return rc;
     }
     if (e != cudaSuccess) return fail(RTFMM_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-    // kernel nodes keep the priority of the stream they were captured from
-    e = cudaGraphInstantiateWithFlags(&f->pass_graph, g, GRAPH_NODE_PRIO ? cudaGraphInstantiateFlagUseNodePriority : 0);
+    e = cudaGraphInstantiateWithFlags(&f->pass_graph, g, cudaGraphInstantiateFlagUseNodePriority);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) {
       f->pass_graph = nullptr;
       return fail(RTFMM_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
     }
+    f->graph_grad_q_valid = f->grad_q_valid;
   }
   CK(cudaEventRecord(f->ev_g0, f->s0));
   CK(cudaGraphLaunch(f->pass_graph, f->s0));
   CK(cudaEventRecord(f->ev_g1, f->s0));
+  f->grad_q_valid = f->graph_grad_q_valid;
+  return RTFMM_OK;
+}
+
+// Waits for the pass launched by launch_pass; *total = its device time.
+int pass_times(rtfmm_fmm* f, float* total) {
+  if (!use_graph(f)) return collect_times(f, total);
   CK(cudaEventSynchronize(f->ev_g1));
-  float t = 0;
-  CK(cudaEventElapsedTime(&t, f->ev_g0, f->ev_g1));
-  if (ms) *ms = t;
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, f->ev_g0, f->ev_g1));
+  if (total) *total = ms;
+  for (int k = 0; k < ST_N; ++k) f->stage_ms[k] = 0;
   return RTFMM_OK;
 }
 
@@ -994,7 +1009,8 @@ int rtfmm_b200_create(const rtfmm_args* a, rtfmm_fmm** out) {
   if (!(a->cycle > 0) || !std::isfinite(a->cycle)) return fail(RTFMM_EINVAL, "cycle must be positive and finite");
   if (a->precision != RTFMM_FP64 && a->precision != RTFMM_FP32_MIXED)
     return fail(RTFMM_EINVAL, "unknown precision");
-  if (a->stages & ~(RTFMM_STAGE_ALL | RTFMM_STAGE_SERIAL)) return fail(RTFMM_EINVAL, "unknown stage bits");
+  if (a->stages & ~(RTFMM_STAGE_ALL | RTFMM_STAGE_SERIAL | RTFMM_STAGE_TIMED))
+    return fail(RTFMM_EINVAL, "unknown stage bits");
   for (int k = 0; k < 3; ++k)
     if (!std::isfinite(a->x[k])) return fail(RTFMM_EINVAL, "centre must be finite");
   rtfmm_fmm* f = new (std::nothrow) rtfmm_fmm();
@@ -1093,16 +1109,11 @@ int rtfmm_b200_evaluate_device(rtfmm_fmm* f, float* ms) {
     if (ms) *ms = 0;
     return RTFMM_OK;
   }
+  int rc = launch_pass(f);
+  if (rc) return rc;
   float t = 0;
-  if (USE_PASS_GRAPH && !(f->args.stages & RTFMM_STAGE_SERIAL)) {
-    int rc = run_pass_graph(f, &t);
-    if (rc) return rc;
-  } else {
-    int rc = enqueue_pass(f);
-    if (rc) return rc;
-    rc = collect_times(f, &t);
-    if (rc) return rc;
-  }
+  rc = pass_times(f, &t);
+  if (rc) return rc;
   CK(cudaGetLastError());
   if (ms) *ms = t;
   f->pass_done = true;
@@ -1118,13 +1129,13 @@ int rtfmm_b200_forward_device(rtfmm_fmm* f, const double* q_dev, double* phi_dev
   if (n == 0) return RTFMM_OK;
   CK(cudaSetDevice(f->dev));
   if (q_dev) CK(launch_set_charges(f->d_body64, q_dev, f->d_perm, (int)n, f->s0));
-  int rc = enqueue_pass(f);
+  int rc = launch_pass(f);
   if (rc) return rc;
   if (phi_dev) CK(cudaMemcpyAsync(phi_dev, f->d_out_phi, sizeof(double) * n, cudaMemcpyDeviceToDevice, f->s0));
   if (grad_dev)
     CK(cudaMemcpyAsync(grad_dev, f->d_out_grad, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, f->s0));
   float t = 0;
-  rc = collect_times(f, &t);
+  rc = pass_times(f, &t);
   if (rc) return rc;
   CK(cudaStreamSynchronize(f->s0));
   CK(cudaGetLastError());
@@ -1165,14 +1176,14 @@ int rtfmm_b200_evaluate(rtfmm_fmm* f, const double* q, double* phi, double* grad
     CK(launch_gather_bodies(f->d_xin, f->d_qin, f->d_perm, (int)n, f->d_body64, f->s0));
     f->pos_on_device = true;
   }
-  int rc = enqueue_pass(f);
+  int rc = launch_pass(f);
   if (rc) return rc;
   f->launches++;
   if (phi) CK(cudaMemcpyAsync(phi, f->d_out_phi, sizeof(double) * n, cudaMemcpyDeviceToHost, f->s0));
   if (grad) CK(cudaMemcpyAsync(grad, f->d_out_grad, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, f->s0));
   CK(cudaStreamSynchronize(f->s0));
   CK(cudaGetLastError());
-  rc = collect_times(f, nullptr);
+  rc = pass_times(f, nullptr);
   if (rc) return rc;
   f->pass_done = true;
   return RTFMM_OK;

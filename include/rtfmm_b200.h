@@ -52,6 +52,11 @@ typedef enum rtfmm_precision {
 /* Diagnostic bit: run P2P after the far field on one stream (no overlap), so
  * that per-stage times are those of each stage alone. */
 #define RTFMM_STAGE_SERIAL 4u
+/* Diagnostic bit: record per-stage events (rtfmm_b200_stage_times).  Without
+ * it, and without RTFMM_STAGE_SERIAL, a forward pass is captured as a CUDA
+ * graph on first use and replayed by every later call on the same device
+ * tables; rtfmm_b200_stage_times then reports zeros. */
+#define RTFMM_STAGE_TIMED 8u
 
 /*
  * Run parameters.  Replaces rtfmm::Argument (3dpp/include/argument.h:11-45,
