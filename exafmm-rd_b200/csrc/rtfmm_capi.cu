@@ -14,11 +14,13 @@
 #include <functional>
 #include <new>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/rtfmm_b200.h"
 #include "rtfmm_kernels.cuh"
 #include "rtfmm_plan.h"
+#include "rtfmm_tree.h"
 
 #ifndef M_PI
 #define M_PI 3.14159265358979323846
@@ -116,7 +118,17 @@ struct rtfmm_fmm {
   cudaStream_t s0 = nullptr, s1 = nullptr;
   cudaEvent_t ev_start = nullptr, ev_near0 = nullptr, ev_near = nullptr, ev_stop = nullptr;
   cudaEvent_t ev_st[ST_N] = {};
-  std::vector<void*> allocs;
+  // device buffers by the handle field that holds them, kept across set-ups
+  // and grown (with a quarter of headroom) only when a plan needs more, so a
+  // new body set of similar size reuses them without cudaMalloc/cudaFree
+  struct DevSlot {
+    void* p = nullptr;
+    size_t bytes = 0;
+  };
+  std::unordered_map<const void*, DevSlot> pool;
+  // operator tables: generation built on the host / uploaded to the device
+  uint64_t ops_gen = 0, ops_dev_gen = 0;
+  size_t h_xin_cap = 0;  // doubles in h_xin
   double4* d_body64 = nullptr;
   float4* d_body32 = nullptr;
   int* d_body_leaf = nullptr;
@@ -154,9 +166,10 @@ struct rtfmm_fmm {
   // d_body64 holds this set-up's positions (tree order); an evaluate then
   // only moves the charges
   bool pos_on_device = false;
-  // host set-up wall times of the last setup (s): tree, lists, operators
-  // (0 when cached), device tables, whole call
-  double setup_s[5] = {0, 0, 0, 0, 0};
+  // set-up wall times (s): tree, lists, operators (0 when cached), host
+  // tables, the setup call, and the upload of the device tables (in the call
+  // that did it)
+  double setup_s[6] = {0, 0, 0, 0, 0, 0};
   // the forward pass captured as a CUDA graph (launch_pass), dropped with
   // the device tables
   cudaGraphExec_t pass_graph = nullptr;
@@ -170,29 +183,43 @@ struct rtfmm_fmm {
 
 namespace {
 
+// *p = the pooled buffer of slot `key` (default: the field p itself) with
+// room for count elements, reallocated only when the slot is too small
+// (cudaFree waits for the device, so no pending work still reads it).
 template <typename T>
-int dalloc(rtfmm_fmm* f, T** p, size_t count) {
+int dalloc(rtfmm_fmm* f, T** p, size_t count, const void* key = nullptr) {
   *p = nullptr;
-  if (count == 0) count = 1;
-  void* q = nullptr;
-  cudaError_t e = cudaMalloc(&q, sizeof(T) * count);
-  if (e != cudaSuccess)
-    return fail(RTFMM_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-  f->allocs.push_back(q);
-  *p = reinterpret_cast<T*>(q);
+  const size_t need = sizeof(T) * std::max<size_t>(count, 1);
+  rtfmm_fmm::DevSlot& slot = f->pool[key ? key : (const void*)p];
+  if (slot.bytes < need) {
+    if (slot.p) CK(cudaFree(slot.p));
+    slot.p = nullptr;
+    slot.bytes = 0;
+    size_t cap = need + need / 4;
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, cap);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      cap = need;
+      e = cudaMalloc(&q, cap);
+    }
+    if (e != cudaSuccess)
+      return fail(RTFMM_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    slot.p = q;
+    slot.bytes = cap;
+  }
+  *p = reinterpret_cast<T*>(slot.p);
   return RTFMM_OK;
 }
 
 template <typename T>
-int dupload(rtfmm_fmm* f, T** p, const std::vector<T>& h) {
-  int rc = dalloc(f, p, h.size());
+int dupload(rtfmm_fmm* f, T** p, const std::vector<T>& h, const void* key = nullptr) {
+  int rc = dalloc(f, p, h.size(), key);
   if (rc) return rc;
   if (!h.empty()) CK(cudaMemcpy(*p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
   return RTFMM_OK;
 }
 
-// Frees every device buffer of the handle and forgets the pointers that
-// are allocated lazily (L2 flush, adjoint scratch), so that none dangles.
 void drop_graph(rtfmm_fmm* f) {
   if (f->pass_graph) {
     cudaGraphExecDestroy(f->pass_graph);
@@ -200,12 +227,11 @@ void drop_graph(rtfmm_fmm* f) {
   }
 }
 
+// Forgets the device state of the current plan: the captured pass graph and
+// the lazily sized adjoint scratch (fetched from the pool again at its next
+// use).  The buffers themselves stay in the pool.
 void drop_allocs(rtfmm_fmm* f) {
   drop_graph(f);
-  for (void* p : f->allocs) cudaFree(p);
-  f->allocs.clear();
-  f->d_flush = nullptr;
-  f->flush_bytes = 0;
   f->d_adj_q = f->d_adj_gq = f->d_adj_gw = f->d_adj_w = f->d_adj_dq = f->d_adj_dx = nullptr;
   f->grad_q_valid = false;
   f->pos_on_device = false;
@@ -217,7 +243,14 @@ void free_device(rtfmm_fmm* f) {
     cudaFreeHost(f->h_xin);
     f->h_xin = nullptr;
   }
+  f->h_xin_cap = 0;
   drop_allocs(f);
+  for (auto& kv : f->pool)
+    if (kv.second.p) cudaFree(kv.second.p);
+  f->pool.clear();
+  f->ops_dev_gen = 0;
+  f->d_flush = nullptr;
+  f->flush_bytes = 0;
   if (f->s0) cudaStreamDestroy(f->s0);
   if (f->s1) cudaStreamDestroy(f->s1);
   f->s0 = f->s1 = nullptr;
@@ -334,8 +367,10 @@ void build_tables(rtfmm_fmm* f) {
     f->list_off[l + 1] += f->list_off[l];
     item_off[l + 1] += item_off[l];
   }
-  f->list32.assign(f->list_off[nlf], P2PSrc32{});
-  f->list64.assign(f->list_off[nlf], P2PSrc64{});
+  // the list form of the handle's precision only
+  const bool mixed = f->args.precision == RTFMM_FP32_MIXED;
+  f->list32.assign(mixed ? f->list_off[nlf] : 0, P2PSrc32{});
+  f->list64.assign(mixed ? 0 : f->list_off[nlf], P2PSrc64{});
   f->items2.assign(item_off[nlf], P2PItem32{});
 #pragma omp parallel for schedule(dynamic, 64)
   for (int l = 0; l < nlf; ++l) {
@@ -360,16 +395,19 @@ void build_tables(rtfmm_fmm* f) {
           a.boff = f->leaves[sl].boff;
           a.bnum = f->leaves[sl].bnum;
           a.pad = 0;
-          f->list32[k] = a;
-          P2PSrc64 b;
-          b.ox = e.off[0];
-          b.oy = e.off[1];
-          b.oz = e.off[2];
-          b.leaf = sl;
-          b.self = a.self;
-          b.boff = a.boff;
-          b.bnum = a.bnum;
-          f->list64[k] = b;
+          if (mixed) {
+            f->list32[k] = a;
+          } else {
+            P2PSrc64 b;
+            b.ox = e.off[0];
+            b.oy = e.off[1];
+            b.oz = e.off[2];
+            b.leaf = sl;
+            b.self = a.self;
+            b.boff = a.boff;
+            b.bnum = a.bnum;
+            f->list64[k] = b;
+          }
           ++k;
         }
       }
@@ -585,46 +623,16 @@ int ensure_device(rtfmm_fmm* f) {
   return RTFMM_OK;
 }
 
-// Upload the plan (everything but the per-pass body values) to the device.
-int upload_plan(rtfmm_fmm* f) {
-  int rc = ensure_device(f);
-  if (rc) return rc;
-  // drop buffers of a previous plan, keep streams/events
-  CK(cudaDeviceSynchronize());
-  drop_allocs(f);
-  Plan& p = f->plan;
+// The operator tables of f->ops on the device (surfaces, DFT twiddles, the
+// FP64 operator stacks, the M2L kernel spectra): once per set of operators.
+int upload_operators(rtfmm_fmm* f) {
   const Operators& o = f->ops;
-  const int64_t n = p.n;
   const int ns = o.ns, Nf = o.Nf;
-  const size_t ncell = p.cells.size(), nleaf = f->leaves.size();
-  const bool mixed = f->args.precision == RTFMM_FP32_MIXED;
 #define RC(x)          \
   do {                 \
     int r_ = (x);      \
     if (r_) return r_; \
   } while (0)
-  RC(dalloc(f, &f->d_body64, n));
-  RC(dalloc(f, &f->d_body32, n));
-  RC(dupload(f, &f->d_body_leaf, f->body_leaf));
-  RC(dupload(f, &f->d_perm, p.perm));
-  RC(dalloc(f, &f->d_xin, 3 * n));
-  RC(dalloc(f, &f->d_qin, n));
-  RC(dupload(f, &f->d_leaves, f->leaves));
-  RC(dalloc(f, &f->d_qeq, ncell * ns));
-  RC(dalloc(f, &f->d_pchk, ncell * ns));
-  RC(dalloc(f, &f->d_leafvec, nleaf * ns));
-  RC(dalloc(f, &f->d_leafvec2, nleaf * ns));
-  RC(dalloc(f, &f->d_y, ncell * ns));
-  RC(dalloc(f, &f->d_far_phi, n));
-  RC(dalloc(f, &f->d_far_grad, 3 * n));
-  RC(dalloc(f, &f->d_near_phi, n));
-  RC(dalloc(f, &f->d_near_grad, 3 * n));
-  RC(dalloc(f, &f->d_out_phi, n));
-  RC(dalloc(f, &f->d_out_grad, 3 * n));
-  RC(dupload(f, &f->d_items2, f->items2));
-  RC(dupload(f, &f->d_list_off, f->list_off));
-  RC(dupload(f, &f->d_list32, f->list32));
-  RC(dupload(f, &f->d_list64, f->list64));
   RC(dupload(f, &f->d_surf_unit, o.surf_unit));
   RC(dupload(f, &f->d_surf_ijk, o.surf_ijk));
   std::vector<double> tw(2 * o.N);
@@ -668,8 +676,6 @@ int upload_plan(rtfmm_fmm* f) {
   // y = (sum of M2M_img)^T x (B[j][n] = sum[j][n])
   RC(dupload(f, &f->d_B[B_ADJ_IMG_UP], o.l2l_img));
   RC(dupload(f, &f->d_B[B_ADJ_IMG_DOWN], o.m2m_img_sum));
-  RC(dupload(f, &f->d_idx_pool, f->idx_pool));
-  RC(dupload(f, &f->d_scale_pool, f->scale_pool));
   // M2L: kernel spectra re-laid frequency-major, G[f][d][pair]
   std::vector<double> g64(o.cc8.size());
   for (int d = 0; d < 26; ++d)
@@ -680,33 +686,87 @@ int upload_plan(rtfmm_fmm* f) {
         g64[to] = o.cc8[from];
         g64[to + 1] = o.cc8[from + 1];
       }
+  if (f->m2l32) {
+    std::vector<float> g(g64.size());
+    for (size_t i = 0; i < g.size(); ++i) g[i] = (float)g64[i];
+    float* gp;
+    RC(dupload(f, &gp, g, &f->d_G8));
+    f->d_G8 = gp;
+  } else {
+    double* gp;
+    RC(dupload(f, &gp, g64, &f->d_G8));
+    f->d_G8 = gp;
+  }
+  RC(dupload(f, &f->d_G27, o.cc27sum));
+#undef RC
+  (void)ns;
+  return RTFMM_OK;
+}
+
+// Upload the plan (everything but the per-pass body values) to the device.
+int upload_plan(rtfmm_fmm* f) {
+  const double t0 = wall_s();
+  int rc = ensure_device(f);
+  if (rc) return rc;
+  // a previous plan's buffers are reused (grown if needed); nothing of it
+  // may still run
+  CK(cudaDeviceSynchronize());
+  drop_allocs(f);
+  Plan& p = f->plan;
+  const Operators& o = f->ops;
+  const int64_t n = p.n;
+  const int ns = o.ns, Nf = o.Nf;
+  const size_t ncell = p.cells.size(), nleaf = f->leaves.size();
+  const bool mixed = f->args.precision == RTFMM_FP32_MIXED;
+#define RC(x)          \
+  do {                 \
+    int r_ = (x);      \
+    if (r_) return r_; \
+  } while (0)
+  RC(dalloc(f, &f->d_body64, n));
+  RC(dalloc(f, &f->d_body32, n));
+  RC(dupload(f, &f->d_body_leaf, f->body_leaf));
+  RC(dupload(f, &f->d_perm, p.perm));
+  RC(dalloc(f, &f->d_xin, 3 * n));
+  RC(dalloc(f, &f->d_qin, n));
+  RC(dupload(f, &f->d_leaves, f->leaves));
+  RC(dalloc(f, &f->d_qeq, ncell * ns));
+  RC(dalloc(f, &f->d_pchk, ncell * ns));
+  RC(dalloc(f, &f->d_leafvec, nleaf * ns));
+  RC(dalloc(f, &f->d_leafvec2, nleaf * ns));
+  RC(dalloc(f, &f->d_y, ncell * ns));
+  RC(dalloc(f, &f->d_far_phi, n));
+  RC(dalloc(f, &f->d_far_grad, 3 * n));
+  RC(dalloc(f, &f->d_near_phi, n));
+  RC(dalloc(f, &f->d_near_grad, 3 * n));
+  RC(dalloc(f, &f->d_out_phi, n));
+  RC(dalloc(f, &f->d_out_grad, 3 * n));
+  RC(dupload(f, &f->d_items2, f->items2));
+  RC(dupload(f, &f->d_list_off, f->list_off));
+  if (mixed)
+    RC(dupload(f, &f->d_list32, f->list32));
+  else
+    RC(dupload(f, &f->d_list64, f->list64));
+  RC(dupload(f, &f->d_idx_pool, f->idx_pool));
+  RC(dupload(f, &f->d_scale_pool, f->scale_pool));
   std::vector<int> tsrcT(f->tsrc8.size());
   for (int t = 0; t < f->nT8; ++t)
     for (int d = 0; d < 26; ++d) tsrcT[(size_t)d * f->nT8 + t] = f->tsrc8[(size_t)t * 26 + d];
   RC(dupload(f, &f->d_tsrc8, tsrcT));
   f->m2l32 = mixed && o.P <= kM2L32MaxP;
-  if (f->m2l32) {
-    std::vector<float> g(g64.size());
-    for (size_t i = 0; i < g.size(); ++i) g[i] = (float)g64[i];
-    float* gp;
-    RC(dupload(f, &gp, g));
-    f->d_G8 = gp;
-    float *qp, *pp;
-    RC(dalloc(f, &qp, (size_t)f->nS8 * 8 * Nf * 2));
-    RC(dalloc(f, &pp, (size_t)f->nT8 * 8 * Nf * 2));
-    f->d_Q8 = qp;
-    f->d_Pk8 = pp;
-  } else {
-    double* gp;
-    RC(dupload(f, &gp, g64));
-    f->d_G8 = gp;
-    double *qp, *pp;
-    RC(dalloc(f, &qp, (size_t)f->nS8 * 8 * Nf * 2));
-    RC(dalloc(f, &pp, (size_t)f->nT8 * 8 * Nf * 2));
+  if (f->ops_dev_gen != f->ops_gen) {
+    RC(upload_operators(f));
+    f->ops_dev_gen = f->ops_gen;
+  }
+  {
+    // M2L spectra of the sources and targets, FP32 or FP64
+    const size_t e = f->m2l32 ? sizeof(float) : sizeof(double);
+    char *qp = nullptr, *pp = nullptr;
+    RC(dalloc(f, &qp, (size_t)f->nS8 * 8 * Nf * 2 * e, &f->d_Q8));
+    RC(dalloc(f, &pp, (size_t)f->nT8 * 8 * Nf * 2 * e, &f->d_Pk8));
     f->d_Q8 = qp;
     f->d_Pk8 = pp;
   }
-  RC(dupload(f, &f->d_G27, o.cc27sum));
   RC(dalloc(f, &f->d_Q27, (size_t)f->nS27 * 8 * Nf * 2));
   RC(dalloc(f, &f->d_Pk27, (size_t)f->nT27 * 8 * Nf * 2));
   // M2L up/down blocks: groups of sp child slots (sized to shared memory)
@@ -740,11 +800,17 @@ int upload_plan(rtfmm_fmm* f) {
   RC(dupload(f, &f->d_tscale27, f->tscale27));
   RC(dalloc(f, &f->d_dip, 3 * 256 + 3));
 #undef RC
-  if (f->h_xin) cudaFreeHost(f->h_xin);
-  f->h_xin = nullptr;
-  CK(cudaMallocHost(&f->h_xin, sizeof(double) * std::max<int64_t>(1, 3 * n)));
+  if (f->h_xin_cap < (size_t)std::max<int64_t>(1, 3 * n)) {
+    if (f->h_xin) cudaFreeHost(f->h_xin);
+    f->h_xin = nullptr;
+    f->h_xin_cap = 0;
+    const size_t cap = (size_t)std::max<int64_t>(1, 3 * n + 3 * n / 4);
+    CK(cudaMallocHost(&f->h_xin, sizeof(double) * cap));
+    f->h_xin_cap = cap;
+  }
   if (n > 0) std::memcpy(f->h_xin, f->x_in.data(), sizeof(double) * 3 * n);
   f->device_ready = true;
+  f->setup_s[5] = wall_s() - t0;
   return RTFMM_OK;
 }
 
@@ -1036,6 +1102,50 @@ int rtfmm_b200_destroy(rtfmm_fmm* f) {
   return RTFMM_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Lists, operators (unless cached for this P, images and radius) and device
+// tables of the plan whose tree is built; st[1..3] get their wall times.
+void finish_setup(rtfmm_fmm* f) {
+  double* st = f->setup_s;
+  double t = wall_s();
+  traverse(f->plan);
+  st[1] = wall_s() - t;
+  if (!f->ops_valid || f->ops.P != f->args.P || f->ops.images != f->args.images || f->ops.r0 != f->plan.r0) {
+    t = wall_s();
+    build_operators(f->ops, f->args.P, f->plan.r0, f->args.images);
+    f->ops_valid = true;
+    f->ops_gen++;
+    st[2] = wall_s() - t;
+  }
+  t = wall_s();
+  build_tables(f);
+  st[3] = wall_s() - t;
+}
+
+void begin_setup(rtfmm_fmm* f, int64_t n) {
+  f->setup_done = false;
+  f->pass_done = false;
+  f->plan = Plan();
+  f->plan.args = f->args;
+  f->plan.n = n;
+  for (int k = 0; k < 6; ++k) f->setup_s[k] = 0;
+}
+
+void end_setup(rtfmm_fmm* f, double t0) {
+  f->setup_s[4] = wall_s() - t0;
+  f->setup_done = true;
+  f->device_ready = false;
+  f->grad_q_valid = false;
+  f->pos_on_device = false;
+}
+
+}  // namespace
+
+extern "C" {
+
 int rtfmm_b200_setup(rtfmm_fmm* f, int64_t n, const double* x, const double* q) {
   if (!f) return fail(RTFMM_EINVAL, "null handle");
   if (n < 0 || n > (int64_t)1 << 30) return fail(RTFMM_EINVAL, "n out of range");
@@ -1043,45 +1153,87 @@ int rtfmm_b200_setup(rtfmm_fmm* f, int64_t n, const double* x, const double* q) 
   const double t0 = wall_s();
   if (!finite_all(x, 3 * n) || !finite_all(q, n)) return fail(RTFMM_EINVAL, "non-finite body position or charge");
   try {
-    f->setup_done = false;
-    f->pass_done = false;
-    f->plan = Plan();
-    f->plan.args = f->args;
-    f->plan.n = n;
+    begin_setup(f, n);
     f->x_in.assign(x, x + 3 * n);
     f->q_in.assign(q, q + n);
-    double* st = f->setup_s;
-    for (int k = 0; k < 5; ++k) st[k] = 0;
     double t = wall_s();
     std::string err = build_tree(f->plan, x, q);
     if (!err.empty()) return fail(RTFMM_EINVAL, err);
-    st[0] = wall_s() - t;
-    t = wall_s();
-    traverse(f->plan);
-    st[1] = wall_s() - t;
-    if (!f->ops_valid || f->ops.P != f->args.P || f->ops.images != f->args.images ||
-        f->ops.r0 != f->plan.r0) {
-      t = wall_s();
-      build_operators(f->ops, f->args.P, f->plan.r0, f->args.images);
-      f->ops_valid = true;
-      st[2] = wall_s() - t;
-    }
-    t = wall_s();
-    build_tables(f);
-    st[3] = wall_s() - t;
-    st[4] = wall_s() - t0;
+    f->setup_s[0] = wall_s() - t;
+    finish_setup(f);
   } catch (const std::bad_alloc&) {
     return fail(RTFMM_ENOMEM, "host allocation failed during set-up");
   } catch (const std::exception& e) {
     return fail(RTFMM_EINVAL, std::string("set-up failed: ") + e.what());
   }
-  f->setup_done = true;
-  f->device_ready = false;
-  f->grad_q_valid = false;
-  f->pos_on_device = false;
+  end_setup(f, t0);
   return RTFMM_OK;
 }
 
+int rtfmm_b200_setup_device(rtfmm_fmm* f, int64_t n, const double* x_dev, const double* q_dev) {
+  if (!f) return fail(RTFMM_EINVAL, "null handle");
+  if (n < 0 || n > (int64_t)1 << 30) return fail(RTFMM_EINVAL, "n out of range");
+  if (n > 0 && (!x_dev || !q_dev)) return fail(RTFMM_EINVAL, "null body arrays");
+  const double t0 = wall_s();
+  int rc = ensure_device(f);
+  if (rc) return rc;
+  try {
+    begin_setup(f, n);
+    double t = wall_s();
+    std::string msg;
+    const int tr = device_build_tree(x_dev, n, f->s0, f->plan, msg);
+    if (tr == kTreeError) {
+      f->plan = Plan();
+      return fail(msg == "non-finite body position" ? RTFMM_EINVAL : RTFMM_ECUDA,
+                  msg == "non-finite body position" ? "non-finite body position or charge" : msg);
+    }
+    // host copies: the host-buffer entry points and the tree-order arrays
+    f->x_in.resize(3 * n);
+    f->q_in.resize(n);
+    if (n > 0) {
+      CK(cudaMemcpyAsync(f->x_in.data(), x_dev, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, f->s0));
+      CK(cudaMemcpyAsync(f->q_in.data(), q_dev, sizeof(double) * n, cudaMemcpyDeviceToHost, f->s0));
+      CK(cudaStreamSynchronize(f->s0));
+    }
+    if (!finite_all(f->q_in.data(), n)) {
+      f->plan = Plan();
+      return fail(RTFMM_EINVAL, "non-finite body position or charge");
+    }
+    if (tr == kTreeTooDeep) {
+      std::string err = build_tree(f->plan, f->x_in.data(), f->q_in.data());
+      if (!err.empty()) return fail(RTFMM_EINVAL, err);
+    } else {
+      Plan& p = f->plan;
+      p.x.resize(3 * n);
+      p.q.resize(n);
+#pragma omp parallel for schedule(static)
+      for (int64_t i = 0; i < n; ++i) {
+        const int64_t k = p.perm[i];
+        p.x[3 * i + 0] = f->x_in[3 * k + 0];
+        p.x[3 * i + 1] = f->x_in[3 * k + 1];
+        p.x[3 * i + 2] = f->x_in[3 * k + 2];
+        p.q[i] = f->q_in[k];
+      }
+    }
+    f->setup_s[0] = wall_s() - t;
+    finish_setup(f);
+  } catch (const std::bad_alloc&) {
+    return fail(RTFMM_ENOMEM, "host allocation failed during set-up");
+  } catch (const std::exception& e) {
+    return fail(RTFMM_EINVAL, std::string("set-up failed: ") + e.what());
+  }
+  end_setup(f, t0);
+  // device tables, then the bodies gathered into tree order on the device
+  rc = upload_plan(f);
+  if (rc) return rc;
+  if (n > 0) {
+    CK(launch_gather_bodies(x_dev, q_dev, f->d_perm, (int)n, f->d_body64, f->s0));
+    CK(cudaStreamSynchronize(f->s0));
+  }
+  f->pos_on_device = true;
+  f->setup_s[4] = wall_s() - t0;
+  return RTFMM_OK;
+}
 int rtfmm_b200_upload(rtfmm_fmm* f) {
   if (!f) return fail(RTFMM_EINVAL, "null handle");
   if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");
@@ -1310,9 +1462,11 @@ int rtfmm_b200_flush_l2(rtfmm_fmm* f) {
   if (!f->s0) return fail(RTFMM_ESTATE, "no device state");
   CK(cudaSetDevice(f->dev));
   if (!f->d_flush) {
+    char* fl = nullptr;
+    int rc = dalloc(f, &fl, (size_t)256 << 20, &f->d_flush);
+    if (rc) return rc;
+    f->d_flush = fl;
     f->flush_bytes = (size_t)256 << 20;
-    CK(cudaMalloc(&f->d_flush, f->flush_bytes));
-    f->allocs.push_back(f->d_flush);
   }
   CK(cudaMemsetAsync(f->d_flush, f->launches & 0xff, f->flush_bytes, f->s0));
   CK(cudaStreamSynchronize(f->s0));
@@ -1322,7 +1476,7 @@ int rtfmm_b200_flush_l2(rtfmm_fmm* f) {
 int rtfmm_b200_setup_times(rtfmm_fmm* f, double* s, int cap) {
   if (!f || !s) return fail(RTFMM_EINVAL, "null argument");
   if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");
-  for (int k = 0; k < 5 && k < cap; ++k) s[k] = f->setup_s[k];
+  for (int k = 0; k < 6 && k < cap; ++k) s[k] = f->setup_s[k];
   return RTFMM_OK;
 }
 
@@ -1332,7 +1486,8 @@ int rtfmm_b200_info(rtfmm_fmm* f, int64_t* info, int cap) {
   int64_t pairs = 0;
   for (size_t l = 0; l < f->leaves.size(); ++l)
     for (int e = f->list_off[l]; e < f->list_off[l + 1]; ++e)
-      pairs += (int64_t)f->leaves[l].bnum * f->leaves[f->list32[e].leaf].bnum;
+      pairs += (int64_t)f->leaves[l].bnum *
+               f->leaves[f->list32.empty() ? f->list64[e].leaf : f->list32[e].leaf].bnum;
   int64_t td = 0;
   for (int v8 : f->tsrc8) td += v8 >= 0;
   int64_t v[12] = {(int64_t)f->plan.cells.size(), (int64_t)f->leaves.size(), f->plan.dmin, f->plan.dmax,

@@ -32,6 +32,7 @@ STAGE_NAMES = ("prep", "P2M", "M2M", "M2L_up", "M2L_hadamard", "M2L_down", "L2L"
 # Every entry point declared in include/rtfmm_b200.h.
 EXPORTS = (
     "rtfmm_b200_default_args", "rtfmm_b200_create", "rtfmm_b200_destroy", "rtfmm_b200_setup",
+    "rtfmm_b200_setup_device",
     "rtfmm_b200_evaluate", "rtfmm_b200_solve", "rtfmm_b200_upload", "rtfmm_b200_evaluate_device",
     "rtfmm_b200_download", "rtfmm_b200_forward_device", "rtfmm_b200_adjoint", "rtfmm_b200_adjoint_device",
     "rtfmm_b200_stage_times",
@@ -78,6 +79,7 @@ def lib():
         "rtfmm_b200_create": (ctypes.c_int, [ctypes.POINTER(_Args), ctypes.POINTER(_vp)]),
         "rtfmm_b200_destroy": (ctypes.c_int, [_vp]),
         "rtfmm_b200_setup": (ctypes.c_int, [_vp, ctypes.c_int64, _dp, _dp]),
+        "rtfmm_b200_setup_device": (ctypes.c_int, [_vp, ctypes.c_int64, _vp, _vp]),
         "rtfmm_b200_evaluate": (ctypes.c_int, [_vp, _dp, _dp, _dp]),
         "rtfmm_b200_solve": (ctypes.c_int, [_vp, ctypes.c_int64, _dp, _dp, _dp, _dp]),
         "rtfmm_b200_upload": (ctypes.c_int, [_vp]),
@@ -208,6 +210,16 @@ class LaplaceFMM:
         _check(lib().rtfmm_b200_setup(self._h, self.n, _ptr(self.x), _ptr(self.q)))
         self._set_up = True
 
+    def setup_device(self, x_ptr, q_ptr, n=None):
+        """Set-up from bodies in device memory: integer device addresses
+        (e.g. a torch tensor's data_ptr()) of x (n, 3) and q (n), float64.
+        The octree is built on the GPU; the bodies stay on the device, so
+        evaluate_device() / forward_device() follow without upload()."""
+        n = self.n if n is None else int(n)
+        _check(lib().rtfmm_b200_setup_device(self._h, n, _vp(x_ptr or None), _vp(q_ptr or None)))
+        self.n = n
+        self._set_up = True
+
     def evaluate(self, q=None):
         """The evaluation pass with host buffers; returns (phi, grad)."""
         if not self._set_up:
@@ -278,11 +290,12 @@ class LaplaceFMM:
 
     # -- introspection ------------------------------------------------------------
     def setup_times(self):
-        """Wall seconds of the last setup's phases: tree, lists, operators
-        (0 when cached), device tables, total."""
-        v = np.zeros(5)
-        _check(lib().rtfmm_b200_setup_times(self._h, _ptr(v), 5))
-        return dict(zip(("tree", "lists", "operators", "tables", "total"), v.tolist()))
+        """Wall seconds of the last set-up's phases: tree, lists, operators
+        (0 when cached), host tables, the setup call, and the upload of the
+        device tables."""
+        v = np.zeros(6)
+        _check(lib().rtfmm_b200_setup_times(self._h, _ptr(v), 6))
+        return dict(zip(("tree", "lists", "operators", "tables", "total", "upload"), v.tolist()))
 
     def info(self):
         v = np.zeros(12, dtype=np.int64)

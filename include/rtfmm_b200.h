@@ -105,6 +105,20 @@ int rtfmm_b200_destroy(rtfmm_fmm* fmm);
 int rtfmm_b200_setup(rtfmm_fmm* fmm, int64_t n, const double* x, const double* q);
 
 /*
+ * rtfmm_b200_setup for bodies already in device memory (x_dev n*3, q_dev n,
+ * on the handle's device).  The octree is built on the GPU (path keys, a
+ * radix sort, one split pass per level) and equals rtfmm_b200_setup's tree
+ * and body order exactly; a tree deeper than 21 levels is built on the host
+ * instead.  The lists, operators and tables follow as in rtfmm_b200_setup,
+ * then the device tables are uploaded and the bodies gathered into tree
+ * order on the device, so rtfmm_b200_evaluate_device and
+ * rtfmm_b200_forward_device can run at once (no rtfmm_b200_upload).  Host
+ * copies of x and q are kept for the host-buffer entry points.  Same error
+ * codes as rtfmm_b200_setup.
+ */
+int rtfmm_b200_setup_device(rtfmm_fmm* fmm, int64_t n, const double* x_dev, const double* q_dev);
+
+/*
  * The evaluation pass with host buffers: copies q (and, on the first call
  * after setup, the positions the tree was built on; they then stay on the
  * device) to the device, runs P2M, M2M, M2L, L2L, L2P and P2P
@@ -205,11 +219,13 @@ int rtfmm_b200_flush_l2(rtfmm_fmm* fmm);
 
 /* ---- introspection (host data after setup; used by parity tests) ---- */
 
-/* Host set-up wall times of the last rtfmm_b200_setup, in seconds:
- * s[0] octree, s[1] interaction lists, s[2] operator tables (0 when the
- * handle's cached tables were reused), s[3] device tables, s[4] the whole
- * call.  The reference times the same phases separately from the
- * evaluation (3dpp/src/fmm.cpp:13-50).  Writes min(cap, 5) values. */
+/* Set-up wall times of the last set-up, in seconds: s[0] octree, s[1]
+ * interaction lists, s[2] operator tables (0 when the handle's cached tables
+ * were reused), s[3] host tables of the pass, s[4] the whole setup call,
+ * s[5] the upload of the device tables (done by rtfmm_b200_setup_device, or
+ * by the first upload/evaluate after rtfmm_b200_setup).  The reference times
+ * the same phases separately from the evaluation (3dpp/src/fmm.cpp:13-50).
+ * Writes min(cap, 6) values. */
 int rtfmm_b200_setup_times(rtfmm_fmm* fmm, double* s, int cap);
 
 /* Tree and list sizes.  info[0..11] = ncell (incl. image cells), nleaf,
