@@ -13,6 +13,7 @@
 #include <cstring>
 #include <functional>
 #include <new>
+#include <stdexcept>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -129,6 +130,11 @@ struct rtfmm_fmm {
   // operator tables: generation built on the host / uploaded to the device
   uint64_t ops_gen = 0, ops_dev_gen = 0;
   size_t h_xin_cap = 0;  // doubles in h_xin
+  // x_in, q_in, plan.x, plan.q, plan.perm and h_xin hold the set-up bodies;
+  // after a device set-up they are fetched from d_xin, d_qin and d_perm on
+  // first use (ensure_host_bodies)
+  bool host_bodies = true;
+  char tree_slots[64] = {};  // pool keys of the device tree's and walk's scratch
   double4* d_body64 = nullptr;
   float4* d_body32 = nullptr;
   int* d_body_leaf = nullptr;
@@ -726,7 +732,10 @@ int upload_plan(rtfmm_fmm* f) {
   RC(dalloc(f, &f->d_body64, n));
   RC(dalloc(f, &f->d_body32, n));
   RC(dupload(f, &f->d_body_leaf, f->body_leaf));
-  RC(dupload(f, &f->d_perm, p.perm));
+  if (f->host_bodies)
+    RC(dupload(f, &f->d_perm, p.perm));
+  else
+    RC(dalloc(f, &f->d_perm, n));  // written by the device tree
   RC(dalloc(f, &f->d_xin, 3 * n));
   RC(dalloc(f, &f->d_qin, n));
   RC(dupload(f, &f->d_leaves, f->leaves));
@@ -808,7 +817,7 @@ int upload_plan(rtfmm_fmm* f) {
     CK(cudaMallocHost(&f->h_xin, sizeof(double) * cap));
     f->h_xin_cap = cap;
   }
-  if (n > 0) std::memcpy(f->h_xin, f->x_in.data(), sizeof(double) * 3 * n);
+  if (n > 0 && f->host_bodies) std::memcpy(f->h_xin, f->x_in.data(), sizeof(double) * 3 * n);
   f->device_ready = true;
   f->setup_s[5] = wall_s() - t0;
   return RTFMM_OK;
@@ -1106,12 +1115,66 @@ int rtfmm_b200_destroy(rtfmm_fmm* f) {
 
 namespace {
 
-// Lists, operators (unless cached for this P, images and radius) and device
-// tables of the plan whose tree is built; st[1..3] get their wall times.
-void finish_setup(rtfmm_fmm* f) {
+// After a device set-up: the input-order bodies and the permutation from
+// the device into x_in, q_in, plan.perm, plus (with tree_order) plan.x,
+// plan.q and the pinned staging copy.  Called before anything overwrites
+// d_xin or d_qin.
+int ensure_host_bodies(rtfmm_fmm* f, bool tree_order = true) {
+  if (f->host_bodies) return RTFMM_OK;
+  Plan& p = f->plan;
+  const int64_t n = p.n;
+  f->x_in.resize(3 * n);
+  f->q_in.resize(n);
+  if (n > 0) {
+    CK(cudaSetDevice(f->dev));
+    CK(cudaMemcpyAsync(f->x_in.data(), f->d_xin, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, f->s0));
+    CK(cudaMemcpyAsync(f->q_in.data(), f->d_qin, sizeof(double) * n, cudaMemcpyDeviceToHost, f->s0));
+    if (tree_order) {
+      p.perm.resize(n);
+      CK(cudaMemcpyAsync(p.perm.data(), f->d_perm, sizeof(int64_t) * n, cudaMemcpyDeviceToHost, f->s0));
+    }
+    CK(cudaStreamSynchronize(f->s0));
+  }
+  if (!tree_order) return RTFMM_OK;
+  p.x.resize(3 * n);
+  p.q.resize(n);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t k = p.perm[i];
+    p.x[3 * i + 0] = f->x_in[3 * k + 0];
+    p.x[3 * i + 1] = f->x_in[3 * k + 1];
+    p.x[3 * i + 2] = f->x_in[3 * k + 2];
+    p.q[i] = f->q_in[k];
+  }
+  if (f->h_xin && f->h_xin_cap >= (size_t)(3 * n) && n > 0)
+    std::memcpy(f->h_xin, f->x_in.data(), sizeof(double) * 3 * n);
+  f->host_bodies = true;
+  return RTFMM_OK;
+}
+
+// First scratch slot of the GPU walk (the tree uses the ones below).
+constexpr int kWalkSlots = 16;
+
+// Lists (the P2P walk on the GPU with `gpu` scratch), operators (unless
+// cached for this P, images and radius) and host tables of the plan whose
+// tree is built; st[1..3] get their wall times.
+void finish_setup(rtfmm_fmm* f, const TreeScratchFn* gpu = nullptr) {
   double* st = f->setup_s;
   double t = wall_s();
-  traverse(f->plan);
+  if (gpu) {
+    // the P2P walk on the GPU (the host walk when it is too deep for it)
+    const std::vector<WalkRoot> roots = traverse_begin(f->plan);
+    std::string msg;
+    const int rc = device_p2p_walk(f->plan, roots, f->s0, *gpu, kWalkSlots, msg);
+    if (rc == kTreeError) throw std::runtime_error(msg);
+    if (rc == kTreeTooDeep) {
+      f->plan.p2p.clear();
+      traverse_p2p(f->plan, roots);
+    }
+    traverse_finish(f->plan);
+  } else {
+    traverse(f->plan);
+  }
   st[1] = wall_s() - t;
   if (!f->ops_valid || f->ops.P != f->args.P || f->ops.images != f->args.images || f->ops.r0 != f->plan.r0) {
     t = wall_s();
@@ -1154,6 +1217,7 @@ int rtfmm_b200_setup(rtfmm_fmm* f, int64_t n, const double* x, const double* q) 
   if (!finite_all(x, 3 * n) || !finite_all(q, n)) return fail(RTFMM_EINVAL, "non-finite body position or charge");
   try {
     begin_setup(f, n);
+    f->host_bodies = true;
     f->x_in.assign(x, x + 3 * n);
     f->q_in.assign(q, q + n);
     double t = wall_s();
@@ -1177,46 +1241,47 @@ int rtfmm_b200_setup_device(rtfmm_fmm* f, int64_t n, const double* x_dev, const 
   const double t0 = wall_s();
   int rc = ensure_device(f);
   if (rc) return rc;
+  // nothing of a previous plan may still read the buffers reused below
+  CK(cudaDeviceSynchronize());
   try {
     begin_setup(f, n);
     double t = wall_s();
+    // the bodies in input order (d_xin, d_qin) and the permutation (d_perm)
+    // stay on the device; the host copies follow on first use
+    double *dx = nullptr, *dq = nullptr;
+    int64_t* dp = nullptr;
+    if ((rc = dalloc(f, &dx, 3 * n, &f->d_xin)) || (rc = dalloc(f, &dq, n, &f->d_qin)) ||
+        (rc = dalloc(f, &dp, n, &f->d_perm)))
+      return rc;
+    f->d_xin = dx;
+    f->d_qin = dq;
+    f->d_perm = dp;
     std::string msg;
-    const int tr = device_build_tree(x_dev, n, f->s0, f->plan, msg);
+    TreeScratchFn scratch = [f](int slot, size_t bytes) -> void* {
+      if (slot < 0 || slot >= (int)sizeof(f->tree_slots)) return nullptr;
+      char* q = nullptr;
+      return dalloc(f, &q, bytes, &f->tree_slots[slot]) ? nullptr : (void*)q;
+    };
+    const int tr = device_build_tree(x_dev, q_dev, n, f->s0, f->plan, dp, scratch, msg);
     if (tr == kTreeError) {
       f->plan = Plan();
-      return fail(msg == "non-finite body position" ? RTFMM_EINVAL : RTFMM_ECUDA,
-                  msg == "non-finite body position" ? "non-finite body position or charge" : msg);
+      const bool bad = msg == "non-finite body position or charge";
+      return fail(bad ? RTFMM_EINVAL : RTFMM_ECUDA, msg);
     }
-    // host copies: the host-buffer entry points and the tree-order arrays
-    f->x_in.resize(3 * n);
-    f->q_in.resize(n);
     if (n > 0) {
-      CK(cudaMemcpyAsync(f->x_in.data(), x_dev, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, f->s0));
-      CK(cudaMemcpyAsync(f->q_in.data(), q_dev, sizeof(double) * n, cudaMemcpyDeviceToHost, f->s0));
-      CK(cudaStreamSynchronize(f->s0));
+      CK(cudaMemcpyAsync(dx, x_dev, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, f->s0));
+      CK(cudaMemcpyAsync(dq, q_dev, sizeof(double) * n, cudaMemcpyDeviceToDevice, f->s0));
     }
-    if (!finite_all(f->q_in.data(), n)) {
-      f->plan = Plan();
-      return fail(RTFMM_EINVAL, "non-finite body position or charge");
-    }
+    f->host_bodies = false;
     if (tr == kTreeTooDeep) {
+      rc = ensure_host_bodies(f, false);
+      if (rc) return rc;
       std::string err = build_tree(f->plan, f->x_in.data(), f->q_in.data());
       if (!err.empty()) return fail(RTFMM_EINVAL, err);
-    } else {
-      Plan& p = f->plan;
-      p.x.resize(3 * n);
-      p.q.resize(n);
-#pragma omp parallel for schedule(static)
-      for (int64_t i = 0; i < n; ++i) {
-        const int64_t k = p.perm[i];
-        p.x[3 * i + 0] = f->x_in[3 * k + 0];
-        p.x[3 * i + 1] = f->x_in[3 * k + 1];
-        p.x[3 * i + 2] = f->x_in[3 * k + 2];
-        p.q[i] = f->q_in[k];
-      }
+      f->host_bodies = true;
     }
     f->setup_s[0] = wall_s() - t;
-    finish_setup(f);
+    finish_setup(f, &scratch);
   } catch (const std::bad_alloc&) {
     return fail(RTFMM_ENOMEM, "host allocation failed during set-up");
   } catch (const std::exception& e) {
@@ -1227,13 +1292,14 @@ int rtfmm_b200_setup_device(rtfmm_fmm* f, int64_t n, const double* x_dev, const 
   rc = upload_plan(f);
   if (rc) return rc;
   if (n > 0) {
-    CK(launch_gather_bodies(x_dev, q_dev, f->d_perm, (int)n, f->d_body64, f->s0));
+    CK(launch_gather_bodies(f->d_xin, f->d_qin, f->d_perm, (int)n, f->d_body64, f->s0));
     CK(cudaStreamSynchronize(f->s0));
   }
   f->pos_on_device = true;
   f->setup_s[4] = wall_s() - t0;
   return RTFMM_OK;
 }
+
 int rtfmm_b200_upload(rtfmm_fmm* f) {
   if (!f) return fail(RTFMM_EINVAL, "null handle");
   if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");
@@ -1242,11 +1308,15 @@ int rtfmm_b200_upload(rtfmm_fmm* f) {
     if (rc) return rc;
   }
   CK(cudaSetDevice(f->dev));
-  if (f->plan.n > 0) {
-    std::vector<double4> b(f->plan.n);
-    for (int64_t i = 0; i < f->plan.n; ++i)
-      b[i] = make_double4(f->plan.x[3 * i], f->plan.x[3 * i + 1], f->plan.x[3 * i + 2], f->plan.q[i]);
-    CK(cudaMemcpy(f->d_body64, b.data(), sizeof(double4) * b.size(), cudaMemcpyHostToDevice));
+  int rc = ensure_host_bodies(f);
+  if (rc) return rc;
+  const int64_t n = f->plan.n;
+  if (n > 0) {
+    // input order up (positions from the pinned copy), tree order on the device
+    CK(cudaMemcpyAsync(f->d_xin, f->h_xin, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, f->s0));
+    CK(cudaMemcpyAsync(f->d_qin, f->q_in.data(), sizeof(double) * n, cudaMemcpyHostToDevice, f->s0));
+    CK(launch_gather_bodies(f->d_xin, f->d_qin, f->d_perm, (int)n, f->d_body64, f->s0));
+    CK(cudaStreamSynchronize(f->s0));
   }
   f->grad_q_valid = false;
   f->pos_on_device = true;
@@ -1318,6 +1388,8 @@ int rtfmm_b200_evaluate(rtfmm_fmm* f, const double* q, double* phi, double* grad
     if (rc) return rc;
   }
   CK(cudaSetDevice(f->dev));
+  int rc0 = ensure_host_bodies(f);
+  if (rc0) return rc0;
   // host -> device (input order), then into tree order on the device; the
   // positions move only on the first call after set-up
   CK(cudaMemcpyAsync(f->d_qin, q ? q : f->q_in.data(), sizeof(double) * n, cudaMemcpyHostToDevice, f->s0));
@@ -1407,6 +1479,8 @@ int rtfmm_b200_adjoint(rtfmm_fmm* f, const double* w, double* dLdq, double* dLdx
   }
   CK(cudaSetDevice(f->dev));
   int rc = ensure_adj_scratch(f);
+  if (rc) return rc;
+  rc = ensure_host_bodies(f);
   if (rc) return rc;
   // the bodies with the set-up charges, as the forward solve had them
   CK(cudaMemcpyAsync(f->d_xin, f->h_xin, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, f->s0));
@@ -1525,6 +1599,8 @@ int rtfmm_b200_get_cells(rtfmm_fmm* f, int32_t* ints, double* reals) {
 int rtfmm_b200_get_perm(rtfmm_fmm* f, int64_t* perm) {
   if (!f || !perm) return fail(RTFMM_EINVAL, "null argument");
   if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");
+  int rc = ensure_host_bodies(f);
+  if (rc) return rc;
   std::memcpy(perm, f->plan.perm.data(), sizeof(int64_t) * f->plan.perm.size());
   return RTFMM_OK;
 }

@@ -3,6 +3,7 @@
 // operators are the same sets the reference builds; the evaluation pass
 // itself runs on the GPU (rtfmm_kernels.cu).
 #include "rtfmm_plan.h"
+#include "rtfmm_walk.h"
 
 #include <algorithm>
 #include <array>
@@ -199,56 +200,19 @@ struct Walker {
   // horizontal_origin (traverser.cpp:70-148) as a stack of frames; children
   // are visited in the reference's recursion order.  M2P/P2L cases become P2P
   // (traverser.cpp:75-86); M2L pairs of the dual walk are counted only (the
-  // M2L of the pass uses the parent map).
-  struct Frame {
-    int tc, sc, tcp, scp;
+  // M2L of the pass uses the parent map).  The step itself is walk_step
+  // (rtfmm_walk.h), which the GPU walk runs too.
+  using Frame = WalkFrame;
+  struct Cells {
+    const std::vector<Cell>& c;
+    double x(int i, int k) const { return c[i].x[k]; }
+    double r(int i) const { return c[i].r; }
+    int depth(int i) const { return c[i].depth; }
+    int cnum(int i) const { return c[i].cnum; }
+    int coff(int i) const { return c[i].coff; }
   };
-  // One frame: returns 1 and sets *hit for a P2P pair, or writes the child
-  // frames in visiting order to kids (returning -count), or returns 0.
   int step(const Frame& f, const V3& off, int* hit, Frame* kids) const {
-    int divide = 0;
-    const Cell& T = p.cells[f.tc];
-    const Cell& S = p.cells[f.sc];
-    if (!adjacent(f.tc, f.sc, off)) {
-      if (adjacent(f.tc, f.scp, off) && leaf(f.tc) && p.cells[f.scp].depth >= T.depth) {
-        *hit = f.sc;
-        return 1;
-      } else if (adjacent(f.tcp, f.sc, off) && leaf(f.sc) && p.cells[f.tcp].depth >= S.depth) {
-        *hit = f.sc;
-        return 1;
-      } else if (neighbour(f.tcp, f.scp, off)) {
-        // an M2L pair of the dual walk; served by the parent map
-      } else {
-        if (leaf(f.tc) && leaf(f.sc)) {
-        } else if (!leaf(f.tc) && leaf(f.sc)) {
-          divide = 1;
-        } else if (leaf(f.tc) && !leaf(f.sc)) {
-          divide = 2;
-        } else {
-          divide = T.r >= S.r ? 1 : 2;
-        }
-      }
-    } else {
-      if (leaf(f.tc) && leaf(f.sc)) {
-        *hit = f.sc;
-        return 1;
-      } else if (!leaf(f.tc) && leaf(f.sc)) {
-        divide = 1;
-      } else if (leaf(f.tc) && !leaf(f.sc)) {
-        divide = 2;
-      } else {
-        divide = T.r >= S.r ? 1 : 2;
-      }
-    }
-    if (divide == 1) {
-      for (int i = 0; i < T.cnum; ++i) kids[i] = {T.coff + i, f.sc, f.tc, f.scp};
-      return -T.cnum;
-    }
-    if (divide == 2) {
-      for (int i = 0; i < S.cnum; ++i) kids[i] = {f.tc, S.coff + i, f.tcp, f.sc};
-      return -S.cnum;
-    }
-    return 0;
+    return walk_step(Cells{p.cells}, f, off.data(), hit, kids);
   }
 
   // The walk below one frame, its P2P pairs (target, source) appended in the
@@ -318,39 +282,52 @@ struct Walker {
 
 }  // namespace
 
-void traverse(Plan& plan) {
+std::vector<WalkRoot> traverse_begin(Plan& plan) {
   const Args& a = plan.args;
   const double cycle = a.cycle;
-  Walker w(plan);
   plan.p2p.clear();
   plan.m2l.clear();
   // The depth -1 super-cell exists before the tree-level M2L parent map is
   // built (traverser.cpp:30-35); deeper image cells are added afterwards.
-  if (a.images == 0) {
-    w.walks({{0, 0, 0, 0}}, {V3{0, 0, 0}});
-  } else {
-    Cell c;
-    c.octant = 13;
-    c.depth = -1;
-    c.r = plan.cells[0].r * 3;
-    c.x = plan.cells[0].x;
-    c.coff = 0;
-    c.cnum = 1;
-    c.boff = 0;
-    c.bnum = plan.cells[0].bnum;
-    plan.cells.push_back(c);
-    const int cidx = (int)plan.cells.size() - 1;
-    std::vector<Walker::Frame> roots;
-    std::vector<V3> offs;
-    for (int pz = -1; pz <= 1; ++pz)
-      for (int py = -1; py <= 1; ++py)
-        for (int px = -1; px <= 1; ++px) {
-          roots.push_back({0, 0, cidx, cidx});
-          offs.push_back(V3{px * cycle, py * cycle, pz * cycle});
-        }
-    w.walks(roots, offs);
-  }
+  if (a.images == 0) return {WalkRoot{0, 0, 0, 0, V3{0, 0, 0}}};
+  Cell c;
+  c.octant = 13;
+  c.depth = -1;
+  c.r = plan.cells[0].r * 3;
+  c.x = plan.cells[0].x;
+  c.coff = 0;
+  c.cnum = 1;
+  c.boff = 0;
+  c.bnum = plan.cells[0].bnum;
+  plan.cells.push_back(c);
+  const int cidx = (int)plan.cells.size() - 1;
+  std::vector<WalkRoot> roots;
+  for (int pz = -1; pz <= 1; ++pz)
+    for (int py = -1; py <= 1; ++py)
+      for (int px = -1; px <= 1; ++px) roots.push_back({0, 0, cidx, cidx, V3{px * cycle, py * cycle, pz * cycle}});
+  return roots;
+}
 
+void traverse_p2p(Plan& plan, const std::vector<WalkRoot>& roots) {
+  Walker w(plan);
+  std::vector<Walker::Frame> frames;
+  std::vector<V3> offs;
+  for (const WalkRoot& r : roots) {
+    frames.push_back({r.tc, r.sc, r.tcp, r.scp});
+    offs.push_back(r.off);
+  }
+  w.walks(frames, offs);
+}
+
+void traverse(Plan& plan) {
+  traverse_p2p(plan, traverse_begin(plan));
+  traverse_finish(plan);
+}
+
+void traverse_finish(Plan& plan) {
+  const Args& a = plan.args;
+  const double cycle = a.cycle;
+  Walker w(plan);
   // M2L parent map over the tree cells (make_M2L_parent_map and the
   // periodic part of make_M2L_parent_map_i1, traverser.cpp:234-282).  The
   // reference tests every cell pair; same-depth cells sit on a lattice of

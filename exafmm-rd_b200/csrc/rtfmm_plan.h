@@ -126,7 +126,23 @@ struct Plan {
 
 // Tree and lists (exact restatement of the reference's algorithms).
 std::string build_tree(Plan& plan, const double* x, const double* q);
-void traverse(Plan& plan);
+void traverse(Plan& plan);  // = traverse_begin, traverse_p2p, traverse_finish
+
+// One root frame of the P2P dual-tree walk: (target, source, target parent,
+// source parent) and the periodic offset of the walk.
+struct WalkRoot {
+  int tc, sc, tcp, scp;
+  V3 off;
+};
+// Clears the lists, adds the depth -1 image super-cell (images >= 1) and
+// returns the walk's root frames, one per periodic offset, in walk order.
+std::vector<WalkRoot> traverse_begin(Plan& plan);
+// The P2P lists by the dual-tree walk from the roots (horizontal_origin,
+// traverser.cpp:70-176), on the host.
+void traverse_p2p(Plan& plan, const std::vector<WalkRoot>& roots);
+// The M2L parent map, the deeper image cells and the list counts.
+void traverse_finish(Plan& plan);
+
 
 // Operator tables.
 void build_operators(Operators& ops, int P, double r0, int images);

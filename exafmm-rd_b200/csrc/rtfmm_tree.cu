@@ -22,7 +22,8 @@
 // The cells and the permutation are the host builder's, bit for bit: the
 // centres are recomputed on the host from the parents exactly as the host
 // build does, and only the octants, counts and order come from the device.
-// A tree that needs more than 21 levels is left to the host builder.
+// The permutation stays on the device.  A tree that needs more than 21
+// levels is left to the host builder.
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
@@ -37,12 +38,13 @@ namespace {
 
 constexpr int kKeyLevels = 21;
 
-__global__ void k_path_keys(const double* __restrict__ x, int n, double cx, double cy, double cz, double r0,
-                            unsigned long long* __restrict__ key, int* __restrict__ idx, int* __restrict__ bad) {
+__global__ void k_path_keys(const double* __restrict__ x, const double* __restrict__ q, int n, double cx, double cy,
+                            double cz, double r0, unsigned long long* __restrict__ key, int* __restrict__ idx,
+                            int* __restrict__ bad) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double px = x[3 * i], py = x[3 * i + 1], pz = x[3 * i + 2];
-  if (!isfinite(px) || !isfinite(py) || !isfinite(pz)) atomicExch(bad, 1);
+  if (!isfinite(px) || !isfinite(py) || !isfinite(pz) || !isfinite(q[i])) atomicExch(bad, 1);
   double c0 = cx, c1 = cy, c2 = cz, r = r0;
   unsigned long long k = 0;
   for (int l = 0; l < kKeyLevels; ++l) {
@@ -122,19 +124,19 @@ __global__ void k_leaf_keys(const int* __restrict__ lboff, const int* __restrict
   }
 }
 
-struct DevBufs {
-  std::vector<void*> p;
-  ~DevBufs() {
-    for (void* q : p) cudaFree(q);
-  }
+__global__ void k_perm_out(const unsigned long long* __restrict__ key2, int n, int64_t* __restrict__ perm) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) perm[i] = (int64_t)(key2[i] & 0xffffffffull);
+}
+
+// Scratch buffers by slot from the caller's allocator.
+struct Scratch {
+  const TreeScratchFn& fn;
+  int next = 0;
   template <typename T>
   cudaError_t get(T** out, size_t count) {
-    void* q = nullptr;
-    cudaError_t e = cudaMalloc(&q, std::max<size_t>(1, count) * sizeof(T));
-    if (e != cudaSuccess) return e;
-    p.push_back(q);
-    *out = (T*)q;
-    return cudaSuccess;
+    *out = (T*)fn(next++, std::max<size_t>(1, count) * sizeof(T));
+    return *out ? cudaSuccess : cudaErrorMemoryAllocation;
   }
 };
 
@@ -151,7 +153,8 @@ int cdiv(int64_t a, int b) { return (int)((a + b - 1) / b); }
     }                                                          \
   } while (0)
 
-int device_build_tree(const double* x_dev, int64_t n64, cudaStream_t st, Plan& plan, std::string& msg) {
+int device_build_tree(const double* x_dev, const double* q_dev, int64_t n64, cudaStream_t st, Plan& plan,
+                      int64_t* d_perm, const TreeScratchFn& scratch, std::string& msg) {
   const Args& a = plan.args;
   const int n = (int)n64;
   plan.n = n64;
@@ -167,12 +170,12 @@ int device_build_tree(const double* x_dev, int64_t n64, cudaStream_t st, Plan& p
   root.boff = 0;
   root.bnum = n;
   plan.cells.push_back(root);
-  plan.perm.resize(n64);
+  plan.perm.clear();
   if (n == 0) {
     plan.ntree = 1;
     return kTreeOk;
   }
-  DevBufs B;
+  Scratch B{scratch};
   unsigned long long *key = nullptr, *key_alt = nullptr;
   int *idx = nullptr, *idx_alt = nullptr, *flags = nullptr;
   TCK(B.get(&key, n));
@@ -181,7 +184,7 @@ int device_build_tree(const double* x_dev, int64_t n64, cudaStream_t st, Plan& p
   TCK(B.get(&idx_alt, n));
   TCK(B.get(&flags, 2));
   TCK(cudaMemsetAsync(flags, 0, 2 * sizeof(int), st));
-  k_path_keys<<<cdiv(n, 256), 256, 0, st>>>(x_dev, n, a.x[0], a.x[1], a.x[2], plan.r0, key, idx, flags);
+  k_path_keys<<<cdiv(n, 256), 256, 0, st>>>(x_dev, q_dev, n, a.x[0], a.x[1], a.x[2], plan.r0, key, idx, flags);
   TCK(cudaGetLastError());
 
   // stable sort by the 63 key bits
@@ -228,7 +231,7 @@ int device_build_tree(const double* x_dev, int64_t n64, cudaStream_t st, Plan& p
     TCK(cudaMemcpyAsync(h_flags, flags, sizeof(h_flags), cudaMemcpyDeviceToHost, st));
     TCK(cudaStreamSynchronize(st));
     if (h_flags[0]) {
-      msg = "non-finite body position";
+      msg = "non-finite body position or charge";
       return kTreeError;
     }
     if (h_flags[1]) return kTreeTooDeep;
@@ -292,10 +295,8 @@ int device_build_tree(const double* x_dev, int64_t n64, cudaStream_t st, Plan& p
   int bits = 1;
   while ((1ll << bits) < n64) ++bits;
   TCK(cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, key, key_alt, n, 0, 32 + bits, st));
-  std::vector<unsigned long long> k2(n);
-  TCK(cudaMemcpyAsync(k2.data(), key_alt, sizeof(unsigned long long) * n, cudaMemcpyDeviceToHost, st));
-  TCK(cudaStreamSynchronize(st));
-  for (int i = 0; i < n; ++i) plan.perm[i] = (int64_t)(k2[i] & 0xffffffffull);
+  k_perm_out<<<cdiv(n, 256), 256, 0, st>>>(key_alt, n, d_perm);
+  TCK(cudaGetLastError());
   return kTreeOk;
 }
 

@@ -75,6 +75,24 @@ CASES = [
 def test_device_tree_equals_host_tree(pkg, name, make, kw):
     x, q = make()
     h, d = build_both(pkg, x, q, **kw)
+    # the pass: the device set-up leaves the bodies resident
+    h.upload()
+    h.evaluate_device()
+    d.evaluate_device()
+    ph, gh = h.download()
+    pd, gd = d.download()
+    assert np.array_equal(ph, pd) and np.array_equal(gh, gd)
+    # the host-buffer calls on the device-built plan (they fetch the
+    # set-up bodies from the device first): new charges, the adjoint
+    q2 = np.random.default_rng(45).standard_normal(len(q))
+    p2h, g2h = h.evaluate(q2)
+    p2d, g2d = d.evaluate(q2)
+    assert np.array_equal(p2h, p2d) and np.array_equal(g2h, g2d)
+    w = np.random.default_rng(46).standard_normal(len(q))
+    dqh, dxh = h.adjoint(w)
+    dqd, dxd = d.adjoint(w)
+    assert np.array_equal(dqh, dqd) and np.array_equal(dxh, dxd)
+    # the plan itself
     hi, hr = h.cells()
     di, dr = d.cells()
     assert np.array_equal(hi, di) and np.array_equal(hr, dr)
@@ -86,18 +104,6 @@ def test_device_tree_equals_host_tree(pkg, name, make, kw):
     dm = d.m2l_lists()
     assert all(np.array_equal(u, v) for u, v in zip(hm, dm))
     assert h.info() == d.info()
-    # the pass: the device set-up leaves the bodies resident
-    h.upload()
-    h.evaluate_device()
-    d.evaluate_device()
-    ph, gh = h.download()
-    pd, gd = d.download()
-    assert np.array_equal(ph, pd) and np.array_equal(gh, gd)
-    # and the host-buffer calls still work on the device-built plan
-    q2 = np.random.default_rng(45).standard_normal(len(q))
-    p2h, g2h = h.evaluate(q2)
-    p2d, g2d = d.evaluate(q2)
-    assert np.array_equal(p2h, p2d) and np.array_equal(g2h, g2d)
     st = d.setup_times()
     assert st["tree"] > 0 and st["total"] >= st["tree"]
     h.close()
