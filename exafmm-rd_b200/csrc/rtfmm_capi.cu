@@ -102,6 +102,13 @@ struct rtfmm_fmm {
   std::vector<int> body_leaf;
   std::vector<P2PItem32> items2; // P2P work items (target groups), both precisions
   std::vector<int> list_off;
+  int n_items2 = 0;               // work items (host or device built)
+  int64_t p2p_pairs = 0;          // body pairs of the P2P lists
+  // the P2P lists, offsets and items were built on the GPU (device set-up):
+  // the host vectors above are empty
+  bool p2p_on_device = false;
+  std::vector<int> h_parent, h_dfs, h_dfs_pos;  // inputs of the device build
+  DeviceWalk dwalk;                             // the GPU walk's device output
   std::vector<P2PSrc32> list32;
   std::vector<P2PSrc64> list64;
   std::vector<int> idx_pool;
@@ -288,11 +295,12 @@ bool finite_all(const double* a, int64_t n) {
 // Longest root-to-leaf path of the octree (its depth limit is 40).
 constexpr int kMaxPath = 48;
 
-// Host tables for the device pass, derived from the plan.
-void build_tables(rtfmm_fmm* f) {
+void build_pass_tables(rtfmm_fmm* f);
+
+// Host tables for the device pass, derived from the plan.  Without
+// host_p2p the P2P lists and items are left to the GPU (device_p2p_tables).
+void build_tables(rtfmm_fmm* f, bool host_p2p = true) {
   Plan& p = f->plan;
-  const Operators& o = f->ops;
-  const int ns = o.ns;
   f->leaves.clear();
   for (int c = 0; c < p.ntree; ++c) {
     const Cell& cl = p.cells[c];
@@ -328,14 +336,27 @@ void build_tables(rtfmm_fmm* f) {
   // their first body.  Each leaf's list is counted, then filled, in
   // parallel.
   const int nlf = (int)f->leaves.size();
-  std::vector<int> parent(p.ntree, -1);
+  std::vector<int>& parent = f->h_parent;
+  parent.assign(p.ntree, -1);
   for (int c = 0; c < p.ntree; ++c)
     for (int k = 0; k < p.cells[c].cnum; ++k)
       if (p.cells[c].coff + k < p.ntree) parent[p.cells[c].coff + k] = c;
-  std::vector<int> dfs(nlf), dfs_pos(nlf);
+  std::vector<int>& dfs = f->h_dfs;
+  std::vector<int>& dfs_pos = f->h_dfs_pos;
+  dfs.resize(nlf);
+  dfs_pos.resize(nlf);
   for (int l = 0; l < nlf; ++l) dfs[l] = l;
   std::sort(dfs.begin(), dfs.end(), [&](int a, int b) { return f->leaves[a].boff < f->leaves[b].boff; });
   for (int i = 0; i < nlf; ++i) dfs_pos[dfs[i]] = i;
+  f->p2p_on_device = !host_p2p;
+  if (!host_p2p) {
+    f->list_off.clear();
+    f->list32.clear();
+    f->list64.clear();
+    f->items2.clear();
+    build_pass_tables(f);
+    return;
+  }
   auto leaf_run = [&](int c, int* lo, int* hi) {
     const Cell& cl = p.cells[c];
     if (cl.bnum == 0) {  // an empty root leaf (no bodies): itself
@@ -378,7 +399,9 @@ void build_tables(rtfmm_fmm* f) {
   f->list32.assign(mixed ? f->list_off[nlf] : 0, P2PSrc32{});
   f->list64.assign(mixed ? 0 : f->list_off[nlf], P2PSrc64{});
   f->items2.assign(item_off[nlf], P2PItem32{});
-#pragma omp parallel for schedule(dynamic, 64)
+  f->n_items2 = item_off[nlf];
+  int64_t pairs = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : pairs)
   for (int l = 0; l < nlf; ++l) {
     const int c = f->leaves[l].cell;
     const Cell& T = p.cells[c];
@@ -401,6 +424,7 @@ void build_tables(rtfmm_fmm* f) {
           a.boff = f->leaves[sl].boff;
           a.bnum = f->leaves[sl].bnum;
           a.pad = 0;
+          pairs += (int64_t)f->leaves[l].bnum * a.bnum;
           if (mixed) {
             f->list32[k] = a;
           } else {
@@ -427,6 +451,16 @@ void build_tables(rtfmm_fmm* f) {
       f->items2[j] = {l, f->leaves[l].boff + t0, rem, lw};
     }
   }
+  f->p2p_pairs = pairs;
+  build_pass_tables(f);
+}
+
+// The far-field tables: batched operator applications (P2M, M2M, L2L, L2P)
+// and the FFT-M2L source/target lists.
+void build_pass_tables(rtfmm_fmm* f) {
+  Plan& p = f->plan;
+  const Operators& o = f->ops;
+  const int ns = o.ns;
 
   // batched operator applications
   f->idx_pool.clear();
@@ -750,12 +784,14 @@ int upload_plan(rtfmm_fmm* f) {
   RC(dalloc(f, &f->d_near_grad, 3 * n));
   RC(dalloc(f, &f->d_out_phi, n));
   RC(dalloc(f, &f->d_out_grad, 3 * n));
-  RC(dupload(f, &f->d_items2, f->items2));
-  RC(dupload(f, &f->d_list_off, f->list_off));
-  if (mixed)
-    RC(dupload(f, &f->d_list32, f->list32));
-  else
-    RC(dupload(f, &f->d_list64, f->list64));
+  if (!f->p2p_on_device) {  // else device_p2p_tables writes them
+    RC(dupload(f, &f->d_items2, f->items2));
+    RC(dupload(f, &f->d_list_off, f->list_off));
+    if (mixed)
+      RC(dupload(f, &f->d_list32, f->list32));
+    else
+      RC(dupload(f, &f->d_list64, f->list64));
+  }
   RC(dupload(f, &f->d_idx_pool, f->idx_pool));
   RC(dupload(f, &f->d_scale_pool, f->scale_pool));
   std::vector<int> tsrcT(f->tsrc8.size());
@@ -875,11 +911,11 @@ int enqueue_pass(rtfmm_fmm* f, bool adjoint = false, bool no_dipole = false) {
     }
     CK(cudaEventRecord(f->ev_near0, s1));
     if (mixed) {
-      CK(launch_p2p32(f->d_body32, f->d_items2, (int)f->items2.size(), f->d_list_off, f->d_list32,
+      CK(launch_p2p32(f->d_body32, f->d_items2, f->n_items2, f->d_list_off, f->d_list32,
                       f->d_near_phi, f->d_near_grad, s1));
       f->launches += 1;
     } else {
-      CK(launch_p2p64(f->d_body64, f->d_items2, (int)f->items2.size(), f->d_list_off, f->d_list64,
+      CK(launch_p2p64(f->d_body64, f->d_items2, f->n_items2, f->d_list_off, f->d_list64,
                       f->d_near_phi, f->d_near_grad, s1));
       f->launches += 1;
     }
@@ -1152,8 +1188,10 @@ int ensure_host_bodies(rtfmm_fmm* f, bool tree_order = true) {
   return RTFMM_OK;
 }
 
-// First scratch slot of the GPU walk (the tree uses the ones below).
+// Scratch slots: the device tree 0..15, the walk 16..47, the P2P tables
+// 48..63.
 constexpr int kWalkSlots = 16;
+constexpr int kTableSlots = 48;
 
 // Lists (the P2P walk on the GPU with `gpu` scratch), operators (unless
 // cached for this P, images and radius) and host tables of the plan whose
@@ -1161,16 +1199,19 @@ constexpr int kWalkSlots = 16;
 void finish_setup(rtfmm_fmm* f, const TreeScratchFn* gpu = nullptr) {
   double* st = f->setup_s;
   double t = wall_s();
+  bool device_tables = false;
   if (gpu) {
     // the P2P walk on the GPU (the host walk when it is too deep for it)
     const std::vector<WalkRoot> roots = traverse_begin(f->plan);
     std::string msg;
-    const int rc = device_p2p_walk(f->plan, roots, f->s0, *gpu, kWalkSlots, msg);
+    f->dwalk = DeviceWalk();
+    const int rc = device_p2p_walk(f->plan, roots, f->s0, *gpu, kWalkSlots, &f->dwalk, msg);
     if (rc == kTreeError) throw std::runtime_error(msg);
     if (rc == kTreeTooDeep) {
       f->plan.p2p.clear();
       traverse_p2p(f->plan, roots);
     }
+    device_tables = rc == kTreeOk && f->plan.n > 0 && f->dwalk.npairs > 0;
     traverse_finish(f->plan);
   } else {
     traverse(f->plan);
@@ -1184,8 +1225,37 @@ void finish_setup(rtfmm_fmm* f, const TreeScratchFn* gpu = nullptr) {
     st[2] = wall_s() - t;
   }
   t = wall_s();
-  build_tables(f);
+  build_tables(f, !device_tables);
   st[3] = wall_s() - t;
+}
+
+// The P2P lists, offsets and work items on the GPU from the walk's pairs,
+// into the handle's device buffers (after upload_plan).
+int device_tables(rtfmm_fmm* f, const TreeScratchFn& scratch) {
+  const int nlf = (int)f->leaves.size();
+  const int slots[3] = {kTableSlots + 8, kTableSlots + 9, kTableSlots + 10};
+  const std::vector<int>* src[3] = {&f->h_parent, &f->h_dfs, &f->h_dfs_pos};
+  int* dev[3];
+  for (int k = 0; k < 3; ++k) {
+    dev[k] = (int*)scratch(slots[k], sizeof(int) * std::max<size_t>(1, src[k]->size()));
+    if (!dev[k]) return fail(RTFMM_ENOMEM, "device allocation failed");
+    if (!src[k]->empty())
+      CK(cudaMemcpyAsync(dev[k], src[k]->data(), sizeof(int) * src[k]->size(), cudaMemcpyHostToDevice, f->s0));
+  }
+  DeviceLeafInput in{f->d_leaves, nlf, dev[0], f->d_body_leaf, dev[1], dev[2]};
+  P2PTableAlloc alloc;
+  alloc.list_off = [f](int n) { return dalloc(f, &f->d_list_off, n) ? nullptr : f->d_list_off; };
+  alloc.list32 = [f](int n) { return dalloc(f, &f->d_list32, n) ? nullptr : f->d_list32; };
+  alloc.list64 = [f](int n) { return dalloc(f, &f->d_list64, n) ? nullptr : f->d_list64; };
+  alloc.items = [f](int n) { return dalloc(f, &f->d_items2, n) ? nullptr : f->d_items2; };
+  P2PTablesOut out;
+  std::string msg;
+  const bool mixed = f->args.precision == RTFMM_FP32_MIXED;
+  if (device_p2p_tables(f->dwalk, in, mixed, f->s0, scratch, kTableSlots, alloc, &out, msg) != kTreeOk)
+    return fail(RTFMM_ECUDA, msg);
+  f->n_items2 = out.nitems;
+  f->p2p_pairs = out.pairs;
+  return RTFMM_OK;
 }
 
 void begin_setup(rtfmm_fmm* f, int64_t n) {
@@ -1243,6 +1313,11 @@ int rtfmm_b200_setup_device(rtfmm_fmm* f, int64_t n, const double* x_dev, const 
   if (rc) return rc;
   // nothing of a previous plan may still read the buffers reused below
   CK(cudaDeviceSynchronize());
+  const TreeScratchFn scratch = [f](int slot, size_t bytes) -> void* {
+    if (slot < 0 || slot >= (int)sizeof(f->tree_slots)) return nullptr;
+    char* q = nullptr;
+    return dalloc(f, &q, bytes, &f->tree_slots[slot]) ? nullptr : (void*)q;
+  };
   try {
     begin_setup(f, n);
     double t = wall_s();
@@ -1257,11 +1332,6 @@ int rtfmm_b200_setup_device(rtfmm_fmm* f, int64_t n, const double* x_dev, const 
     f->d_qin = dq;
     f->d_perm = dp;
     std::string msg;
-    TreeScratchFn scratch = [f](int slot, size_t bytes) -> void* {
-      if (slot < 0 || slot >= (int)sizeof(f->tree_slots)) return nullptr;
-      char* q = nullptr;
-      return dalloc(f, &q, bytes, &f->tree_slots[slot]) ? nullptr : (void*)q;
-    };
     const int tr = device_build_tree(x_dev, q_dev, n, f->s0, f->plan, dp, scratch, msg);
     if (tr == kTreeError) {
       f->plan = Plan();
@@ -1288,9 +1358,16 @@ int rtfmm_b200_setup_device(rtfmm_fmm* f, int64_t n, const double* x_dev, const 
     return fail(RTFMM_EINVAL, std::string("set-up failed: ") + e.what());
   }
   end_setup(f, t0);
-  // device tables, then the bodies gathered into tree order on the device
+  // device tables (the P2P ones built on the GPU), then the bodies gathered
+  // into tree order on the device
   rc = upload_plan(f);
   if (rc) return rc;
+  if (f->p2p_on_device) {
+    const double t = wall_s();
+    rc = device_tables(f, scratch);
+    if (rc) return rc;
+    f->setup_s[3] += wall_s() - t;
+  }
   if (n > 0) {
     CK(launch_gather_bodies(f->d_xin, f->d_qin, f->d_perm, (int)n, f->d_body64, f->s0));
     CK(cudaStreamSynchronize(f->s0));
@@ -1557,11 +1634,7 @@ int rtfmm_b200_setup_times(rtfmm_fmm* f, double* s, int cap) {
 int rtfmm_b200_info(rtfmm_fmm* f, int64_t* info, int cap) {
   if (!f || !info) return fail(RTFMM_EINVAL, "null argument");
   if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");
-  int64_t pairs = 0;
-  for (size_t l = 0; l < f->leaves.size(); ++l)
-    for (int e = f->list_off[l]; e < f->list_off[l + 1]; ++e)
-      pairs += (int64_t)f->leaves[l].bnum *
-               f->leaves[f->list32.empty() ? f->list64[e].leaf : f->list32[e].leaf].bnum;
+  const int64_t pairs = f->p2p_pairs;
   int64_t td = 0;
   for (int v8 : f->tsrc8) td += v8 >= 0;
   int64_t v[12] = {(int64_t)f->plan.cells.size(), (int64_t)f->leaves.size(), f->plan.dmin, f->plan.dmax,

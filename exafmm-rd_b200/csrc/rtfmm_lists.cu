@@ -145,7 +145,7 @@ struct Scratch {
   } while (0)
 
 int device_p2p_walk(Plan& plan, const std::vector<WalkRoot>& roots, cudaStream_t st, const TreeScratchFn& scratch,
-                    int slot_base, std::string& msg) {
+                    int slot_base, DeviceWalk* dw, std::string& msg) {
   const int nc = (int)plan.cells.size();
   if (nc >= (1 << kCellBits) || roots.size() > 31) return kTreeTooDeep;
   Scratch S{scratch, slot_base};
@@ -154,11 +154,11 @@ int device_p2p_walk(Plan& plan, const std::vector<WalkRoot>& roots, cudaStream_t
     S_FR0, S_HI0, S_LO0, S_FR1, S_HI1, S_LO1,
     S_NKID, S_NHIT, S_KOFF, S_HOFF, S_FLAG, S_TMP,
     S_HHI0, S_HLO0, S_HVAL0, S_HHI1, S_HLO1, S_HVAL1,
-    S_IDX0, S_IDX1, S_G0, S_G1
+    S_IDX0, S_IDX1, S_G0, S_G1, S_CB, S_CM
   };
   // cells, structure of arrays
   std::vector<double> hx(3 * (size_t)nc), hr(nc);
-  std::vector<int> hd(nc), hn(nc), ho(nc);
+  std::vector<int> hd(nc), hn(nc), ho(nc), hb(nc), hm(nc);
   for (int c = 0; c < nc; ++c) {
     const Cell& cl = plan.cells[c];
     for (int k = 0; k < 3; ++k) hx[3 * (size_t)c + k] = cl.x[k];
@@ -166,6 +166,8 @@ int device_p2p_walk(Plan& plan, const std::vector<WalkRoot>& roots, cudaStream_t
     hd[c] = cl.depth;
     hn[c] = cl.cnum;
     ho[c] = cl.coff;
+    hb[c] = cl.boff;
+    hm[c] = cl.bnum;
   }
   const int nw = (int)roots.size();
   std::vector<double> hoff(3 * nw);
@@ -186,6 +188,11 @@ int device_p2p_walk(Plan& plan, const std::vector<WalkRoot>& roots, cudaStream_t
   LCK(cudaMemcpyAsync(dcn, hn.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, st));
   LCK(cudaMemcpyAsync(dco, ho.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, st));
   LCK(cudaMemcpyAsync(doff, hoff.data(), sizeof(double) * hoff.size(), cudaMemcpyHostToDevice, st));
+  int *dcb, *dcm;
+  LCK(S.get(S_CB, &dcb, nc));
+  LCK(S.get(S_CM, &dcm, nc));
+  LCK(cudaMemcpyAsync(dcb, hb.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, st));
+  LCK(cudaMemcpyAsync(dcm, hm.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, st));
   C.cx = dcx;
   C.cr = dcr;
   C.cdepth = dcd;
@@ -318,6 +325,17 @@ int device_p2p_walk(Plan& plan, const std::vector<WalkRoot>& roots, cudaStream_t
     LCK(cub::DeviceRadixSort::SortKeys(tmp, tb, g0, g1, H, kCellBits + 5, 2 * kCellBits + 5, st));
     LCK(cudaMemcpyAsync(out.data(), g1, sizeof(unsigned long long) * H, cudaMemcpyDeviceToHost, st));
     LCK(cudaStreamSynchronize(st));
+    if (dw) {
+      dw->pairs = g1;
+      dw->npairs = H;
+    }
+  }
+  if (dw) {
+    dw->offs = doff;
+    dw->nwalk = nw;
+    dw->ncell = nc;
+    dw->cboff = dcb;
+    dw->cbnum = dcm;
   }
 
   // each target's run becomes its list
@@ -339,6 +357,197 @@ int device_p2p_walk(Plan& plan, const std::vector<WalkRoot>& roots, cudaStream_t
       L[i - a] = P2PEntry{sc, roots[w].off};
     }
   }
+  return kTreeOk;
+}
+
+
+namespace {
+
+struct LeafTables {
+  const LeafInfo* __restrict__ leaves;
+  int nlf;
+  const int* __restrict__ parent;
+  const int* __restrict__ cboff;
+  const int* __restrict__ cbnum;
+  const int* __restrict__ body_leaf;
+  const int* __restrict__ dfs;
+  const int* __restrict__ dfs_pos;
+  const int* __restrict__ cstart;
+  const int* __restrict__ cend;
+  const unsigned long long* __restrict__ pairs;
+  const double* __restrict__ offs;
+};
+
+constexpr int kMaxPathLen = 48;
+
+__global__ void k_pair_bounds(const unsigned long long* __restrict__ pairs, int H, int* __restrict__ cstart,
+                              int* __restrict__ cend) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= H) return;
+  const unsigned long long t = pairs[i] >> (kCellBits + 5);
+  if (i == 0 || (pairs[i - 1] >> (kCellBits + 5)) != t) cstart[t] = i;
+  if (i == H - 1 || (pairs[i + 1] >> (kCellBits + 5)) != t) cend[t] = i + 1;
+}
+
+// Cells from the root down to c that have pairs (ascending index).
+__device__ int leaf_path(const LeafTables& T, int c, int* path) {
+  int k = 0;
+  for (int a = c; a >= 0 && k < kMaxPathLen; a = T.parent[a])
+    if (T.cend[a] > T.cstart[a]) path[k++] = a;
+  for (int i = 0; i < k / 2; ++i) {
+    const int t = path[i];
+    path[i] = path[k - 1 - i];
+    path[k - 1 - i] = t;
+  }
+  return k;
+}
+
+// The leaves under cell c: a run of the leaves in first-body order.
+__device__ __forceinline__ void leaf_run(const LeafTables& T, int c, int* lo, int* hi) {
+  const int b0 = T.cboff[c], nb = T.cbnum[c];
+  *lo = T.dfs_pos[T.body_leaf[b0]];
+  *hi = T.dfs_pos[T.body_leaf[b0 + nb - 1]] + 1;
+}
+
+__global__ void k_leaf_list_count(LeafTables T, int* __restrict__ cnt, int* __restrict__ icnt) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= T.nlf) return;
+  int path[kMaxPathLen];
+  const int np = leaf_path(T, T.leaves[l].cell, path);
+  int c = 0;
+  for (int i = 0; i < np; ++i)
+    for (int e = T.cstart[path[i]]; e < T.cend[path[i]]; ++e) {
+      const int sc = (int)((T.pairs[e] >> 5) & ((1ull << kCellBits) - 1));
+      int lo, hi;
+      leaf_run(T, sc, &lo, &hi);
+      c += hi - lo;
+    }
+  cnt[l] = c;
+  icnt[l] = (T.leaves[l].bnum + 31) / 32;
+}
+
+__global__ void k_leaf_list_fill(LeafTables T, const int* __restrict__ off, const int* __restrict__ ioff, int mixed,
+                                 P2PSrc32* __restrict__ l32, P2PSrc64* __restrict__ l64,
+                                 P2PItem32* __restrict__ items, unsigned long long* __restrict__ pair_total) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= T.nlf) return;
+  const LeafInfo Tl = T.leaves[l];
+  int path[kMaxPathLen];
+  const int np = leaf_path(T, Tl.cell, path);
+  int k = off[l];
+  unsigned long long pairs = 0;
+  for (int i = 0; i < np; ++i)
+    for (int e = T.cstart[path[i]]; e < T.cend[path[i]]; ++e) {
+      const unsigned long long v = T.pairs[e];
+      const int sc = (int)((v >> 5) & ((1ull << kCellBits) - 1));
+      const double* o = T.offs + 3 * (int)(v & 31);
+      int lo, hi;
+      leaf_run(T, sc, &lo, &hi);
+      for (int r = lo; r < hi; ++r) {
+        const int sl = T.dfs[r];
+        const LeafInfo Sl = T.leaves[sl];
+        const int self = (Sl.cell == Tl.cell && o[0] == 0 && o[1] == 0 && o[2] == 0) ? 1 : 0;
+        if (mixed) {
+          P2PSrc32 a;
+          // the host build's expression: (c_src + offset) - c_tar in FP64, then FP32
+          a.dx = (float)(Sl.cx + o[0] - Tl.cx);
+          a.dy = (float)(Sl.cy + o[1] - Tl.cy);
+          a.dz = (float)(Sl.cz + o[2] - Tl.cz);
+          a.leaf = sl;
+          a.self = self;
+          a.boff = Sl.boff;
+          a.bnum = Sl.bnum;
+          a.pad = 0;
+          l32[k] = a;
+        } else {
+          P2PSrc64 b;
+          b.ox = o[0];
+          b.oy = o[1];
+          b.oz = o[2];
+          b.leaf = sl;
+          b.self = self;
+          b.boff = Sl.boff;
+          b.bnum = Sl.bnum;
+          l64[k] = b;
+        }
+        pairs += (unsigned long long)Tl.bnum * (unsigned long long)Sl.bnum;
+        ++k;
+      }
+    }
+  atomicAdd(pair_total, pairs);
+  // work items: 32 targets each; the last <= 16 targets of a leaf take a
+  // narrower lane group (16, 8 or 4 lanes)
+  int j = ioff[l];
+  for (int t0 = 0; t0 < Tl.bnum; t0 += 32, ++j) {
+    const int rem = min(32, Tl.bnum - t0);
+    int lw = 5;
+    while (lw > 2 && rem <= (1 << (lw - 1))) --lw;
+    items[j] = P2PItem32{l, Tl.boff + t0, rem, lw};
+  }
+}
+
+}  // namespace
+
+int device_p2p_tables(const DeviceWalk& w, const DeviceLeafInput& in, bool mixed, cudaStream_t st,
+                      const TreeScratchFn& scratch, int slot_base, const P2PTableAlloc& alloc, P2PTablesOut* out,
+                      std::string& msg) {
+  Scratch S{scratch, slot_base};
+  const int nlf = in.nlf;
+  int *cstart, *cend, *cnt, *icnt, *off, *ioff;
+  unsigned long long* total;
+  LCK(S.get(0, &cstart, w.ncell));
+  LCK(S.get(1, &cend, w.ncell));
+  LCK(S.get(2, &cnt, nlf + 1));
+  LCK(S.get(3, &icnt, nlf + 1));
+  LCK(S.get(4, &ioff, nlf + 1));
+  LCK(S.get(5, &total, 1));
+  LCK(cudaMemsetAsync(cstart, 0, sizeof(int) * w.ncell, st));
+  LCK(cudaMemsetAsync(cend, 0, sizeof(int) * w.ncell, st));
+  LCK(cudaMemsetAsync(cnt + nlf, 0, sizeof(int), st));
+  LCK(cudaMemsetAsync(icnt + nlf, 0, sizeof(int), st));
+  LCK(cudaMemsetAsync(total, 0, sizeof(unsigned long long), st));
+  if (w.npairs > 0) {
+    k_pair_bounds<<<cdiv(w.npairs, 256), 256, 0, st>>>(w.pairs, w.npairs, cstart, cend);
+    LCK(cudaGetLastError());
+  }
+  LeafTables T{in.leaves, nlf, in.parent, w.cboff, w.cbnum, in.body_leaf, in.dfs, in.dfs_pos, cstart, cend,
+               w.pairs, w.offs};
+  k_leaf_list_count<<<cdiv(nlf, 128), 128, 0, st>>>(T, cnt, icnt);
+  LCK(cudaGetLastError());
+  off = alloc.list_off(nlf + 1);
+  if (!off) {
+    msg = "device allocation of the P2P list offsets failed";
+    return kTreeError;
+  }
+  size_t tb = 0;
+  LCK(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, off, nlf + 1, st));
+  char* tmp = nullptr;
+  LCK(S.get(6, &tmp, tb));
+  LCK(cub::DeviceScan::ExclusiveSum(tmp, tb, cnt, off, nlf + 1, st));
+  LCK(cub::DeviceScan::ExclusiveSum(tmp, tb, icnt, ioff, nlf + 1, st));
+  int tot[2];
+  LCK(cudaMemcpyAsync(&tot[0], off + nlf, sizeof(int), cudaMemcpyDeviceToHost, st));
+  LCK(cudaMemcpyAsync(&tot[1], ioff + nlf, sizeof(int), cudaMemcpyDeviceToHost, st));
+  LCK(cudaStreamSynchronize(st));
+  P2PSrc32* l32 = nullptr;
+  P2PSrc64* l64 = nullptr;
+  if (mixed)
+    l32 = alloc.list32(tot[0]);
+  else
+    l64 = alloc.list64(tot[0]);
+  P2PItem32* items = alloc.items(tot[1]);
+  if ((mixed && !l32) || (!mixed && !l64) || !items) {
+    msg = "device allocation of the P2P lists failed";
+    return kTreeError;
+  }
+  k_leaf_list_fill<<<cdiv(nlf, 128), 128, 0, st>>>(T, off, ioff, mixed ? 1 : 0, l32, l64, items, total);
+  LCK(cudaGetLastError());
+  unsigned long long pairs = 0;
+  LCK(cudaMemcpyAsync(&pairs, total, sizeof(pairs), cudaMemcpyDeviceToHost, st));
+  LCK(cudaStreamSynchronize(st));
+  out->nlist = tot[0];
+  out->nitems = tot[1];
+  out->pairs = (int64_t)pairs;
   return kTreeOk;
 }
 

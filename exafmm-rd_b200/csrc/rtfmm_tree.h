@@ -7,6 +7,7 @@
 #include <string>
 #include <vector>
 
+#include "rtfmm_kernels.cuh"
 #include "rtfmm_plan.h"
 
 namespace rtfmm_b200 {
@@ -33,7 +34,47 @@ int device_build_tree(const double* x_dev, const double* q_dev, int64_t n, cudaS
 // Scratch slots slot_base .. slot_base + 27.  kTreeTooDeep: the walk is
 // deeper than 40 divisions or the tree has 2^25 cells or more (use
 // traverse_p2p).
+// What the GPU walk leaves on the device (in its scratch slots, valid until
+// they are reused): the pairs sorted by target cell, depth-first within one
+// (target << 30 | source << 5 | walk), the walks' offsets, the cells' body
+// ranges.
+struct DeviceWalk {
+  const unsigned long long* pairs = nullptr;
+  int npairs = 0;
+  const double* offs = nullptr;
+  int nwalk = 0, ncell = 0;
+  const int* cboff = nullptr;
+  const int* cbnum = nullptr;
+};
 int device_p2p_walk(Plan& plan, const std::vector<WalkRoot>& roots, cudaStream_t st, const TreeScratchFn& scratch,
-                    int slot_base, std::string& msg);
+                    int slot_base, DeviceWalk* dw, std::string& msg);
+
+// The pass's P2P tables built on the GPU from the walk's pairs: list
+// offsets by target leaf, the list entries (FP32 or FP64 form) and the work
+// items, equal to the host build's.  Inputs on the device: the leaf table,
+// the cells' parents (-1 at the root), each body's leaf, the leaves in
+// first-body order and each leaf's position in it.
+struct DeviceLeafInput {
+  const LeafInfo* leaves;
+  int nlf;
+  const int* parent;
+  const int* body_leaf;
+  const int* dfs;
+  const int* dfs_pos;
+};
+// Device buffers of the outputs, from the caller (nullptr on failure).
+struct P2PTableAlloc {
+  std::function<int*(int)> list_off;
+  std::function<P2PSrc32*(int)> list32;
+  std::function<P2PSrc64*(int)> list64;
+  std::function<P2PItem32*(int)> items;
+};
+struct P2PTablesOut {
+  int nlist = 0, nitems = 0;
+  int64_t pairs = 0;  // body pairs: sum over entries of n_target * n_source
+};
+int device_p2p_tables(const DeviceWalk& w, const DeviceLeafInput& in, bool mixed, cudaStream_t st,
+                      const TreeScratchFn& scratch, int slot_base, const P2PTableAlloc& alloc, P2PTablesOut* out,
+                      std::string& msg);
 
 }  // namespace rtfmm_b200
