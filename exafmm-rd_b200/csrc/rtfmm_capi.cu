@@ -572,8 +572,11 @@ void build_pass_tables(rtfmm_fmm* f) {
     }
   }
 
-  // FFT-M2L lists (m2l_fft_precompute_t, kernel.cpp:1153-1245)
-  std::map<int, int> s8, s27;
+  // FFT-M2L lists (m2l_fft_precompute_t, kernel.cpp:1153-1245).  Source
+  // parents are numbered in ascending cell index (s8/s27: cell -> number,
+  // -1 for none).
+  const int ncell = (int)p.cells.size();
+  std::vector<int> s8(ncell, -1), s27(ncell, -1);
   std::vector<int> t8cells, t27cells;
   for (const auto& kv : p.m2l) {
     bool single = false, normal = false;
@@ -582,24 +585,23 @@ void build_pass_tables(rtfmm_fmm* f) {
     if (single) t27cells.push_back(kv.first);
     for (const M2LEntry& e : kv.second) (e.single ? s27 : s8)[e.src] = 0;
   }
-  int k = 0;
-  for (auto& kv : s8) kv.second = k++;
-  k = 0;
-  for (auto& kv : s27) kv.second = k++;
-  f->nS8 = (int)s8.size();
-  f->nS27 = (int)s27.size();
+  int k8 = 0, k27 = 0;
+  for (int c = 0; c < ncell; ++c) {
+    if (s8[c] >= 0) s8[c] = k8++;
+    if (s27[c] >= 0) s27[c] = k27++;
+  }
+  f->nS8 = k8;
+  f->nS27 = k27;
   f->nT8 = (int)t8cells.size();
   f->nT27 = (int)t27cells.size();
   auto child_slot = [&](int ch) { return p.cells[ch].octant == 13 ? 0 : p.cells[ch].octant; };
   f->up8_slots.assign((size_t)f->nS8 * 8, -1);
   f->up27_slots.assign((size_t)f->nS27 * 8, -1);
-  for (auto& kv : s8) {
-    const Cell& cl = p.cells[kv.first];
-    for (int c = 0; c < cl.cnum; ++c) f->up8_slots[(size_t)kv.second * 8 + child_slot(cl.coff + c)] = cl.coff + c;
-  }
-  for (auto& kv : s27) {
-    const Cell& cl = p.cells[kv.first];
-    f->up27_slots[(size_t)kv.second * 8] = cl.coff;
+  for (int c0 = 0; c0 < ncell; ++c0) {
+    const Cell& cl = p.cells[c0];
+    if (s8[c0] >= 0)
+      for (int c = 0; c < cl.cnum; ++c) f->up8_slots[(size_t)s8[c0] * 8 + child_slot(cl.coff + c)] = cl.coff + c;
+    if (s27[c0] >= 0) f->up27_slots[(size_t)s27[c0] * 8] = cl.coff;
   }
   auto direction = [&](int t, const M2LEntry& e) {
     const Cell& T = p.cells[t];
@@ -610,16 +612,17 @@ void build_pass_tables(rtfmm_fmm* f) {
     return d > 13 ? d - 1 : d;
   };
   const double N3 = (double)o.N * o.N * o.N;
-  auto fill_targets = [&](const std::vector<int>& tcells, bool single, std::map<int, int>& smap,
+  auto fill_targets = [&](const std::vector<int>& tcells, bool single, const std::vector<int>& smap,
                           std::vector<int>& tsrc, std::vector<double>& tscale, std::vector<int>& down) {
     tsrc.assign(tcells.size() * 26, -1);
     tscale.assign(tcells.size(), 0.0);
     down.assign(tcells.size() * 8, -1);
+#pragma omp parallel for schedule(static)
     for (int ti = 0; ti < (int)tcells.size(); ++ti) {
       const int t = tcells[ti];
-      for (const M2LEntry& e : p.m2l[t]) {
+      for (const M2LEntry& e : p.m2l.at(t)) {
         if ((e.single != 0) != single) continue;
-        tsrc[ti * 26 + direction(t, e)] = smap[e.src];
+        tsrc[(size_t)ti * 26 + direction(t, e)] = smap[e.src];
       }
       const Cell& T = p.cells[t];
       tscale[ti] = std::pow(T.depth >= -1 ? 2.0 : 3.0, T.depth + 1) / N3;

@@ -346,6 +346,10 @@ void traverse_finish(Plan& plan) {
       coord[c][k] = (int64_t)std::llround((cl.x[k] - lo[k]) / (2 * cl.r) - 0.5);
     if (cl.cnum > 0) lattice[key(cl.depth, coord[c][0], coord[c][1], coord[c][2])] = c;
   }
+  // each parent's list is written by one thread (lists sized up front; the
+  // lattice is only read)
+  if ((int)plan.m2l.v.size() < plan.ntree) plan.m2l.v.resize(plan.ntree);
+#pragma omp parallel for schedule(dynamic, 256)
   for (int j = 0; j < plan.ntree; ++j) {
     const Cell& T = plan.cells[j];
     if (T.cnum == 0) continue;
@@ -372,7 +376,7 @@ void traverse_finish(Plan& plan) {
           (inside ? near : far).push_back({it->second, off, 0});
         }
     if (!near.empty() || !far.empty()) {
-      auto& lst = plan.m2l[j];
+      auto& lst = plan.m2l.v[(size_t)j];
       lst.insert(lst.end(), near.begin(), near.end());
       lst.insert(lst.end(), far.begin(), far.end());
     }
