@@ -15,7 +15,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "librtfmm_b200.so")
 SOURCES = ["rtfmm_plan.cpp", "rtfmm_kernels.cu", "rtfmm_capi.cu", "rtfmm_noalloc.cu", "rtfmm_ewald.cu",
-           "rtfmm_tree.cu", "rtfmm_lists.cu"]
+           "rtfmm_tree.cu", "rtfmm_lists.cu", "rtfmm_precompute.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "-Xcompiler", "-fPIC,-fopenmp,-O3", "--expt-relaxed-constexpr"]

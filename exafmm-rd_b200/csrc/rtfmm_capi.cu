@@ -21,6 +21,7 @@
 #include "../../include/rtfmm_b200.h"
 #include "rtfmm_kernels.cuh"
 #include "rtfmm_plan.h"
+#include "rtfmm_precompute.h"
 #include "rtfmm_tree.h"
 
 #ifndef M_PI
@@ -1195,6 +1196,9 @@ int ensure_host_bodies(rtfmm_fmm* f, bool tree_order = true) {
 // 48..63.
 constexpr int kWalkSlots = 16;
 constexpr int kTableSlots = 48;
+// Surface points from which a device set-up builds its operators' dense
+// parts on the GPU (P >= 10).
+constexpr int kDenseGpuMinSurf = 480;
 
 // Lists (the P2P walk on the GPU with `gpu` scratch), operators (unless
 // cached for this P, images and radius) and host tables of the plan whose
@@ -1222,7 +1226,12 @@ void finish_setup(rtfmm_fmm* f, const TreeScratchFn* gpu = nullptr) {
   st[1] = wall_s() - t;
   if (!f->ops_valid || f->ops.P != f->args.P || f->ops.images != f->args.images || f->ops.r0 != f->plan.r0) {
     t = wall_s();
-    build_operators(f->ops, f->args.P, f->plan.r0, f->args.images);
+    // with a device set-up at P >= 10, the SVD sweeps and the M2M products
+    // run on the GPU (the same tables, bit for bit); below that the host's
+    // 16-core build is as fast
+    const DenseBackend be = gpu_dense_backend(f->s0);
+    const bool dense_gpu = gpu && surface_point_num(f->args.P) >= kDenseGpuMinSurf;
+    build_operators(f->ops, f->args.P, f->plan.r0, f->args.images, dense_gpu ? &be : nullptr);
     f->ops_valid = true;
     f->ops_gen++;
     st[2] = wall_s() - t;

@@ -431,22 +431,35 @@ void traverse_finish(Plan& plan) {
 // pairs of W = A V until they are mutually orthogonal; then W = U S.  Pairs
 // follow a round-robin tournament so that each round's rotations are
 // independent and run in parallel.
-void jacobi_svd(int n, const double* A, std::vector<double>& U, std::vector<double>& s,
-                std::vector<double>& V) {
+std::vector<int> jacobi_pairs(int n) {
   const int m = n + (n & 1);
-  std::vector<double> W((size_t)m * n, 0.0), Vc((size_t)m * m, 0.0);
-  for (int j = 0; j < n; ++j)
-    for (int i = 0; i < n; ++i) W[(size_t)j * n + i] = A[(size_t)i * n + j];
-  for (int j = 0; j < m; ++j) Vc[(size_t)j * m + j] = 1.0;
-  std::vector<int> ring(m);
+  std::vector<int> ring(m), out;
   for (int i = 0; i < m; ++i) ring[i] = i;
-  for (int sweep = 0; sweep < 40; ++sweep) {
+  for (int round = 0; round < m - 1; ++round) {
+    for (int k = 0; k < m / 2; ++k) {
+      int p = ring[k], q = ring[m - 1 - k];
+      if (p > q) std::swap(p, q);
+      out.push_back(p);
+      out.push_back(q);
+    }
+    // rotate the tournament ring, keeping ring[0] fixed
+    int last = ring[m - 1];
+    for (int i = m - 1; i > 1; --i) ring[i] = ring[i - 1];
+    ring[1] = last;
+  }
+  return out;
+}
+
+void jacobi_sweeps_host(int n, std::vector<double>& W, std::vector<double>& Vc) {
+  const int m = n + (n & 1);
+  const std::vector<int> pairs = jacobi_pairs(n);
+  for (int sweep = 0; sweep < kJacobiMaxSweeps; ++sweep) {
     double off_max = 0.0;
     for (int round = 0; round < m - 1; ++round) {
+      const int* pr = &pairs[(size_t)round * m];
 #pragma omp parallel for schedule(static) reduction(max : off_max)
       for (int k = 0; k < m / 2; ++k) {
-        int p = ring[k], q = ring[m - 1 - k];
-        if (p > q) std::swap(p, q);
+        const int p = pr[2 * k], q = pr[2 * k + 1];
         if (q >= n) continue;  // padding column
         double* wp = &W[(size_t)p * n];
         double* wq = &W[(size_t)q * n];
@@ -459,7 +472,7 @@ void jacobi_svd(int n, const double* A, std::vector<double>& U, std::vector<doub
         if (alpha == 0.0 || beta == 0.0) continue;
         const double rel = std::fabs(gamma) / std::sqrt(alpha * beta);
         off_max = std::max(off_max, rel);
-        if (rel < 1e-15) continue;
+        if (rel < kJacobiTol) continue;
         const double zeta = (beta - alpha) / (2.0 * gamma);
         const double t = (zeta >= 0 ? 1.0 : -1.0) / (std::fabs(zeta) + std::sqrt(1.0 + zeta * zeta));
         const double c = 1.0 / std::sqrt(1.0 + t * t);
@@ -477,13 +490,22 @@ void jacobi_svd(int n, const double* A, std::vector<double>& U, std::vector<doub
           vq[i] = sn * a1 + c * b1;
         }
       }
-      // rotate the tournament ring, keeping ring[0] fixed
-      int last = ring[m - 1];
-      for (int i = m - 1; i > 1; --i) ring[i] = ring[i - 1];
-      ring[1] = last;
     }
-    if (off_max < 1e-15) break;
+    if (off_max < kJacobiTol) break;
   }
+}
+
+void jacobi_svd(int n, const double* A, std::vector<double>& U, std::vector<double>& s, std::vector<double>& V,
+                const DenseBackend* be) {
+  const int m = n + (n & 1);
+  std::vector<double> W((size_t)m * n, 0.0), Vc((size_t)m * m, 0.0);
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) W[(size_t)j * n + i] = A[(size_t)i * n + j];
+  for (int j = 0; j < m; ++j) Vc[(size_t)j * m + j] = 1.0;
+  if (be && be->jacobi_sweeps)
+    be->jacobi_sweeps(n, W, Vc);
+  else
+    jacobi_sweeps_host(n, W, Vc);
   std::vector<std::pair<double, int>> sv(n);
   for (int j = 0; j < n; ++j) {
     double nr = 0;
@@ -611,6 +633,7 @@ static void surface(const Operators& o, double r, const V3& c, std::vector<doubl
 // G[t][s] = 1/|x_t - y_s| (0 when coincident), get_p2p_matrix (kernel.cpp:1535-1556)
 static void p2p_matrix(int nt, const double* xt, int ns, const double* xs, std::vector<double>& G) {
   G.resize((size_t)nt * ns);
+#pragma omp parallel for schedule(static)
   for (int t = 0; t < nt; ++t)
     for (int s = 0; s < ns; ++s) {
       double d0 = xt[3 * t] - xs[3 * s], d1 = xt[3 * t + 1] - xs[3 * s + 1], d2 = xt[3 * t + 2] - xs[3 * s + 2];
@@ -619,7 +642,7 @@ static void p2p_matrix(int nt, const double* xt, int ns, const double* xs, std::
     }
 }
 
-static void matmul(int n, const double* A, const double* B, double* C) {
+void matmul_host(int n, const double* A, const double* B, double* C) {
 #pragma omp parallel for schedule(static)
   for (int i = 0; i < n; ++i) {
     double* c = C + (size_t)i * n;
@@ -638,7 +661,13 @@ static int hash_rel(int i, int j, int k) {
   return std::abs(i) * 1000 + std::abs(j) * 100 + std::abs(k) * 10 + signs;
 }
 
-void build_operators(Operators& o, int P, double r0, int images) {
+void build_operators(Operators& o, int P, double r0, int images, const DenseBackend* be) {
+  auto matmul = [be](int n, const double* A, const double* B, double* C) {
+    if (be && be->matmul)
+      be->matmul(n, A, B, C);
+    else
+      matmul_host(n, A, B, C);
+  };
   o.P = P;
   o.r0 = r0;
   o.images = images;
@@ -666,7 +695,7 @@ void build_operators(Operators& o, int P, double r0, int images) {
   surface(o, r0 * 1.05, V3{0, 0, 0}, xe);
   p2p_matrix(ns, xc.data(), ns, xe.data(), e2c);
   std::vector<double> U, s, V;
-  jacobi_svd(ns, e2c.data(), U, s, V);
+  jacobi_svd(ns, e2c.data(), U, s, V, be);
   // pseudo_inverse: drop singular values <= 4e-16 * s_max (mathfunc.cpp:154-169)
   double smax = 0;
   for (double v : s) smax = std::max(smax, std::fabs(v));
@@ -687,30 +716,52 @@ void build_operators(Operators& o, int P, double r0, int images) {
   o.pinv_down.assign((size_t)ns * ns, 0);
   for (int i = 0; i < ns; ++i)
     for (int j = 0; j < ns; ++j) o.pinv_down[(size_t)i * ns + j] = o.pinv_up[(size_t)j * ns + i];
+  // out_k = VSinv (UT G_k) for a batch of child check matrices G_k
+  auto chain = [&](std::vector<std::vector<double>>& Gs, std::vector<std::vector<double>>& outs) {
+    outs.assign(Gs.size(), std::vector<double>((size_t)ns * ns, 0.0));
+    if (be && be->chain) {
+      std::vector<const double*> g(Gs.size());
+      std::vector<double*> r(Gs.size());
+      for (size_t k = 0; k < Gs.size(); ++k) {
+        g[k] = Gs[k].data();
+        r[k] = outs[k].data();
+      }
+      be->chain(ns, o.VSinv.data(), o.UT.data(), (int)Gs.size(), g.data(), r.data());
+      return;
+    }
+    std::vector<double> m1((size_t)ns * ns);
+    for (size_t k = 0; k < Gs.size(); ++k) {
+      matmul(ns, o.UT.data(), Gs[k].data(), m1.data());
+      matmul(ns, o.VSinv.data(), m1.data(), outs[k].data());
+    }
+  };
   // M2M[octant] = VSinv (UT G_child) (kernel.cpp:1660-1668)
-  std::vector<double> G, m1((size_t)ns * ns);
-  for (int oc = 0; oc < 8; ++oc) {
-    V3 cc = child_center(V3{0, 0, 0}, r0, oc);
-    std::vector<double> xch;
-    surface(o, r0 / 2 * 1.05, cc, xch);
-    p2p_matrix(ns, xc.data(), ns, xch.data(), G);
-    matmul(ns, o.UT.data(), G.data(), m1.data());
-    o.m2m[oc].assign((size_t)ns * ns, 0);
-    matmul(ns, o.VSinv.data(), m1.data(), o.m2m[oc].data());
+  {
+    std::vector<std::vector<double>> Gs(8), outs;
+    for (int oc = 0; oc < 8; ++oc) {
+      V3 cc = child_center(V3{0, 0, 0}, r0, oc);
+      std::vector<double> xch;
+      surface(o, r0 / 2 * 1.05, cc, xch);
+      p2p_matrix(ns, xc.data(), ns, xch.data(), Gs[oc]);
+    }
+    chain(Gs, outs);
+    for (int oc = 0; oc < 8; ++oc) o.m2m[oc].swap(outs[oc]);
   }
   // image M2M over the 27 children of a 3x3x3 super-cell (kernel.cpp:1671-1683)
   o.m2m_img_sum.assign((size_t)ns * ns, 0);
   o.l2l_img.assign((size_t)ns * ns, 0);
   if (images > 0) {
-    std::vector<double> mi((size_t)ns * ns);
+    std::vector<std::vector<double>> Gs(27), outs;
     for (int oc = 0; oc < 27; ++oc) {
       int kk = oc / 9 - 1, jj = (oc % 9) / 3 - 1, ii = oc % 3 - 1;
       V3 cc{ii * (r0 * 2 / 3.0), jj * (r0 * 2 / 3.0), kk * (r0 * 2 / 3.0)};
       std::vector<double> xch;
       surface(o, r0 / 3 * 1.05, cc, xch);
-      p2p_matrix(ns, xc.data(), ns, xch.data(), G);
-      matmul(ns, o.UT.data(), G.data(), m1.data());
-      matmul(ns, o.VSinv.data(), m1.data(), mi.data());
+      p2p_matrix(ns, xc.data(), ns, xch.data(), Gs[oc]);
+    }
+    chain(Gs, outs);
+    for (int oc = 0; oc < 27; ++oc) {
+      const std::vector<double>& mi = outs[oc];
       for (size_t e = 0; e < mi.size(); ++e) o.m2m_img_sum[e] += mi[e];
       if (oc == 13)
         for (int i = 0; i < ns; ++i)

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <array>
+#include <functional>
 #include <cstdint>
 #include <map>
 #include <string>
@@ -144,12 +145,34 @@ void traverse_p2p(Plan& plan, const std::vector<WalkRoot>& roots);
 void traverse_finish(Plan& plan);
 
 
-// Operator tables.
-void build_operators(Operators& ops, int P, double r0, int images);
+// Dense kernels of the operator build that another backend (the GPU) may
+// run instead of the host: the Jacobi sweeps (on W, the n columns of A, and
+// Vc, m x m, column-major, m = n rounded up to even) and C = A B (n x n,
+// row-major).  A backend gives the host's results bit for bit.
+struct DenseBackend {
+  std::function<void(int n, std::vector<double>& W, std::vector<double>& Vc)> jacobi_sweeps;
+  std::function<void(int n, const double* A, const double* B, double* C)> matmul;
+  // out[k] = A (B G[k]) for k < nG, each product as matmul
+  std::function<void(int n, const double* A, const double* B, int nG, const double* const* G, double* const* out)>
+      chain;
+};
 
-// Dense helpers.
-void jacobi_svd(int n, const double* A, std::vector<double>& U, std::vector<double>& s,
-                std::vector<double>& V);
+// Operator tables.
+void build_operators(Operators& ops, int P, double r0, int images, const DenseBackend* be = nullptr);
+
+// Dense helpers.  The one-sided Jacobi SVD pairs columns by a round-robin
+// tournament: jacobi_pairs lists (p, q), p < q, for each of the m - 1
+// rounds of a sweep (m/2 pairs a round; q >= n is the padding column);
+// sweeps end when every pair's |gamma|/sqrt(alpha beta) is below kJacobiTol
+// or after kJacobiMaxSweeps.
+constexpr double kJacobiTol = 1e-15;
+constexpr int kJacobiMaxSweeps = 40;
+std::vector<int> jacobi_pairs(int n);
+void jacobi_sweeps_host(int n, std::vector<double>& W, std::vector<double>& Vc);
+void jacobi_svd(int n, const double* A, std::vector<double>& U, std::vector<double>& s, std::vector<double>& V,
+                const DenseBackend* be = nullptr);
+// C = A B, each C[i][j] summed over k in order (multiply, then add)
+void matmul_host(int n, const double* A, const double* B, double* C);
 void dft3_r2c(int N, const double* in, double* out);  // out: N*N*(N/2+1) complex
 
 inline int surface_point_num(int p) { return 6 * (p - 1) * (p - 1) + 2; }

@@ -165,3 +165,27 @@ def test_resetup_reuses_buffers(pkg, precision):
         g.close()
         assert np.array_equal(phi, rphi) and np.array_equal(grad, rgrad), step
     f.close()
+
+
+@pytest.mark.parametrize("P,images", [(4, 2), (8, 3), (10, 3), (12, 1)])
+def test_gpu_operators_equal_host(pkg, P, images):
+    """A device set-up at P >= 10 builds its operators with the SVD sweeps
+    and the M2M products on the GPU (below that on the host); either way the
+    tables equal the host set-up's bit for bit."""
+    x, q = uniform01(500, 70 + P)
+    a = pkg.Argument(P=P, ncrit=32, images=images, cycle=1.0, x=(0.5, 0.5, 0.5), dipole_correction=0)
+    h = pkg.LaplaceFMM(x, q, a)
+    h.setup()
+    d = pkg.LaplaceFMM(x, q, a)
+    xd = torch.from_numpy(x).cuda()
+    qd = torch.from_numpy(q).cuda()
+    d.setup_device(xd.data_ptr(), qd.data_ptr(), len(q))
+    assert d.setup_times()["operators"] > 0
+    ns = 6 * (P - 1) ** 2 + 2
+    N = 2 * P - 1
+    nf = N * N * (N // 2 + 1)
+    for which, size in [(0, ns * ns), (1, 8 * ns * ns), (2, ns * ns), (3, 26 * 64 * nf * 2), (4, ns * ns),
+                        (5, ns * ns)]:
+        assert np.array_equal(h.operator(which, size), d.operator(which, size)), which
+    h.close()
+    d.close()
