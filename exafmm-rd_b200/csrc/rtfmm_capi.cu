@@ -288,9 +288,10 @@ double wall_s() {
 }
 
 bool finite_all(const double* a, int64_t n) {
-  for (int64_t i = 0; i < n; ++i)
-    if (!std::isfinite(a[i])) return false;
-  return true;
+  int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad) if (n > (1 << 16))
+  for (int64_t i = 0; i < n; ++i) bad |= !std::isfinite(a[i]);
+  return !bad;
 }
 
 // Longest root-to-leaf path of the octree (its depth limit is 40).
@@ -1471,7 +1472,6 @@ int rtfmm_b200_evaluate(rtfmm_fmm* f, const double* q, double* phi, double* grad
   if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");
   const int64_t n = f->plan.n;
   if (n == 0) return RTFMM_OK;
-  if (q && !finite_all(q, n)) return fail(RTFMM_EINVAL, "non-finite charge");
   if (!f->device_ready) {
     int rc = upload_plan(f);
     if (rc) return rc;
@@ -1480,8 +1480,14 @@ int rtfmm_b200_evaluate(rtfmm_fmm* f, const double* q, double* phi, double* grad
   int rc0 = ensure_host_bodies(f);
   if (rc0) return rc0;
   // host -> device (input order), then into tree order on the device; the
-  // positions move only on the first call after set-up
+  // positions move only on the first call after set-up.  The charges are
+  // checked on the host while they are copied; nothing reads d_qin before
+  // the check passes.
   CK(cudaMemcpyAsync(f->d_qin, q ? q : f->q_in.data(), sizeof(double) * n, cudaMemcpyHostToDevice, f->s0));
+  if (q && !finite_all(q, n)) {
+    CK(cudaStreamSynchronize(f->s0));
+    return fail(RTFMM_EINVAL, "non-finite charge");
+  }
   if (f->pos_on_device) {
     CK(launch_set_charges(f->d_body64, f->d_qin, f->d_perm, (int)n, f->s0));
   } else {

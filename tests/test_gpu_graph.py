@@ -65,3 +65,19 @@ def test_graph_replay_equals_direct_launches(pkg, precision, dipole):
     assert np.array_equal(p4g2, p4d) and np.array_equal(g4g2, g4d)
     for f in (g, d, g4, d4):
         f.close()
+
+
+def test_non_finite_charges_leave_the_handle_usable(pkg):
+    """A non-finite charge is refused (checked while the charges are copied)
+    and the next call with valid charges gives the same outputs as before."""
+    x, q = uniform01(8000, 35)
+    f = pkg.LaplaceFMM(x, q, args(pkg, 1, pkg.STAGE_ALL))
+    p0, g0 = f.solve()
+    bad = q.copy()
+    bad[123] = np.nan
+    with pytest.raises(pkg.RtfmmError) as e:
+        f.evaluate(bad)
+    assert e.value.code == 1
+    p1, g1 = f.evaluate(q)
+    assert np.array_equal(p0, p1) and np.array_equal(g0, g1)
+    f.close()
