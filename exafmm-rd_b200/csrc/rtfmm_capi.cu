@@ -1010,7 +1010,7 @@ int enqueue_pass(rtfmm_fmm* f, bool adjoint = false, bool no_dipole = false) {
   }
   const double coef = 4 * M_PI / (3 * a.cycle * a.cycle * a.cycle);
   CK(launch_post(far ? f->d_far_phi : nullptr, f->d_far_grad, near ? f->d_near_phi : nullptr, f->d_near_grad,
-                 f->d_body64, f->d_perm, n, f->d_dip, coef, dipole,
+                 f->d_body64, f->d_perm, n, f->d_dip, coef, dipole, a.x.data(),
                  a.divide_4pi ? 1.0 / (4 * M_PI) : 1.0, f->d_out_phi, f->d_out_grad, s0));
   f->launches++;
   CK(cudaEventRecord(f->ev_st[ST_POST], s0));
@@ -1125,6 +1125,7 @@ int rtfmm_b200_create(const rtfmm_args* a, rtfmm_fmm** out) {
   if (!(a->cycle > 0) || !std::isfinite(a->cycle)) return fail(RTFMM_EINVAL, "cycle must be positive and finite");
   if (a->precision != RTFMM_FP64 && a->precision != RTFMM_FP32_MIXED)
     return fail(RTFMM_EINVAL, "unknown precision");
+  if (a->dipole_correction < 0 || a->dipole_correction > 2) return fail(RTFMM_EINVAL, "dipole_correction must be 0, 1 or 2");
   if (a->stages & ~(RTFMM_STAGE_ALL | RTFMM_STAGE_SERIAL | RTFMM_STAGE_TIMED))
     return fail(RTFMM_EINVAL, "unknown stage bits");
   for (int k = 0; k < 3; ++k)

@@ -1272,33 +1272,36 @@ __global__ void __launch_bounds__(256)
 constexpr int kDipBlocks = 256;
 
 __global__ void k_dipole_partial(const double4* __restrict__ body64, int n, double* __restrict__ partial) {
-  __shared__ double s[3][256];
-  double ax = 0, ay = 0, az = 0;
+  // per block: sum of q x, q y, q z and q
+  __shared__ double s[4][256];
+  double ax = 0, ay = 0, az = 0, aq = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const double4 b = body64[i];
     ax += b.x * b.w;
     ay += b.y * b.w;
     az += b.z * b.w;
+    aq += b.w;
   }
   s[0][threadIdx.x] = ax;
   s[1][threadIdx.x] = ay;
   s[2][threadIdx.x] = az;
+  s[3][threadIdx.x] = aq;
   __syncthreads();
   for (int h = blockDim.x / 2; h > 0; h >>= 1) {
     if (threadIdx.x < h)
-      for (int k = 0; k < 3; ++k) s[k][threadIdx.x] += s[k][threadIdx.x + h];
+      for (int k = 0; k < 4; ++k) s[k][threadIdx.x] += s[k][threadIdx.x + h];
     __syncthreads();
   }
   if (threadIdx.x == 0)
-    for (int k = 0; k < 3; ++k) partial[blockIdx.x * 3 + k] = s[k][0];
+    for (int k = 0; k < 4; ++k) partial[blockIdx.x * 4 + k] = s[k][0];
 }
 
 __global__ void k_dipole_final(double* __restrict__ partial) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  double d[3] = {0, 0, 0};
+  double d[4] = {0, 0, 0, 0};
   for (int b = 0; b < kDipBlocks; ++b)
-    for (int k = 0; k < 3; ++k) d[k] += partial[b * 3 + k];
-  for (int k = 0; k < 3; ++k) partial[3 * kDipBlocks + k] = d[k];
+    for (int k = 0; k < 4; ++k) d[k] += partial[b * 4 + k];
+  for (int k = 0; k < 4; ++k) partial[4 * kDipBlocks + k] = d[k];
 }
 
 // Adjoint support.  k_swap_charges puts the weights w (input order) into the
@@ -1342,8 +1345,8 @@ __global__ void k_adj_combine(const int64_t* __restrict__ perm, const double* __
 __global__ void k_post(const double* __restrict__ phi_far, const double* __restrict__ grad_far,
                        const double* __restrict__ phi_near, const double* __restrict__ grad_near,
                        const double4* __restrict__ body64, const int64_t* __restrict__ perm, int n,
-                       const double* __restrict__ dip, double coef, int dipole, double out_scale,
-                       double* __restrict__ out_phi, double* __restrict__ out_grad) {
+                       const double* __restrict__ dip, double coef, int dipole, double cx, double cy, double cz,
+                       double out_scale, double* __restrict__ out_phi, double* __restrict__ out_grad) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double p = 0, g0 = 0, g1 = 0, g2 = 0;
@@ -1360,9 +1363,19 @@ __global__ void k_post(const double* __restrict__ phi_far, const double* __restr
     g2 += grad_near[3 * i + 2];
   }
   if (dipole) {
-    const double dx = dip[0], dy = dip[1], dz = dip[2];
-    const double dnorm = dx * dx + dy * dy + dz * dz;
-    p -= coef * dnorm / n / body64[i].w;
+    // mu = sum q (x - centre): the reference's dipole, whose box is centred
+    // at the origin (argument.cpp:61-62)
+    const double Q = dip[3];
+    const double dx = dip[0] - Q * cx, dy = dip[1] - Q * cy, dz = dip[2] - Q * cz;
+    if (dipole == 1) {
+      // the reference's per-body form coef |mu|^2 / (N q_i) (kernel.cpp:1593)
+      const double dnorm = dx * dx + dy * dy + dz * dz;
+      p -= coef * dnorm / n / body64[i].w;
+    } else {
+      // the potential of the surface term: coef mu . (x_i - centre)
+      const double4 b = body64[i];
+      p -= coef * (dx * (b.x - cx) + dy * (b.y - cy) + dz * (b.z - cz));
+    }
     g0 -= coef * dx;
     g1 -= coef * dy;
     g2 -= coef * dz;
@@ -1601,12 +1614,12 @@ cudaError_t launch_adj_combine(const int64_t* perm, const double* w, const doubl
 
 cudaError_t launch_post(const double* phi_far, const double* grad_far, const double* phi_near,
                         const double* grad_near, const double4* body64, const int64_t* perm, int n,
-                        const double* dipole_partial, double coef, int dipole, double out_scale,
-                        double* out_phi, double* out_grad, cudaStream_t st) {
+                        const double* dipole_partial, double coef, int dipole, const double* centre,
+                        double out_scale, double* out_phi, double* out_grad, cudaStream_t st) {
   if (n > 0)
     k_post<<<cdiv(n, 256), 256, 0, st>>>(phi_far, grad_far, phi_near, grad_near, body64, perm, n,
-                                          dipole_partial + 3 * kDipBlocks, coef, dipole, out_scale, out_phi,
-                                          out_grad);
+                                          dipole_partial + 4 * kDipBlocks, coef, dipole, centre[0], centre[1],
+                                          centre[2], out_scale, out_phi, out_grad);
   return cudaGetLastError();
 }
 

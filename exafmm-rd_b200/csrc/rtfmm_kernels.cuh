@@ -95,7 +95,9 @@ cudaError_t launch_m2l_down(const T* Pk, const int* items, const double* tscale,
 cudaError_t launch_l2p_eval(const double4* body64, const LeafInfo* leaves, int nleaf,
                             const double* surf_unit, int ns, const double* q_down, double* phi,
                             double* grad, cudaStream_t st, int newton = 2);
-cudaError_t launch_dipole(const double4* body64, int n, double* partial /*>= 4*1024*/, cudaStream_t st);
+// sums of q x, q y, q z and q into partial[4 * 256 .. 4 * 256 + 3] (partial
+// holds 4 * 256 + 4 doubles)
+cudaError_t launch_dipole(const double4* body64, int n, double* partial, cudaStream_t st);
 // adjoint: weights into the tree-order bodies (charges kept in qsave), the
 // charges back, and dL/dx = w grad(phi_q) + q grad(psi_w) in input order
 cudaError_t launch_swap_charges(double4* body64, const double* w, const int64_t* perm, int n, double* qsave,
@@ -105,10 +107,12 @@ cudaError_t launch_restore_charges(double4* body64, const double* qsave, int n, 
 cudaError_t launch_set_charges(double4* body64, const double* q, const int64_t* perm, int n, cudaStream_t st);
 cudaError_t launch_adj_combine(const int64_t* perm, const double* w, const double* qsave, const double* grad_q,
                                const double* grad_w, int n, double* dLdx, cudaStream_t st);
+// dipole: 0 none, 1 the reference's per-body form, 2 the surface term's
+// potential; centre: the box centre (3), the dipole's origin
 cudaError_t launch_post(const double* phi_far, const double* grad_far, const double* phi_near,
                         const double* grad_near, const double4* body64, const int64_t* perm, int n,
-                        const double* dipole_partial, double coef, int dipole, double out_scale,
-                        double* out_phi, double* out_grad, cudaStream_t st);
+                        const double* dipole_partial, double coef, int dipole, const double* centre,
+                        double out_scale, double* out_phi, double* out_grad, cudaStream_t st);
 cudaError_t launch_gather_bodies(const double* x_in, const double* q_in, const int64_t* perm, int n,
                                  double4* body64, cudaStream_t st);
 

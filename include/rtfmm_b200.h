@@ -70,7 +70,12 @@ typedef struct rtfmm_args {
   int images;             /* periodic image levels (0 = free space)               */
   double cycle;           /* period / root cell edge                              */
   double x[3];            /* root cell centre                                     */
-  int dipole_correction;  /* reference's dipole correction (kernel.cpp:1580-1596) */
+  int dipole_correction;  /* 0 none; 1 the reference's dipole correction
+                             (kernel.cpp:1580-1596): grad -= c mu, phi_i -=
+                             c |mu|^2 / (N q_i); 2 the same gradient with the
+                             surface term's potential phi_i -= c mu.(x_i - x).
+                             mu = sum q (x - x) about the centre x,
+                             c = 4 pi / (3 cycle^3)                          */
   int divide_4pi;         /* scale outputs by 1/(4 pi)                            */
   int precision;          /* rtfmm_precision                                      */
   unsigned stages;        /* RTFMM_STAGE_* mask; 0 means RTFMM_STAGE_ALL          */

@@ -638,14 +638,22 @@ class FMM:
                 self.grad[b0:b0 + nb] -= np.einsum("ts,tsk->tk", (ir ** 3) * q[s0:s0 + ns][None, :], d)
 
     def dipole_correction_(self):
-        """``dipole_correction`` (``kernel.cpp:1580-1596``), bodies in tree order."""
+        """``dipole_correction`` (``kernel.cpp:1580-1596``), bodies in tree order.
+        The dipole is taken about the box centre (the reference's box is
+        centred at the origin, ``argument.cpp:61-62``).  Mode 1 is the
+        reference's per-body form coef |mu|^2 / (N q_i); mode 2 (not in the
+        reference) subtracts the surface term's potential coef mu . (x_i - c),
+        which has the same energy sum q_i phi_i and the same gradient."""
         n = len(self.q)
         coef = 4 * math.pi / (3 * self.cycle ** 3)
         dip = np.zeros(3)
         for i in range(n):
-            dip += self.x[i] * self.q[i]
-        dnorm = float(dip @ dip)
-        self.phi -= coef * dnorm / n / self.q
+            dip += (self.x[i] - self.center) * self.q[i]
+        if self.dipole_correction == 2:
+            self.phi -= coef * ((self.x - self.center) @ dip)
+        else:
+            dnorm = float(dip @ dip)
+            self.phi -= coef * dnorm / n / self.q
         self.grad -= coef * dip[None, :]
 
     def solve(self, stages="all"):

@@ -109,6 +109,39 @@ def test_dipole_correction_and_raw_scale(pkg, oracle):
     check(phi, grad, rphi, rgrad, 0, 2)
 
 
+@pytest.mark.parametrize("dipole", [1, 2])
+def test_dipole_modes_non_neutral(pkg, oracle, dipole):
+    """Both dipole modes with a net charge and the box centred at (0.5, 0.5,
+    0.5): the dipole is taken about the centre, as the reference's box is
+    centred at the origin."""
+    x, q = uniform01(2500, 6)
+    q = q + 0.3  # net charge
+    phi, grad, rphi, rgrad = run_both(pkg, oracle, x, q, 6, 32, 2, 0, dipole=dipole, div4pi=1)
+    assert l2(grad, rgrad) < 1e-9
+    assert l2(phi - phi.mean(), rphi - rphi.mean()) < 1e-8
+
+
+def test_physical_dipole_mode_matches_ewald_potential(pkg):
+    """Mode 2 (the surface term's potential coef mu.(x_i - c)) turns the FMM
+    potential into the converged Ewald (tin-foil) potential up to a constant;
+    the gradient of modes 1 and 2 is the same."""
+    x, q = uniform01(20000, 7)
+    t = np.random.default_rng(8).choice(len(q), 300, replace=False)
+    ephi, egrad = pkg.ewald_sampled(x, q, 1.0, t, ksize=11)
+    out = {}
+    for mode in (1, 2):
+        a = pkg.Argument(P=8, ncrit=64, images=3, cycle=1.0, x=(0.5, 0.5, 0.5), dipole_correction=mode,
+                         divide_4pi=0, precision=0)
+        f = pkg.LaplaceFMM(x, q, a)
+        out[mode] = f.solve()
+        f.close()
+    phi2, grad2 = out[2]
+    assert np.array_equal(out[1][1], grad2)
+    d = phi2[t] - ephi
+    assert np.linalg.norm(d - d.mean()) / np.linalg.norm(ephi - ephi.mean()) < 1e-4
+    assert l2(grad2[t], egrad) < 1e-4
+
+
 def test_single_leaf_and_empty(pkg, oracle):
     x, q = uniform01(40, 9)
     phi, grad, rphi, rgrad = run_both(pkg, oracle, x, q, 4, 64, 2, 0)

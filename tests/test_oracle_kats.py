@@ -111,3 +111,19 @@ def test_oracle_rock_salt_madelung(oracle):
     pm = phi - phi.mean()
     assert np.linalg.norm(pm + M * q / a) / np.linalg.norm(M * q / a) < 1e-6
     assert np.abs(grad).max() * a * a / M < 1e-6
+
+
+def test_dipole_modes_share_energy_and_gradient(oracle):
+    """Mode 2 (the surface term's potential) and the reference's mode 1 give
+    the same gradient and the same energy sum q_i phi_i, with a net charge
+    and an off-origin centre."""
+    rng = np.random.default_rng(1)
+    x = rng.random((400, 3))
+    q = rng.random(400) * 2 - 1 + 0.2
+    out = {}
+    for m in (1, 2):
+        F = oracle.FMM(x, q, 4, 32, 2, 1.0, center=(0.5, 0.5, 0.5), dipole_correction=m, divide_4pi=0)
+        out[m] = F.solve()
+    assert np.array_equal(out[1][1], out[2][1])
+    e1, e2 = float(q @ out[1][0]), float(q @ out[2][0])
+    assert abs(e1 - e2) <= 1e-12 * abs(e1)
