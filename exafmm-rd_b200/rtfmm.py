@@ -165,7 +165,8 @@ class Argument:
         a.P, a.ncrit, a.images, a.cycle = self.P, self.ncrit, self.images, self.cycle
         for k in range(3):
             a.x[k] = self.x[k]
-        a.dipole_correction = int(bool(self.dipole_correction))
+        # 0 / 1 as the reference's flag; 2 the surface term's potential
+        a.dipole_correction = int(self.dipole_correction) if self.dipole_correction in (0, 1, 2) else 1
         a.divide_4pi = int(bool(self.divide_4pi))
         a.precision = self.precision
         a.stages = self.stages
