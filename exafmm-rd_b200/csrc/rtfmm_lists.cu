@@ -199,7 +199,7 @@ int device_p2p_walk(Plan& plan, const std::vector<WalkRoot>& roots, cudaStream_t
   C.ccnum = dcn;
   C.ccoff = dco;
 
-  // round 0: the root frames, path = walk index
+  // the first frontier: the root frames, path = walk index
   std::vector<int4> hfr(nw);
   std::vector<unsigned long long> hhi(nw), hlo(nw, 0);
   for (int w = 0; w < nw; ++w) {
