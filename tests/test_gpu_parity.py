@@ -147,6 +147,7 @@ def test_physical_dipole_mode_matches_ewald_potential(pkg):
     assert e2 < 1e-3 and e2 < e0 / 10, (e2, e0)
     assert l2(out[2][1][t], egrad) < 1e-4
 
+
 def test_single_leaf_and_empty(pkg, oracle):
     x, q = uniform01(40, 9)
     phi, grad, rphi, rgrad = run_both(pkg, oracle, x, q, 4, 64, 2, 0)
