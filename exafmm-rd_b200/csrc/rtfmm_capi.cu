@@ -848,7 +848,7 @@ int upload_plan(rtfmm_fmm* f) {
   RC(dupload(f, &f->d_tsrc27, f->tsrc27));
   RC(dupload(f, &f->d_tscale8, f->tscale8));
   RC(dupload(f, &f->d_tscale27, f->tscale27));
-  RC(dalloc(f, &f->d_dip, 3 * 256 + 3));
+  RC(dalloc(f, &f->d_dip, kDipoleScratch));
 #undef RC
   if (f->h_xin_cap < (size_t)std::max<int64_t>(1, 3 * n)) {
     if (f->h_xin) cudaFreeHost(f->h_xin);

@@ -1269,7 +1269,7 @@ __global__ void __launch_bounds__(256)
 // post: far + near, dipole correction (kernel.cpp:1580-1596), 1/(4 pi)
 // (body.cpp:88-96), and the scatter back to input order (body.cpp:177-190).
 // ---------------------------------------------------------------------------
-constexpr int kDipBlocks = 256;
+constexpr int kDipBlocks = kDipoleBlocks;
 
 __global__ void k_dipole_partial(const double4* __restrict__ body64, int n, double* __restrict__ partial) {
   // per block: sum of q x, q y, q z and q

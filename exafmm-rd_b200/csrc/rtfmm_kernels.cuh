@@ -95,8 +95,10 @@ cudaError_t launch_m2l_down(const T* Pk, const int* items, const double* tscale,
 cudaError_t launch_l2p_eval(const double4* body64, const LeafInfo* leaves, int nleaf,
                             const double* surf_unit, int ns, const double* q_down, double* phi,
                             double* grad, cudaStream_t st, int newton = 2);
-// sums of q x, q y, q z and q into partial[4 * 256 .. 4 * 256 + 3] (partial
-// holds 4 * 256 + 4 doubles)
+// sums of q x, q y, q z and q into partial[4 * kDipoleBlocks + 0..3]; partial
+// holds kDipoleScratch doubles (per-block sums, then the totals)
+constexpr int kDipoleBlocks = 256;
+constexpr int kDipoleScratch = 4 * kDipoleBlocks + 4;
 cudaError_t launch_dipole(const double4* body64, int n, double* partial, cudaStream_t st);
 // adjoint: weights into the tree-order bodies (charges kept in qsave), the
 // charges back, and dL/dx = w grad(phi_q) + q grad(psi_w) in input order

@@ -8,7 +8,8 @@ lists, and the same pass outputs.  Cases: uniform bodies, clustered bodies
 with a deep adaptive tree, a lattice whose sites fall exactly on cell
 centres (the split compares with a strict >), leaves larger than a block,
 a tree deeper than the 21 levels of the device keys (built on the host),
-no bodies at all, and non-finite input.
+walks deep enough to need both words of the path keys, the C3 workload at
+full size, no bodies at all, and non-finite input.
 """
 import numpy as np
 import pytest
@@ -68,6 +69,9 @@ CASES = [
     ("lattice", lambda: lattice(24), dict(P=4, ncrit=20, images=3, precision=0)),
     ("big_leaves", lambda: uniform01(20000, 43), dict(P=4, ncrit=1000, images=0, precision=1)),
     ("deeper_than_keys", lambda: deep_pair(44), dict(P=4, ncrit=4, images=2, precision=0)),
+    # tight clusters and tiny leaves: walks of more than 19 divisions (the
+    # second word of the path keys)
+    ("deep_walk", lambda: blobs(60000, 3, 0.0005, 47), dict(P=4, ncrit=4, images=1, precision=1)),
 ]
 
 
@@ -187,5 +191,22 @@ def test_gpu_operators_equal_host(pkg, P, images):
     for which, size in [(0, ns * ns), (1, 8 * ns * ns), (2, ns * ns), (3, 26 * 64 * nf * 2), (4, ns * ns),
                         (5, ns * ns)]:
         assert np.array_equal(h.operator(which, size), d.operator(which, size)), which
+    h.close()
+    d.close()
+
+
+def test_device_setup_at_c3_size(pkg):
+    """The 2^22-body blob workload (P=10, ncrit=128, images=3): the device
+    set-up's tree, permutation, lists and list sizes equal the host's."""
+    x, q = blobs(1 << 22, 64, 0.02, 3)
+    h, d = build_both(pkg, x, q, P=10, ncrit=128, images=3, precision=1)
+    hi, hr = h.cells()
+    di, dr = d.cells()
+    assert np.array_equal(hi, di) and np.array_equal(hr, dr)
+    assert np.array_equal(h.perm(), d.perm())
+    hp, ho = h.p2p_lists()
+    dp, do = d.p2p_lists()
+    assert np.array_equal(hp, dp) and np.array_equal(ho, do)
+    assert h.info() == d.info()
     h.close()
     d.close()
