@@ -39,7 +39,7 @@ EXPORTS = (
     "rtfmm_b200_launch_count",
     "rtfmm_b200_flush_l2", "rtfmm_b200_setup_times", "rtfmm_b200_info", "rtfmm_b200_get_cells", "rtfmm_b200_get_perm",
     "rtfmm_b200_get_p2p", "rtfmm_b200_get_m2l", "rtfmm_b200_get_cell_vectors", "rtfmm_b200_get_operator",
-    "rtfmm_b200_last_error", "rtfmm_b200_version", "rtfmm_b200_p2m_noalloc",
+    "rtfmm_b200_last_error", "rtfmm_b200_version", "rtfmm_b200_clear_operator_cache", "rtfmm_b200_p2m_noalloc",
     "rtfmm_b200_ewald_sampled", "rtfmm_b200_direct_sampled",
 )
 
@@ -97,6 +97,7 @@ def lib():
         "rtfmm_b200_flush_l2": (ctypes.c_int, [_vp]),
         "rtfmm_b200_info": (ctypes.c_int, [_vp, _lp, ctypes.c_int]),
         "rtfmm_b200_setup_times": (ctypes.c_int, [_vp, _dp, ctypes.c_int]),
+        "rtfmm_b200_clear_operator_cache": (None, []),
         "rtfmm_b200_get_cells": (ctypes.c_int, [_vp, _ip, _dp]),
         "rtfmm_b200_get_perm": (ctypes.c_int, [_vp, _lp]),
         "rtfmm_b200_get_p2p": (ctypes.c_int, [_vp, _ip, _dp]),
@@ -346,6 +347,12 @@ class LaplaceFMM:
 # ----------------------------------------------------------------------------
 # bodies and the comparison metric
 # ----------------------------------------------------------------------------
+def clear_operator_cache():
+    """Frees the process-wide cache of operator tables that handles with the
+    same (P, images, cycle) share; the next set-up builds its tables."""
+    lib().rtfmm_b200_clear_operator_cache()
+
+
 def drand48_stream(seed, count):
     """glibc srand48/drand48: 48-bit LCG, a = 0x5DEECE66D, c = 0xB, state
     (seed << 16) | 0x330E; returns ``count`` doubles state / 2^48."""

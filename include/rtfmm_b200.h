@@ -316,6 +316,13 @@ int rtfmm_b200_p2m_noalloc(int P, int64_t nleaf, const rtfmm_leaf* d_leaves, con
                            const double* d_U, const double* d_VSinvT, double* d_q_equiv, void* stream);
 
 /* Last error message of the calling thread ("" if none). */
+/* Handles share their operator tables through a process-wide cache keyed by
+ * (P, images, cycle): a set-up whose tables are cached copies them instead of
+ * building them (the SVD, the M2M products and the kernel spectra).  This
+ * frees the cache (up to 4 sets; about 0.1 GB each at P = 10); handles keep
+ * their own copies. */
+void rtfmm_b200_clear_operator_cache(void);
+
 const char* rtfmm_b200_last_error(void);
 
 /* Library version string. */

@@ -178,8 +178,10 @@ def test_gpu_operators_equal_host(pkg, P, images):
     tables equal the host set-up's bit for bit."""
     x, q = uniform01(500, 70 + P)
     a = pkg.Argument(P=P, ncrit=32, images=images, cycle=1.0, x=(0.5, 0.5, 0.5), dipole_correction=0)
+    pkg.clear_operator_cache()  # each handle builds its own tables
     h = pkg.LaplaceFMM(x, q, a)
     h.setup()
+    pkg.clear_operator_cache()
     d = pkg.LaplaceFMM(x, q, a)
     xd = torch.from_numpy(x).cuda()
     qd = torch.from_numpy(q).cuda()

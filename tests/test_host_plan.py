@@ -247,3 +247,28 @@ def test_svd_factors(pkg, oracle, P):
     pinv = VS @ U.T
     assert np.linalg.norm(A @ pinv @ A - A) / np.linalg.norm(A) < 1e-9
     assert np.allclose(pinv, f.operator(0, ns * ns).reshape(ns, ns), rtol=0, atol=1e-9 * np.abs(pinv).max())
+
+
+def test_operator_tables_shared_between_handles(pkg):
+    """A second handle with the same (P, images, cycle) copies the cached
+    operator tables (bit for bit) instead of building them; clearing the
+    cache makes the next set-up build them again."""
+    x, q = uniform(300, 4)
+    a = pkg.Argument(P=6, ncrit=32, images=2, cycle=1.0, x=(0.5, 0.5, 0.5))
+    pkg.clear_operator_cache()
+    f1 = pkg.LaplaceFMM(x, q, a)
+    f1.setup()
+    t1 = f1.setup_times()["operators"]
+    f2 = pkg.LaplaceFMM(x, q, a)
+    f2.setup()
+    t2 = f2.setup_times()["operators"]
+    ns = 152
+    for which, size in [(0, ns * ns), (1, 8 * ns * ns), (2, ns * ns), (4, ns * ns), (5, ns * ns)]:
+        assert np.array_equal(f1.operator(which, size), f2.operator(which, size))
+    assert t2 < t1 / 3, (t1, t2)
+    pkg.clear_operator_cache()
+    f3 = pkg.LaplaceFMM(x, q, a)
+    f3.setup()
+    assert np.array_equal(f1.operator(1, 8 * ns * ns), f3.operator(1, 8 * ns * ns))
+    for f in (f1, f2, f3):
+        f.close()
