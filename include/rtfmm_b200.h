@@ -103,7 +103,8 @@ int rtfmm_b200_destroy(rtfmm_fmm* fmm);
  * M2L lists with the periodic image cells (Traverser::traverse,
  * 3dpp/src/traverser.cpp:19-68) and the operator tables
  * (LaplaceKernel::precompute / precompute_m2l, 3dpp/src/kernel.cpp:1638-1849;
- * cached inside the handle across calls with the same P and images).
+ * kept by the handle across calls and shared with other handles of the same
+ * P, images and cycle through a process-wide cache).
  * This is LaplaceFMM::solve up to its hot block (fmm.cpp:15-49).  x is n*3
  * (x0,y0,z0,x1,...), q is n.  Touches no GPU.
  */
