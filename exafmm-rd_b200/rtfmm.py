@@ -24,7 +24,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "librtfmm_b200.so")
 
-RTFMM_OK, RTFMM_EINVAL, RTFMM_ENOMEM, RTFMM_ECUDA, RTFMM_ESTATE, RTFMM_ENOTSUP = range(6)
+RTFMM_OK, RTFMM_EINVAL, RTFMM_ENOMEM, RTFMM_ECUDA, RTFMM_ESTATE, RTFMM_ENOTSUP, RTFMM_ETIMEOUT = range(7)
 FP64, FP32_MIXED = 0, 1
 STAGE_NEAR, STAGE_FAR, STAGE_ALL, STAGE_SERIAL, STAGE_TIMED = 1, 2, 3, 4, 8
 STAGE_NAMES = ("prep", "P2M", "M2M", "M2L_up", "M2L_hadamard", "M2L_down", "L2L", "L2P", "P2P", "post")

@@ -32,7 +32,10 @@ typedef enum rtfmm_status {
   RTFMM_ENOMEM = 2,   /* host or device allocation failed                   */
   RTFMM_ECUDA = 3,    /* a CUDA runtime call or kernel launch failed         */
   RTFMM_ESTATE = 4,   /* call out of order (e.g. evaluate before setup)      */
-  RTFMM_ENOTSUP = 5   /* option not supported by this build                  */
+  RTFMM_ENOTSUP = 5,  /* option not supported by this build                  */
+  RTFMM_ETIMEOUT = 6  /* reserved for a bounded wait that gave up; no call of
+                         this build returns it (no kernel waits on another
+                         block, stream or GPU)                                */
 } rtfmm_status;
 
 /* Arithmetic of the evaluation pass. */
