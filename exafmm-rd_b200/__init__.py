@@ -12,8 +12,8 @@ directory name is not a Python identifier, so load it by path:
     pkg = importlib.util.module_from_spec(spec); spec.loader.exec_module(pkg)
 """
 from .rtfmm import (FP32_MIXED, FP64, STAGE_ALL, STAGE_FAR, STAGE_NAMES, STAGE_NEAR, STAGE_SERIAL, STAGE_TIMED,
-                    Argument, LaplaceFMM, RtfmmError, clear_operator_cache, compare, direct_sampled, ewald_sampled, generate_random_bodies, lib)
+                    Argument, LaplaceFMM, RtfmmError, clear_operator_cache, load_operators, compare, direct_sampled, ewald_sampled, generate_random_bodies, lib)
 
-__all__ = ["Argument", "LaplaceFMM", "RtfmmError", "clear_operator_cache", "compare", "direct_sampled", "ewald_sampled",
+__all__ = ["Argument", "LaplaceFMM", "RtfmmError", "clear_operator_cache", "load_operators", "compare", "direct_sampled", "ewald_sampled",
            "generate_random_bodies", "lib", "FP64",
            "FP32_MIXED", "STAGE_ALL", "STAGE_FAR", "STAGE_NEAR", "STAGE_NAMES", "STAGE_SERIAL", "STAGE_TIMED"]

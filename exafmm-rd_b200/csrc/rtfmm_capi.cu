@@ -1805,6 +1805,27 @@ void rtfmm_b200_clear_operator_cache(void) {
   g_ops_cache.clear();
 }
 
+int rtfmm_b200_save_operators(rtfmm_fmm* f, const char* path) {
+  if (!f || !path) return fail(RTFMM_EINVAL, "null argument");
+  if (!f->ops_valid) return fail(RTFMM_ESTATE, "setup has not run");
+  std::string err = save_operators(f->ops, path);
+  if (!err.empty()) return fail(RTFMM_EINVAL, err);
+  return RTFMM_OK;
+}
+
+int rtfmm_b200_load_operators(const char* path) {
+  if (!path) return fail(RTFMM_EINVAL, "null path");
+  try {
+    Operators o;
+    std::string err = load_operators(o, path);
+    if (!err.empty()) return fail(RTFMM_EINVAL, err);
+    if (!ops_lookup(o.P, o.images, o.r0)) ops_store(o);
+  } catch (const std::bad_alloc&) {
+    return fail(RTFMM_ENOMEM, "host allocation failed while loading operators");
+  }
+  return RTFMM_OK;
+}
+
 const char* rtfmm_b200_version(void) { return "rtfmm_b200 0.1 (sm_100a)"; }
 
 }  // extern "C"

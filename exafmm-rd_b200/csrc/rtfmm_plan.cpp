@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <unordered_map>
 #include <utility>
@@ -830,6 +831,101 @@ void build_operators(Operators& o, int P, double r0, int images, const DenseBack
             for (int f = 0; f < 2 * Nf; ++f) o.cc27sum[(size_t)d * Nf * 2 + f] += gk[(size_t)g * Nf * 2 + f];
           }
   }
+}
+
+// ---------------------------------------------------------------------------
+// operator tables on disk
+// ---------------------------------------------------------------------------
+namespace {
+
+const char kOpsMagic[8] = {'R', 'T', 'F', 'M', 'M', 'O', 'P', '1'};
+
+struct OpsFields {
+  // every table of an operator set, in file order, with its expected length
+  template <typename F>
+  static void each(Operators& o, F&& f) {
+    const size_t nn = (size_t)o.ns * o.ns, nf = (size_t)o.Nf;
+    f(o.pinv_up, nn);
+    f(o.pinv_down, nn);
+    f(o.UT, nn);
+    f(o.VSinv, nn);
+    f(o.U, nn);
+    f(o.V, nn);
+    f(o.sinv, (size_t)o.ns);
+    for (int k = 0; k < 8; ++k) f(o.m2m[k], nn);
+    f(o.m2m_img_sum, nn);
+    f(o.l2l_img, nn);
+    f(o.cc8, (size_t)26 * 64 * nf * 2);
+    f(o.cc27sum, (size_t)26 * nf * 2);
+    f(o.surf_unit, (size_t)o.ns * 3);
+  }
+};
+
+struct File {
+  FILE* fp;
+  explicit File(FILE* f) : fp(f) {}
+  ~File() {
+    if (fp) fclose(fp);
+  }
+};
+
+}  // namespace
+
+std::string save_operators(const Operators& ops, const std::string& path) {
+  File f(fopen(path.c_str(), "wb"));
+  if (!f.fp) return "cannot open " + path + " for writing";
+  Operators& o = const_cast<Operators&>(ops);
+  const int32_t hdr[6] = {o.P, o.images, o.ns, o.N, o.Nh, o.Nf};
+  bool ok = fwrite(kOpsMagic, 1, 8, f.fp) == 8 && fwrite(hdr, sizeof(hdr), 1, f.fp) == 1 &&
+            fwrite(&o.r0, sizeof(double), 1, f.fp) == 1;
+  OpsFields::each(o, [&](std::vector<double>& v, size_t) {
+    const uint64_t len = v.size();
+    ok = ok && fwrite(&len, sizeof(len), 1, f.fp) == 1 && (len == 0 || fwrite(v.data(), sizeof(double), len, f.fp) == len);
+  });
+  const uint64_t li = o.surf_ijk.size();
+  ok = ok && fwrite(&li, sizeof(li), 1, f.fp) == 1 &&
+       (li == 0 || fwrite(o.surf_ijk.data(), sizeof(int), li, f.fp) == li);
+  if (!ok) return "write failed: " + path;
+  return "";
+}
+
+std::string load_operators(Operators& out, const std::string& path) {
+  File f(fopen(path.c_str(), "rb"));
+  if (!f.fp) return "cannot open " + path;
+  char magic[8];
+  int32_t hdr[6];
+  Operators o;
+  if (fread(magic, 1, 8, f.fp) != 8 || std::memcmp(magic, kOpsMagic, 8) != 0) return "not an operator file: " + path;
+  if (fread(hdr, sizeof(hdr), 1, f.fp) != 1 || fread(&o.r0, sizeof(double), 1, f.fp) != 1) return "truncated header";
+  o.P = hdr[0];
+  o.images = hdr[1];
+  o.ns = hdr[2];
+  o.N = hdr[3];
+  o.Nh = hdr[4];
+  o.Nf = hdr[5];
+  if (o.P < 2 || o.P > 64 || o.images < 0 || o.ns != surface_point_num(o.P) || o.N != 2 * o.P - 1 ||
+      o.Nh != o.N / 2 + 1 || o.Nf != o.N * o.N * o.Nh || !(o.r0 > 0) || !std::isfinite(o.r0))
+    return "inconsistent header";
+  std::string err;
+  OpsFields::each(o, [&](std::vector<double>& v, size_t want) {
+    if (!err.empty()) return;
+    uint64_t len = 0;
+    if (fread(&len, sizeof(len), 1, f.fp) != 1 || len != want) {
+      err = "table size does not match P";
+      return;
+    }
+    v.resize(len);
+    if (fread(v.data(), sizeof(double), len, f.fp) != len) err = "truncated table";
+  });
+  if (!err.empty()) return err;
+  uint64_t li = 0;
+  if (fread(&li, sizeof(li), 1, f.fp) != 1 || li != (uint64_t)o.ns * 3) return "table size does not match P";
+  o.surf_ijk.resize(li);
+  if (fread(o.surf_ijk.data(), sizeof(int), li, f.fp) != li) return "truncated table";
+  char extra;
+  if (fread(&extra, 1, 1, f.fp) != 0) return "trailing data";
+  out = std::move(o);
+  return "";
 }
 
 }  // namespace rtfmm_b200

@@ -159,6 +159,10 @@ struct DenseBackend {
 
 // Operator tables.
 void build_operators(Operators& ops, int P, double r0, int images, const DenseBackend* be = nullptr);
+// The tables as a versioned binary file (native byte order) and back; ""
+// on success, else what is wrong (a load checks every size against P).
+std::string save_operators(const Operators& ops, const std::string& path);
+std::string load_operators(Operators& ops, const std::string& path);
 
 // Dense helpers.  The one-sided Jacobi SVD pairs columns by a round-robin
 // tournament: jacobi_pairs lists (p, q), p < q, for each of the m - 1

@@ -39,7 +39,8 @@ EXPORTS = (
     "rtfmm_b200_launch_count",
     "rtfmm_b200_flush_l2", "rtfmm_b200_setup_times", "rtfmm_b200_info", "rtfmm_b200_get_cells", "rtfmm_b200_get_perm",
     "rtfmm_b200_get_p2p", "rtfmm_b200_get_m2l", "rtfmm_b200_get_cell_vectors", "rtfmm_b200_get_operator",
-    "rtfmm_b200_last_error", "rtfmm_b200_version", "rtfmm_b200_clear_operator_cache", "rtfmm_b200_p2m_noalloc",
+    "rtfmm_b200_last_error", "rtfmm_b200_version", "rtfmm_b200_clear_operator_cache",
+    "rtfmm_b200_save_operators", "rtfmm_b200_load_operators", "rtfmm_b200_p2m_noalloc",
     "rtfmm_b200_ewald_sampled", "rtfmm_b200_direct_sampled",
 )
 
@@ -98,6 +99,8 @@ def lib():
         "rtfmm_b200_info": (ctypes.c_int, [_vp, _lp, ctypes.c_int]),
         "rtfmm_b200_setup_times": (ctypes.c_int, [_vp, _dp, ctypes.c_int]),
         "rtfmm_b200_clear_operator_cache": (None, []),
+        "rtfmm_b200_save_operators": (ctypes.c_int, [_vp, ctypes.c_char_p]),
+        "rtfmm_b200_load_operators": (ctypes.c_int, [ctypes.c_char_p]),
         "rtfmm_b200_get_cells": (ctypes.c_int, [_vp, _ip, _dp]),
         "rtfmm_b200_get_perm": (ctypes.c_int, [_vp, _lp]),
         "rtfmm_b200_get_p2p": (ctypes.c_int, [_vp, _ip, _dp]),
@@ -291,6 +294,10 @@ class LaplaceFMM:
         return ms.value
 
     # -- introspection ------------------------------------------------------------
+    def save_operators(self, path):
+        """Writes this handle's operator tables to `path` (after setup)."""
+        _check(lib().rtfmm_b200_save_operators(self._h, os.fsencode(path)))
+
     def setup_times(self):
         """Wall seconds of the last set-up's phases: tree, lists, operators
         (0 when cached), host tables, the setup call, and the upload of the
@@ -347,6 +354,12 @@ class LaplaceFMM:
 # ----------------------------------------------------------------------------
 # bodies and the comparison metric
 # ----------------------------------------------------------------------------
+def load_operators(path):
+    """Loads operator tables saved by LaplaceFMM.save_operators into the
+    process-wide cache (set-ups with the same P, images and cycle use them)."""
+    _check(lib().rtfmm_b200_load_operators(os.fsencode(path)))
+
+
 def clear_operator_cache():
     """Frees the process-wide cache of operator tables that handles with the
     same (P, images, cycle) share; the next set-up builds its tables."""

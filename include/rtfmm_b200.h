@@ -327,6 +327,15 @@ int rtfmm_b200_p2m_noalloc(int P, int64_t nleaf, const rtfmm_leaf* d_leaves, con
  * their own copies. */
 void rtfmm_b200_clear_operator_cache(void);
 
+/* The handle's operator tables to a file (a versioned binary image in the
+ * host's byte order; about 0.1 GB at P = 10), and a saved file back into the
+ * process-wide cache, so that set-ups with the same (P, images, cycle) skip
+ * the build (0.2-0.6 s) in a later process.  The reference recomputes the
+ * tables in every solve() (fmm.cpp:37-48).  A load checks every table's size
+ * against P and returns RTFMM_EINVAL for a file that does not match. */
+int rtfmm_b200_save_operators(rtfmm_fmm* fmm, const char* path);
+int rtfmm_b200_load_operators(const char* path);
+
 const char* rtfmm_b200_last_error(void);
 
 /* Library version string. */

@@ -254,7 +254,7 @@ def test_operator_tables_shared_between_handles(pkg):
     operator tables (bit for bit) instead of building them; clearing the
     cache makes the next set-up build them again."""
     x, q = uniform(300, 4)
-    a = pkg.Argument(P=6, ncrit=32, images=2, cycle=1.0, x=(0.5, 0.5, 0.5))
+    a = pkg.Argument(P=6, ncrit=32, images=2, cycle=1.0)
     pkg.clear_operator_cache()
     f1 = pkg.LaplaceFMM(x, q, a)
     f1.setup()
@@ -271,4 +271,42 @@ def test_operator_tables_shared_between_handles(pkg):
     f3.setup()
     assert np.array_equal(f1.operator(1, 8 * ns * ns), f3.operator(1, 8 * ns * ns))
     for f in (f1, f2, f3):
+        f.close()
+
+
+def test_operator_tables_saved_and_loaded(pkg, tmp_path):
+    """Tables written by save_operators and loaded in a (simulated) later
+    process equal the built ones bit for bit and spare the build; files that
+    do not match are refused."""
+    x, q = uniform(300, 5)
+    a = pkg.Argument(P=5, ncrit=32, images=2, cycle=1.0)
+    pkg.clear_operator_cache()
+    f1 = pkg.LaplaceFMM(x, q, a)
+    f1.setup()
+    t_build = f1.setup_times()["operators"]
+    path = str(tmp_path / "ops_p5.bin")
+    f1.save_operators(path)
+    pkg.clear_operator_cache()
+    pkg.load_operators(path)
+    f2 = pkg.LaplaceFMM(x, q, a)
+    f2.setup()
+    assert f2.setup_times()["operators"] < t_build / 3
+    ns = 6 * 4 ** 2 + 2
+    N = 9
+    nf = N * N * (N // 2 + 1)
+    for which, size in [(0, ns * ns), (1, 8 * ns * ns), (2, ns * ns), (3, 26 * 64 * nf * 2), (4, ns * ns),
+                        (5, ns * ns)]:
+        assert np.array_equal(f1.operator(which, size), f2.operator(which, size)), which
+    # malformed files
+    raw = open(path, "rb").read()
+    bad = tmp_path / "bad.bin"
+    for blob in (raw[: len(raw) // 2], b"NOTOPS!!" + raw[8:], raw + b"x"):
+        bad.write_bytes(blob)
+        with pytest.raises(pkg.RtfmmError) as e:
+            pkg.load_operators(str(bad))
+        assert e.value.code == 1
+    with pytest.raises(pkg.RtfmmError):
+        pkg.load_operators(str(tmp_path / "missing.bin"))
+    pkg.clear_operator_cache()
+    for f in (f1, f2):
         f.close()
