@@ -842,8 +842,8 @@ const char kOpsMagic[8] = {'R', 'T', 'F', 'M', 'M', 'O', 'P', '1'};
 
 struct OpsFields {
   // every table of an operator set, in file order, with its expected length
-  template <typename F>
-  static void each(Operators& o, F&& f) {
+  template <typename O, typename F>
+  static void each(O& o, F&& f) {
     const size_t nn = (size_t)o.ns * o.ns, nf = (size_t)o.Nf;
     f(o.pinv_up, nn);
     f(o.pinv_down, nn);
@@ -874,11 +874,11 @@ struct File {
 std::string save_operators(const Operators& ops, const std::string& path) {
   File f(fopen(path.c_str(), "wb"));
   if (!f.fp) return "cannot open " + path + " for writing";
-  Operators& o = const_cast<Operators&>(ops);
+  const Operators& o = ops;
   const int32_t hdr[6] = {o.P, o.images, o.ns, o.N, o.Nh, o.Nf};
   bool ok = fwrite(kOpsMagic, 1, 8, f.fp) == 8 && fwrite(hdr, sizeof(hdr), 1, f.fp) == 1 &&
             fwrite(&o.r0, sizeof(double), 1, f.fp) == 1;
-  OpsFields::each(o, [&](std::vector<double>& v, size_t) {
+  OpsFields::each(o, [&](const std::vector<double>& v, size_t) {
     const uint64_t len = v.size();
     ok = ok && fwrite(&len, sizeof(len), 1, f.fp) == 1 && (len == 0 || fwrite(v.data(), sizeof(double), len, f.fp) == len);
   });
