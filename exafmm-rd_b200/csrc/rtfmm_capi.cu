@@ -1743,6 +1743,58 @@ int rtfmm_b200_get_p2p(rtfmm_fmm* f, int32_t* ints, double* off) {
   return RTFMM_OK;
 }
 
+int rtfmm_b200_get_leaf_lists(rtfmm_fmm* f, int32_t* list_off, int32_t* src_leaf, double* off, int64_t cap) {
+  if (!f) return fail(RTFMM_EINVAL, "null handle");
+  if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");
+  const int nlf = (int)f->leaves.size();
+  const bool mixed = f->args.precision == RTFMM_FP32_MIXED;
+  std::vector<int> lo;
+  std::vector<P2PSrc32> l32;
+  std::vector<P2PSrc64> l64;
+  if (f->p2p_on_device) {  // built on the GPU: fetch them
+    lo.resize(nlf + 1);
+    CK(cudaSetDevice(f->dev));
+    CK(cudaMemcpy(lo.data(), f->d_list_off, sizeof(int) * (nlf + 1), cudaMemcpyDeviceToHost));
+    if (mixed) {
+      l32.resize(lo[nlf]);
+      if (!l32.empty())
+        CK(cudaMemcpy(l32.data(), f->d_list32, sizeof(P2PSrc32) * l32.size(), cudaMemcpyDeviceToHost));
+    } else {
+      l64.resize(lo[nlf]);
+      if (!l64.empty())
+        CK(cudaMemcpy(l64.data(), f->d_list64, sizeof(P2PSrc64) * l64.size(), cudaMemcpyDeviceToHost));
+    }
+  }
+  const std::vector<int>& L = f->p2p_on_device ? lo : f->list_off;
+  const std::vector<P2PSrc32>& A = f->p2p_on_device ? l32 : f->list32;
+  const std::vector<P2PSrc64>& B = f->p2p_on_device ? l64 : f->list64;
+  const int64_t m = L.empty() ? 0 : L[nlf];
+  for (int l = 0; l <= nlf && list_off && !L.empty(); ++l) list_off[l] = L[l];
+  if (!src_leaf && !off) return RTFMM_OK;  // a size query
+  if (cap < m) return fail(RTFMM_EINVAL, "cap smaller than the number of list entries");
+  for (int t = 0; t < nlf && m > 0; ++t) {
+    const Cell& T = f->plan.cells[f->leaves[t].cell];
+    for (int64_t e = L[t]; e < L[t + 1]; ++e) {
+      const int sl = mixed ? A[e].leaf : B[e].leaf;
+      if (src_leaf) src_leaf[e] = sl;
+      if (!off) continue;
+      if (mixed) {
+        // the FP32 form keeps c_src + offset - c_tar; the offset is a whole
+        // number of periods
+        const Cell& S = f->plan.cells[f->leaves[sl].cell];
+        const double d[3] = {A[e].dx, A[e].dy, A[e].dz};
+        for (int k = 0; k < 3; ++k)
+          off[3 * e + k] = std::nearbyint((d[k] - (S.x[k] - T.x[k])) / f->args.cycle) * f->args.cycle;
+      } else {
+        off[3 * e + 0] = B[e].ox;
+        off[3 * e + 1] = B[e].oy;
+        off[3 * e + 2] = B[e].oz;
+      }
+    }
+  }
+  return RTFMM_OK;
+}
+
 int rtfmm_b200_get_m2l(rtfmm_fmm* f, int32_t* ints, double* off) {
   if (!f) return fail(RTFMM_EINVAL, "null handle");
   if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");

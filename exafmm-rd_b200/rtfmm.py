@@ -38,7 +38,7 @@ EXPORTS = (
     "rtfmm_b200_stage_times",
     "rtfmm_b200_launch_count",
     "rtfmm_b200_flush_l2", "rtfmm_b200_setup_times", "rtfmm_b200_info", "rtfmm_b200_get_cells", "rtfmm_b200_get_perm",
-    "rtfmm_b200_get_p2p", "rtfmm_b200_get_m2l", "rtfmm_b200_get_cell_vectors", "rtfmm_b200_get_operator",
+    "rtfmm_b200_get_p2p", "rtfmm_b200_get_m2l", "rtfmm_b200_get_leaf_lists", "rtfmm_b200_get_cell_vectors", "rtfmm_b200_get_operator",
     "rtfmm_b200_last_error", "rtfmm_b200_version", "rtfmm_b200_clear_operator_cache",
     "rtfmm_b200_save_operators", "rtfmm_b200_load_operators", "rtfmm_b200_p2m_noalloc",
     "rtfmm_b200_ewald_sampled", "rtfmm_b200_direct_sampled",
@@ -107,6 +107,7 @@ def lib():
         "rtfmm_b200_get_m2l": (ctypes.c_int, [_vp, _ip, _dp]),
         "rtfmm_b200_get_cell_vectors": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
         "rtfmm_b200_get_operator": (ctypes.c_int, [_vp, ctypes.c_int, _dp, ctypes.c_int64]),
+        "rtfmm_b200_get_leaf_lists": (ctypes.c_int, [_vp, _ip, _ip, _dp, ctypes.c_int64]),
         "rtfmm_b200_last_error": (ctypes.c_char_p, []),
         "rtfmm_b200_version": (ctypes.c_char_p, []),
     }
@@ -331,6 +332,17 @@ class LaplaceFMM:
         off = np.zeros((m, 3))
         _check(lib().rtfmm_b200_get_p2p(self._h, _ptr(ints, _ip), _ptr(off)))
         return ints, off
+
+    def leaf_lists(self):
+        """The pass's P2P lists by target leaf: (list_off, src_leaf, off)."""
+        nleaf = self.info()["nleaf"]
+        lo = np.zeros(nleaf + 1, dtype=np.int32)
+        _check(lib().rtfmm_b200_get_leaf_lists(self._h, _ptr(lo, _ip), None, None, 0))
+        m = int(lo[-1])
+        src = np.zeros(max(m, 1), dtype=np.int32)
+        off = np.zeros((max(m, 1), 3))
+        _check(lib().rtfmm_b200_get_leaf_lists(self._h, _ptr(lo, _ip), _ptr(src, _ip), _ptr(off), m))
+        return lo, src[:m], off[:m]
 
     def m2l_lists(self):
         m = self.info()["n_m2l"]

@@ -257,6 +257,14 @@ int rtfmm_b200_get_perm(rtfmm_fmm* fmm, int64_t* perm);
  * off[3e..3e+2]. */
 int rtfmm_b200_get_p2p(rtfmm_fmm* fmm, int32_t* ints, double* off);
 
+/* The pass's P2P lists by target leaf, every entry leaf to leaf (a
+ * reference pair of a leaf and a non-leaf cell expanded into the leaves
+ * beneath it, in first-body order): list_off (nleaf + 1), src_leaf and the
+ * periodic offset off (3 per entry), leaves numbered in cell order.  cap is
+ * the room in src_leaf / off (list_off[nleaf] entries are written); with
+ * both null only list_off is written (a size query). */
+int rtfmm_b200_get_leaf_lists(rtfmm_fmm* fmm, int32_t* list_off, int32_t* src_leaf, double* off, int64_t cap);
+
 /* M2L parent map (Traverser::M2L_parent_map, traverser.cpp:234-282 and
  * 43-64): entry e is (target, source, is_single_parent) = ints[3e..3e+2]
  * with offset off[3e..3e+2]. */

@@ -108,6 +108,8 @@ def test_device_tree_equals_host_tree(pkg, name, make, kw):
     dm = d.m2l_lists()
     assert all(np.array_equal(u, v) for u, v in zip(hm, dm))
     assert h.info() == d.info()
+    # the pass's leaf lists, built on the host and on the GPU
+    assert all(np.array_equal(u, v) for u, v in zip(h.leaf_lists(), d.leaf_lists()))
     st = d.setup_times()
     assert st["tree"] > 0 and st["total"] >= st["tree"]
     h.close()

@@ -310,3 +310,51 @@ def test_operator_tables_saved_and_loaded(pkg, tmp_path):
     pkg.clear_operator_cache()
     for f in (f1, f2):
         f.close()
+
+
+@pytest.mark.parametrize("kind,n,ncrit,images,precision", [
+    ("uniform", 3000, 32, 2, 0), ("blobs", 4000, 8, 1, 1), ("blobs", 2500, 4, 0, 0)])
+def test_leaf_lists_expand_the_reference_lists(pkg, kind, n, ncrit, images, precision):
+    """The pass's leaf-to-leaf P2P lists are the reference's cell lists with
+    every pair of a leaf and a non-leaf cell expanded into the leaves beneath
+    it: for each target leaf, the lists of its ancestors from the root down
+    (and its own), entries in list order, each source's leaves in
+    first-body order."""
+    x, q = (uniform(n, 21) if kind == "uniform" else blobs(n, 3, 0.01, 22))
+    f = pkg.LaplaceFMM(x, q, pkg.Argument(P=4, ncrit=ncrit, images=images, cycle=1.0, precision=precision))
+    f.setup()
+    ints, reals = f.cells()
+    cnum, coff, boff, bnum = ints[:, 3], ints[:, 2], ints[:, 4], ints[:, 5]
+    ntree = int(np.sum(ints[:, 1] >= 0))
+    leaves = [c for c in range(ntree) if cnum[c] == 0]
+    leaf_index = {c: i for i, c in enumerate(leaves)}
+    parent = {}
+    for c in range(ntree):
+        for k in range(cnum[c]):
+            parent[coff[c] + k] = c
+    by_first_body = sorted(leaves, key=lambda c: boff[c])
+    pi, po = f.p2p_lists()
+    lists = {}
+    for (t, s_), o in zip(pi, po):
+        lists.setdefault(int(t), []).append((int(s_), o))
+
+    first = np.array([boff[l] for l in by_first_body])
+
+    def leaves_under(c):
+        a, b = np.searchsorted(first, [boff[c], boff[c] + bnum[c]])
+        return by_first_body[a:b]
+
+    lo, src, off = f.leaf_lists()
+    assert len(lo) == len(leaves) + 1
+    for i, c in enumerate(leaves):
+        path = [c]
+        while path[-1] in parent:
+            path.append(parent[path[-1]])
+        want = []
+        for a in reversed(path):
+            for s_, o in lists.get(a, []):
+                want += [(leaf_index[l], o) for l in leaves_under(s_)]
+        got_src = src[lo[i]:lo[i + 1]].tolist()
+        assert got_src == [w[0] for w in want], c
+        assert np.allclose(off[lo[i]:lo[i + 1]], np.array([w[1] for w in want]).reshape(-1, 3), atol=1e-12), c
+    f.close()
