@@ -358,3 +358,17 @@ def test_leaf_lists_expand_the_reference_lists(pkg, kind, n, ncrit, images, prec
         assert got_src == [w[0] for w in want], c
         assert np.allclose(off[lo[i]:lo[i + 1]], np.array([w[1] for w in want]).reshape(-1, 3), atol=1e-12), c
     f.close()
+
+
+def test_create_rejects_unknown_dipole_mode(pkg):
+    import ctypes
+    L = pkg.lib()
+    a = pkg.rtfmm._Args()
+    L.rtfmm_b200_default_args(ctypes.byref(a))
+    h = ctypes.c_void_p()
+    for mode, ok in ((0, True), (1, True), (2, True), (3, False), (-1, False)):
+        a.dipole_correction = mode
+        rc = L.rtfmm_b200_create(ctypes.byref(a), ctypes.byref(h))
+        assert (rc == 0) == ok, mode
+        if rc == 0:
+            L.rtfmm_b200_destroy(h)
