@@ -215,7 +215,7 @@ def run_ours(args):
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     torch.cuda.set_device(local)
     pkg = load_pkg()
     W = WORKLOAD
