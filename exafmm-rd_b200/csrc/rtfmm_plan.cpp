@@ -276,8 +276,43 @@ struct Walker {
       else
         walk(it.f, offs[(size_t)it.walk], outs[(size_t)i]);
     }
-    for (size_t i = 0; i < items.size(); ++i)
-      for (const auto& pr : outs[i]) p.p2p[pr.first].push_back({pr.second, offs[(size_t)items[i].walk]});
+    // Merge in item order: chunks of items count their pairs per target,
+    // the counts give each chunk its place in every target's list, and the
+    // chunks fill their places in parallel -- the lists of the sequential
+    // merge, entry for entry.
+    const int ni = (int)items.size();
+    int T = 1;
+#ifdef _OPENMP
+    T = std::max(1, std::min(omp_get_max_threads(), ni));
+#endif
+    int ncell = 0;
+    for (const auto& o : outs)
+      for (const auto& pr : o) ncell = std::max(ncell, pr.first + 1);
+    std::vector<int> cnt((size_t)T * ncell, 0);
+#pragma omp parallel for num_threads(T) schedule(static, 1) if (T > 1)
+    for (int t = 0; t < T; ++t) {
+      int* c = &cnt[(size_t)t * ncell];
+      for (int i = ni * t / T; i < ni * (t + 1) / T; ++i)
+        for (const auto& pr : outs[(size_t)i]) c[pr.first]++;
+    }
+    if ((int)p.p2p.v.size() < ncell) p.p2p.v.resize(ncell);
+#pragma omp parallel for schedule(static)
+    for (int c = 0; c < ncell; ++c) {
+      int run = (int)p.p2p.v[(size_t)c].size();
+      for (int t = 0; t < T; ++t) {
+        const int k = cnt[(size_t)t * ncell + c];
+        cnt[(size_t)t * ncell + c] = run;
+        run += k;
+      }
+      p.p2p.v[(size_t)c].resize(run);
+    }
+#pragma omp parallel for num_threads(T) schedule(static, 1) if (T > 1)
+    for (int t = 0; t < T; ++t) {
+      int* at = &cnt[(size_t)t * ncell];
+      for (int i = ni * t / T; i < ni * (t + 1) / T; ++i)
+        for (const auto& pr : outs[(size_t)i])
+          p.p2p.v[(size_t)pr.first][(size_t)at[pr.first]++] = {pr.second, offs[(size_t)items[(size_t)i].walk]};
+    }
   }
 };
 
