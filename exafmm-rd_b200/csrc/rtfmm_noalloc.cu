@@ -16,6 +16,7 @@
 // equals the pass's leaf equivalent densities.
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <mutex>
 #include <string>
 
@@ -90,6 +91,17 @@ extern "C" int rtfmm_b200_p2m_noalloc(int P, int64_t nleaf, const rtfmm_leaf* d_
   if (nleaf == 0) return RTFMM_OK;
   if (!d_leaves || !d_bodies || !d_U || !d_VSinvT || !d_q_equiv)
     return fail(RTFMM_EINVAL, "p2m_noalloc: null device pointer");
+  // the kernels read bodies as double4, copy operator rows in 16-byte pieces
+  // and store q_equiv as double2; the leaf records are read as 8-byte fields
+  auto misaligned = [](const void* p, uintptr_t a) { return (reinterpret_cast<uintptr_t>(p) & (a - 1)) != 0; };
+  if (misaligned(d_bodies, 16) || misaligned(d_U, 16) || misaligned(d_VSinvT, 16) || misaligned(d_q_equiv, 16) ||
+      misaligned(d_leaves, 8))
+    return fail(RTFMM_EINVAL,
+                "p2m_noalloc: d_bodies, d_U, d_VSinvT and d_q_equiv must be 16-byte aligned, d_leaves 8-byte");
+  // bound nleaf before any product so that the size arithmetic cannot wrap
+  if (nleaf > (int64_t)kScratchDoubles)
+    return fail(RTFMM_EINVAL,
+                "p2m_noalloc: batch too large for the fixed scratch; split the leaves into smaller batches");
   const int ns = 6 * (P - 1) * (P - 1) + 2;
   // scratch: check potentials and U^T p (nleaf*ns each), surface points
   // (3*ns), per-leaf scale (nleaf), then integer row maps (nleaf + 2 ints)
@@ -101,20 +113,29 @@ extern "C" int rtfmm_b200_p2m_noalloc(int P, int64_t nleaf, const rtfmm_leaf* d_
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
     return fail(RTFMM_ECUDA, "p2m_noalloc: no current CUDA device");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // Outside stream capture the scratch array's device address is looked up
+  // on every call (it moves when the module is loaded again after a device
+  // reset); during capture the address cached by an earlier call is used, so
+  // the first call on a device must come before any capture.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cap) != cudaSuccess)
+    return fail(RTFMM_ECUDA, "p2m_noalloc: cudaStreamIsCapturing failed");
   double* base = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch[dev]) {
-      // First call on this device: the symbol's device address, taken with
-      // this device current (the host-side name is not a device address).
+    if (cap == cudaStreamCaptureStatusNone) {
+      // the symbol's device address, taken with this device current (the
+      // host-side name is not a device address)
       void* p = nullptr;
       cudaError_t e = cudaGetSymbolAddress(&p, g_p2m_scratch);
       if (e != cudaSuccess) return fail(RTFMM_ECUDA, "p2m_noalloc: cudaGetSymbolAddress failed");
       g_scratch[dev] = static_cast<double*>(p);
+    } else if (!g_scratch[dev]) {
+      return fail(RTFMM_EINVAL, "p2m_noalloc: the first call on a device must come before any stream capture");
     }
     base = g_scratch[dev];
   }
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int nl = (int)nleaf;
   double* pcheck = base;
   double* ymid = pcheck + (size_t)nl * ns;

@@ -241,7 +241,10 @@ int rtfmm_b200_setup_times(rtfmm_fmm* fmm, double* s, int cap);
  * depth_min, depth_max, n_p2p_entries, n_m2l_parents, n_m2l_entries,
  * num_surf, P2P body pairs (sum over list entries of n_target * n_source),
  * 8x8 M2L (target, direction) pairs, 8x8 M2L source parents, 8x8 M2L
- * target parents.  Returns the number of values available (12). */
+ * target parents, and (FP32-mixed form, after its first pass on the
+ * set-up's positions; else 0) the P2P body pairs whose FP32 terms every pass
+ * replaces by FP64 ones (pairs closer than 1/8 of the larger of their
+ * leaves' half edges).  Returns the number of values available (13). */
 int rtfmm_b200_info(rtfmm_fmm* fmm, int64_t* info, int cap);
 
 /* Cells in the reference's order (Cell3, 3dpp/include/tree.h:9-47):
@@ -305,11 +308,14 @@ int rtfmm_b200_get_operator(rtfmm_fmm* fmm, int which, double* out, int64_t cap)
  *   d_q_equiv  output, nleaf x num_surf, row l for leaf l
  *   stream     cudaStream_t to run on (NULL: the default stream)
  *
- * The batch must fit the scratch: 2*nleaf*num_surf + 3*num_surf + 1.5*nleaf
- * doubles (at P=8, up to 1766 leaves); larger batches return RTFMM_EINVAL
- * and should be split.  The first call on a device looks up the scratch
- * array's device address (cudaGetSymbolAddress), so make that first call
- * before any stream capture.  Every call reuses the same scratch and
+ * d_bodies, d_U, d_VSinvT and d_q_equiv must be 16-byte aligned and
+ * d_leaves 8-byte aligned (RTFMM_EINVAL otherwise).  The batch must fit the
+ * scratch: 2*nleaf*num_surf + 3*num_surf + nleaf + ceil((nleaf + 2) / 2)
+ * doubles (at P=8, up to 1765 leaves); larger batches return RTFMM_EINVAL
+ * and should be split.  A call looks up the scratch array's device address
+ * (cudaGetSymbolAddress) unless its stream is capturing, in which case it
+ * uses the address found by an earlier call on the device: make the first
+ * call on a device before any stream capture.  Every call reuses the same scratch and
  * overwrites what it reads, so nothing carries over between calls; calls
  * that overlap on the GPU (other streams, other host threads) race on it and
  * must be serialised by the caller. */
@@ -327,7 +333,6 @@ typedef struct rtfmm_leaf {
 int rtfmm_b200_p2m_noalloc(int P, int64_t nleaf, const rtfmm_leaf* d_leaves, const double* d_bodies,
                            const double* d_U, const double* d_VSinvT, double* d_q_equiv, void* stream);
 
-/* Last error message of the calling thread ("" if none). */
 /* Handles share their operator tables through a process-wide cache keyed by
  * (P, images, cycle): a set-up whose tables are cached copies them instead of
  * building them (the SVD, the M2M products and the kernel spectra).  This
@@ -344,6 +349,7 @@ void rtfmm_b200_clear_operator_cache(void);
 int rtfmm_b200_save_operators(rtfmm_fmm* fmm, const char* path);
 int rtfmm_b200_load_operators(const char* path);
 
+/* Last error message of the calling thread ("" if none). */
 const char* rtfmm_b200_last_error(void);
 
 /* Library version string. */

@@ -27,15 +27,15 @@ def bind(pkg):
     return fn
 
 
-def test_p2m_noalloc_matches_pass(pkg):
-    import torch
-    rng = np.random.default_rng(11)
-    n, P = 4000, 6
+def setup_case(pkg, n, P, ncrit, seed):
+    """An ordinary far-field FP64 pass and what the allocation-free call
+    needs from its set-up: leaf records, tree-order bodies, U, (V S^-1)^T and
+    the pass's leaf q_equiv."""
+    rng = np.random.default_rng(seed)
     x = rng.random((n, 3))
     q = rng.random(n) * 2 - 1
     q -= q.mean()
-    # the ordinary entry point: far field only, FP64, then its leaf q_equiv
-    a = pkg.Argument(P=P, ncrit=32, images=0, cycle=1.0, x=(0.5, 0.5, 0.5), dipole_correction=0, divide_4pi=1,
+    a = pkg.Argument(P=P, ncrit=ncrit, images=0, cycle=1.0, x=(0.5, 0.5, 0.5), dipole_correction=0, divide_4pi=1,
                      precision=pkg.FP64, stages=pkg.STAGE_FAR)
     f = pkg.LaplaceFMM(x, q, a)
     f.solve()
@@ -52,32 +52,78 @@ def test_p2m_noalloc_matches_pass(pkg):
     bodies = np.ascontiguousarray(np.concatenate([x[perm], q[perm][:, None]], axis=1))
     U = f.operator(4, ns * ns).reshape(ns, ns)
     VSinvT = np.ascontiguousarray(f.operator(5, ns * ns).reshape(ns, ns).T)
-    ref = q_equiv[leaves]
+    f.close()
+    return rec, bodies, U.copy(), VSinvT, q_equiv[leaves], ns
 
-    dev = torch.device("cuda", 0)
-    d_leaves = torch.from_numpy(rec.view(np.uint8).copy()).to(dev)
-    d_bodies = torch.from_numpy(bodies).to(dev)
-    d_U = torch.from_numpy(U.copy()).to(dev)
-    d_VT = torch.from_numpy(VSinvT).to(dev)
-    stream = torch.cuda.current_stream(dev).cuda_stream
-    fn = bind(pkg)
 
-    def call(nl, out):
-        rc = fn(P, nl, d_leaves.data_ptr(), d_bodies.data_ptr(), d_U.data_ptr(), d_VT.data_ptr(),
-                out.data_ptr(), stream)
-        assert rc == 0, pkg.lib().rtfmm_b200_last_error()
-        torch.cuda.synchronize(dev)
+class Dev:
+    def __init__(self, pkg, rec, bodies, U, VSinvT):
+        import torch
+        self.torch = torch
+        self.dev = torch.device("cuda", 0)
+        self.leaves = torch.from_numpy(rec.view(np.uint8).copy()).to(self.dev)
+        self.bodies = torch.from_numpy(bodies).to(self.dev)
+        self.U = torch.from_numpy(U).to(self.dev)
+        self.VT = torch.from_numpy(VSinvT).to(self.dev)
+        self.stream = torch.cuda.current_stream(self.dev).cuda_stream
+        self.fn = bind(pkg)
+        self.pkg = pkg
+
+    def raw(self, P, nl, out_ptr, bodies_ptr=None):
+        return self.fn(P, nl, self.leaves.data_ptr(), bodies_ptr or self.bodies.data_ptr(), self.U.data_ptr(),
+                       self.VT.data_ptr(), out_ptr, self.stream)
+
+    def call(self, P, nl, ns):
+        out = self.torch.full((nl, ns), float("nan"), dtype=self.torch.float64, device=self.dev)
+        rc = self.raw(P, nl, out.data_ptr())
+        assert rc == 0, self.pkg.lib().rtfmm_b200_last_error()
+        self.torch.cuda.synchronize(self.dev)
         return out.cpu().numpy()
 
+
+def test_p2m_noalloc_matches_pass(pkg):
+    P = 6
+    rec, bodies, U, VSinvT, ref, ns = setup_case(pkg, 4000, P, 32, 11)
+    d = Dev(pkg, rec, bodies, U, VSinvT)
     scale = np.abs(ref).max()
     # two calls in a row: all leaves, then the first half into a fresh buffer
-    out1 = call(len(leaves), torch.full((len(leaves), ns), np.nan, dtype=torch.float64, device=dev))
+    out1 = d.call(P, len(rec), ns)
     assert np.abs(out1 - ref).max() / scale < 1e-12
-    half = len(leaves) // 2
-    out2 = call(half, torch.full((half, ns), np.nan, dtype=torch.float64, device=dev))
+    half = len(rec) // 2
+    out2 = d.call(P, half, ns)
     assert np.abs(out2 - ref[:half]).max() / scale < 1e-12
 
-    # a batch larger than the fixed scratch is refused before any launch
-    rc = fn(8, 1 << 20, d_leaves.data_ptr(), d_bodies.data_ptr(), d_U.data_ptr(), d_VT.data_ptr(),
-            d_bodies.data_ptr(), stream)
+    # a batch larger than the fixed scratch is refused before any launch, and
+    # so is a count whose size arithmetic would wrap
+    for nl in (1 << 20, 1 << 62):
+        rc = d.raw(8, nl, d.bodies.data_ptr())
+        assert rc == 1 and b"scratch" in pkg.lib().rtfmm_b200_last_error()
+    # misaligned caller buffers are refused (8-byte offsets into the bodies
+    # and into an output buffer)
+    out = d.torch.zeros(len(rec) * ns + 2, dtype=d.torch.float64, device=d.dev)
+    rc = d.raw(P, len(rec), out.data_ptr(), bodies_ptr=d.bodies.data_ptr() + 8)
+    assert rc == 1 and b"aligned" in pkg.lib().rtfmm_b200_last_error()
+    rc = d.raw(P, len(rec), out.data_ptr() + 8)
+    assert rc == 1 and b"aligned" in pkg.lib().rtfmm_b200_last_error()
+    # the refusals left the output untouched
+    d.torch.cuda.synchronize(d.dev)
+    assert float(out.abs().max()) == 0.0
+
+
+def test_p2m_noalloc_largest_batch_p8(pkg):
+    """At P = 8 the scratch holds 1765 leaves: that batch runs and matches
+    the pass (the scratch used to within 159 doubles of its end), and 1766
+    leaves are refused."""
+    P = 8
+    rec, bodies, U, VSinvT, ref, ns = setup_case(pkg, 60000, P, 32, 12)
+    assert ns == 296 and len(rec) > 1766
+    d = Dev(pkg, rec, bodies, U, VSinvT)
+    scale = np.abs(ref).max()
+    out = d.call(P, 1765, ns)
+    assert np.abs(out - ref[:1765]).max() / scale < 1e-12
+    rc = d.raw(P, 1766, d.bodies.data_ptr())
     assert rc == 1 and b"scratch" in pkg.lib().rtfmm_b200_last_error()
+    # a second call in a row on the same scratch: the last 1765 leaves
+    tail = Dev(pkg, rec[-1765:].copy(), bodies, U, VSinvT)
+    out = tail.call(P, 1765, ns)
+    assert np.abs(out - ref[-1765:]).max() / scale < 1e-12
