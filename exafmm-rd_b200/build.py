@@ -34,16 +34,21 @@ def _stale():
 def build(force=False, verbose=False):
     if not force and not _stale():
         return LIB
-    objs = []
     odir = os.path.join(HERE, "_build")
     os.makedirs(odir, exist_ok=True)
-    for src in SOURCES:
-        obj = os.path.join(odir, src + ".o")
-        cmd = [NVCC] + FLAGS + ["-I", os.path.join(ROOT, "include"), "-c", os.path.join(CSRC, src), "-o", obj]
+    objs = [os.path.join(odir, src + ".o") for src in SOURCES]
+
+    def compile_one(k):
+        cmd = [NVCC] + FLAGS + ["-I", os.path.join(ROOT, "include"), "-c", os.path.join(CSRC, SOURCES[k]), "-o",
+                                objs[k]]
         if verbose:
-            print(" ".join(cmd))
+            print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-        objs.append(obj)
+
+    # the translation units are independent: compile them side by side
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 1)) as ex:
+        list(ex.map(compile_one, range(len(SOURCES))))
     tmp = LIB + ".tmp"
     cmd = [NVCC] + FLAGS + ["-shared", "-o", tmp] + objs + ["-lgomp"]
     if verbose:

@@ -3,7 +3,12 @@
 # its unmodified sources where they lie, into oracle/_ref/ (git-ignored).
 # Test infrastructure only.
 #
-#   bash oracle/build_ref.sh [/path/to/reference]
+#   bash oracle/build_ref.sh [--if-present] [/path/to/reference]
+#
+# The reference checkout is the argument, else $RTFMM_REFERENCE, else the
+# read-only mount this recipe was written against.  --if-present exits 0
+# without building when the sources are not there (a machine without the
+# reference uses a prebuilt oracle/_ref).
 #
 # Missing third-party pieces and their stand-ins:
 #   FFTW3 (not installed)  -> oracle/ref_shim/fftw3.h + fftw_shim.cpp (written here)
@@ -14,9 +19,14 @@
 # qualifiers only, so the CUDA include directory is on the path.
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF="${1:-/root/reference}/3dpp"
+IF_PRESENT=0
+if [ "${1:-}" = "--if-present" ]; then IF_PRESENT=1; shift; fi
+REF="${1:-${RTFMM_REFERENCE:-/root/reference}}/3dpp"
 OUT="$HERE/_ref"
-[ -d "$REF/src" ] || { echo "reference sources not found under $REF" >&2; exit 1; }
+if [ ! -d "$REF/src" ]; then
+  if [ "$IF_PRESENT" = 1 ]; then echo "reference sources not found under $REF; oracle/_ref not rebuilt"; exit 0; fi
+  echo "reference sources not found under $REF" >&2; exit 1
+fi
 BLAS="$(ls "$(python3 -c 'import site; print(site.getsitepackages()[0])')"/opencv_python_headless.libs/libopenblasp-*.so 2>/dev/null | head -1)"
 [ -n "$BLAS" ] || { echo "OpenBLAS shared library not found" >&2; exit 1; }
 mkdir -p "$OUT"

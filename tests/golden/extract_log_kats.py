@@ -109,7 +109,7 @@ def dedupe(runs):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("RTFMM_REFERENCE", "/root/reference")
     expdir = os.path.join(ref, "3dpp", "exp")
     runs = []
     for name in sorted(os.listdir(expdir)):
