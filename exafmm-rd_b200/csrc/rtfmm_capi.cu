@@ -193,6 +193,15 @@ struct rtfmm_fmm {
   cudaEvent_t ev_g0 = nullptr, ev_g1 = nullptr;
   // the 8x8 FFT-M2L (up, Hadamard, down) runs in FP32: the mixed form at P <= 8
   bool m2l32 = false;
+  // mixed form: the P2P pairs much closer than their leaves (tree-order
+  // target t: pairs d_close_pairs[d_close_off[t] .. d_close_off[t+1]]),
+  // found once per set of device positions, refined to FP64 every pass
+  int* d_close_cnt = nullptr;
+  int* d_close_off = nullptr;
+  int2* d_close_pairs = nullptr;
+  void* d_close_tmp = nullptr;
+  int64_t n_close = 0;
+  bool close_valid = false;
   float stage_ms[ST_N] = {};
   int64_t launches = 0;
 };
@@ -248,6 +257,8 @@ void drop_graph(rtfmm_fmm* f) {
 // use).  The buffers themselves stay in the pool.
 void drop_allocs(rtfmm_fmm* f) {
   drop_graph(f);
+  f->close_valid = false;
+  f->n_close = 0;
   f->d_adj_q = f->d_adj_gq = f->d_adj_gw = f->d_adj_w = f->d_adj_dq = f->d_adj_dx = nullptr;
   f->grad_q_valid = false;
   f->pos_on_device = false;
@@ -921,6 +932,11 @@ int enqueue_pass(rtfmm_fmm* f, bool adjoint = false, bool no_dipole = false) {
       CK(launch_p2p32(f->d_body32, f->d_items2, f->n_items2, f->d_list_off, f->d_list32,
                       f->d_near_phi, f->d_near_grad, s1));
       f->launches += 1;
+      if (f->n_close > 0) {
+        CK(launch_close_fix(f->d_body64, f->d_body32, f->d_list32, f->d_close_off, f->d_close_pairs, n,
+                            f->args.images > 0 ? f->args.cycle : 0.0, f->d_near_phi, f->d_near_grad, s1));
+        f->launches += 1;
+      }
     } else {
       CK(launch_p2p64(f->d_body64, f->d_items2, f->n_items2, f->d_list_off, f->d_list64,
                       f->d_near_phi, f->d_near_grad, s1));
@@ -1021,6 +1037,44 @@ int enqueue_pass(rtfmm_fmm* f, bool adjoint = false, bool no_dipole = false) {
   return RTFMM_OK;
 }
 
+// The mixed form's close-pair list for the positions now in d_body64 (once
+// per set of device positions, before a pass is enqueued or captured):
+// FP32 positions, per-target counts, their prefix sum, then the pairs.
+int ensure_close_pairs(rtfmm_fmm* f) {
+  if (f->args.precision != RTFMM_FP32_MIXED || f->close_valid || !(f->args.stages & RTFMM_STAGE_NEAR))
+    return RTFMM_OK;
+  const int n = (int)f->plan.n;
+  cudaStream_t s0 = f->s0;
+  f->n_close = 0;
+  if (n > 0 && f->n_items2 > 0) {
+    int rc = 0;
+    if ((rc = dalloc(f, &f->d_close_cnt, (size_t)n + 1)) || (rc = dalloc(f, &f->d_close_off, (size_t)n + 1)))
+      return rc;
+    CK(launch_prep32(f->d_body64, f->d_body_leaf, f->d_leaves, f->d_body32, n, s0));
+    CK(cudaMemsetAsync(f->d_close_cnt, 0, sizeof(int) * ((size_t)n + 1), s0));
+    CK(launch_close_count(f->d_body32, f->d_items2, f->n_items2, f->d_list_off, f->d_list32, f->d_leaves,
+                          f->d_close_cnt, s0));
+    size_t tmp_bytes = 0;
+    CK(launch_count_scan(f->d_close_cnt, f->d_close_off, n + 1, nullptr, &tmp_bytes, s0));
+    char* tmp = nullptr;
+    if ((rc = dalloc(f, &tmp, tmp_bytes, &f->d_close_tmp))) return rc;
+    f->d_close_tmp = tmp;
+    CK(launch_count_scan(f->d_close_cnt, f->d_close_off, n + 1, tmp, &tmp_bytes, s0));
+    int total = 0;
+    CK(cudaMemcpyAsync(&total, f->d_close_off + n, sizeof(int), cudaMemcpyDeviceToHost, s0));
+    CK(cudaStreamSynchronize(s0));
+    if (total > 0) {
+      if ((rc = dalloc(f, &f->d_close_pairs, (size_t)total))) return rc;
+      CK(launch_close_emit(f->d_body32, f->d_items2, f->n_items2, f->d_list_off, f->d_list32, f->d_leaves,
+                           f->d_close_off, f->d_close_pairs, s0));
+      CK(cudaStreamSynchronize(s0));
+    }
+    f->n_close = total;
+  }
+  f->close_valid = true;
+  return RTFMM_OK;
+}
+
 int collect_times(rtfmm_fmm* f, float* total) {
   CK(cudaEventSynchronize(f->ev_stop));
   float ms = 0;
@@ -1056,6 +1110,8 @@ bool use_graph(const rtfmm_fmm* f) {
 
 // Enqueues one forward pass on s0 (graph replay or direct launches).
 int launch_pass(rtfmm_fmm* f) {
+  int rc0 = ensure_close_pairs(f);
+  if (rc0) return rc0;
   if (!use_graph(f)) return enqueue_pass(f);
   if (!f->pass_graph) {
     cudaGraph_t g = nullptr;
@@ -1568,6 +1624,8 @@ int adjoint_core(rtfmm_fmm* f, const double* w, double* dq, double* dx) {
   const int n = (int)f->plan.n;
   int rc = ensure_adj_scratch(f);
   if (rc) return rc;
+  rc = ensure_close_pairs(f);
+  if (rc) return rc;
   cudaStream_t s0 = f->s0;
   const bool have_gq = f->grad_q_valid;
   if (have_gq) CK(cudaMemcpyAsync(f->d_adj_gq, f->d_out_grad, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, s0));
@@ -1685,10 +1743,11 @@ int rtfmm_b200_info(rtfmm_fmm* f, int64_t* info, int cap) {
   const int64_t pairs = f->p2p_pairs;
   int64_t td = 0;
   for (int v8 : f->tsrc8) td += v8 >= 0;
-  int64_t v[12] = {(int64_t)f->plan.cells.size(), (int64_t)f->leaves.size(), f->plan.dmin, f->plan.dmax,
-                   f->plan.n_p2p, (int64_t)f->plan.m2l.size(), f->plan.n_m2l, f->ops.ns, pairs, td, f->nS8, f->nT8};
-  for (int k = 0; k < 12 && k < cap; ++k) info[k] = v[k];
-  return 12;
+  int64_t v[13] = {(int64_t)f->plan.cells.size(), (int64_t)f->leaves.size(), f->plan.dmin, f->plan.dmax,
+                   f->plan.n_p2p, (int64_t)f->plan.m2l.size(), f->plan.n_m2l, f->ops.ns, pairs, td, f->nS8, f->nT8,
+                   f->close_valid ? f->n_close : 0};
+  for (int k = 0; k < 13 && k < cap; ++k) info[k] = v[k];
+  return 13;
 }
 
 int rtfmm_b200_get_cells(rtfmm_fmm* f, int32_t* ints, double* reals) {

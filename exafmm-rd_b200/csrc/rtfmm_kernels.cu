@@ -20,6 +20,10 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
+
+#include <cub/cub.cuh>
+
 // FP64 pair kernels: seed the reciprocal square root with the FP64 (1) or
 // FP32 (0) hardware approximation
 #ifndef RSQ_SEED64
@@ -435,6 +439,121 @@ __global__ void __launch_bounds__(32 * kP2PWarps)
     case 3: p2p64_item<4>(body64, it, list_off, list, sbuf[warp], lane, phi, grad); break;
     default: p2p64_item<8>(body64, it, list_off, list, sbuf[warp], lane, phi, grad); break;
   }
+}
+
+// ---------------------------------------------------------------------------
+// Close-pair refinement of the FP32 P2P (mixed form).
+//
+// The FP32 positions are leaf-relative, so each coordinate carries an
+// absolute rounding of about 2^-24 of the leaf size, and a pair at distance
+// d gets a relative error of about (leaf size / d) 2^-24 in its terms.  The
+// relative L2 error of the whole gradient is dominated by the few closest
+// pairs of the input (at N = 2^20 uniform bodies they sit ~1e-4 apart, a
+// leaf is ~0.05 wide).  So the pairs closer than kCloseFrac times the larger
+// of their two leaves' half edges are listed once per set-up (k_close_scan,
+// a count pass and an emit pass in list order), and every pass replaces
+// their FP32 terms by FP64 ones (k_close_fix): it recomputes the FP32 term
+// of each listed pair with the P2P kernel's exact operation sequence (same
+// FP32 inputs, same roundings, same rsqrt.approx) and adds the FP64 term
+// minus it.  What remains of the FP32 term is its rounding inside the FP32
+// partial sum, ~2^-24 of the term.
+// ---------------------------------------------------------------------------
+#ifndef CLOSE_FRAC
+#define CLOSE_FRAC 0.125f
+#endif
+constexpr float kCloseFrac = CLOSE_FRAC;
+
+// One warp per P2P work item, one lane per target (lanes >= nt idle); the
+// lanes of an item share its list, so source loads are warp broadcasts.
+// EMIT = false: cnt[t] = close sources of target t.  EMIT = true: the pairs
+// (source body, list entry) of target t at pairs[off[t] ...], in list order.
+template <bool EMIT>
+__global__ void __launch_bounds__(256)
+    k_close_scan(const float4* __restrict__ body32, const P2PItem32* __restrict__ items, int nitems,
+                 const int* __restrict__ list_off, const P2PSrc32* __restrict__ list,
+                 const LeafInfo* __restrict__ leaves, int* __restrict__ cnt, const int* __restrict__ off,
+                 int2* __restrict__ pairs) {
+  const int item = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (item >= nitems) return;
+  const P2PItem32 it = items[item];
+  if (lane >= it.nt) return;
+  const int t = it.boff + lane;
+  const float4 xt = body32[t];
+  const float rt = (float)leaves[it.leaf].r;
+  int c = 0;
+  int pos = EMIT ? off[t] : 0;
+  const int pend = EMIT ? off[t + 1] : 0;  // the count pass's total for t bounds the writes
+  const int e1 = list_off[it.leaf + 1];
+  for (int e = list_off[it.leaf]; e < e1; ++e) {
+    const P2PSrc32 s = list[e];
+    const float rc = kCloseFrac * fmaxf(rt, (float)leaves[s.leaf].r);
+    const float rc2 = rc * rc;
+    const float px = xt.x - s.dx, py = xt.y - s.dy, pz = xt.z - s.dz;
+    for (int k = 0; k < s.bnum; ++k) {
+      const float4 b = body32[s.boff + k];
+      const float dx = px - b.x, dy = py - b.y, dz = pz - b.z;
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      if (r2 < rc2 && !(s.self && s.boff + k == t)) {
+        if (EMIT) {
+          if (pos < pend) pairs[pos++] = make_int2(s.boff + k, e);
+        } else
+          ++c;
+      }
+    }
+  }
+  if (!EMIT) cnt[t] = c;
+}
+
+// One thread per target body (tree order).  cycle > 0: periodic, the pair's
+// FP64 difference taken at its nearest image (a close pair is far closer
+// than half a period, so that is the image its list entry carries).
+__global__ void k_close_fix(const double4* __restrict__ body64, const float4* __restrict__ body32,
+                            const P2PSrc32* __restrict__ list, const int* __restrict__ off,
+                            const int2* __restrict__ pairs, int n, double cycle, double* __restrict__ phi,
+                            double* __restrict__ grad) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int b0 = off[t], b1 = off[t + 1];
+  if (b0 == b1) return;
+  const float4 xt = body32[t];
+  const double4 yt = body64[t];
+  double P = 0.0, Gx = 0.0, Gy = 0.0, Gz = 0.0;
+  for (int k = b0; k < b1; ++k) {
+    const int2 pr = pairs[k];
+    const P2PSrc32 s = list[pr.y];
+    // the FP32 terms exactly as k_p2p32 formed them
+    const float4 b = body32[pr.x];
+    const float px = xt.x - s.dx, py = xt.y - s.dy, pz = xt.z - s.dz;
+    const float dx = __fadd_rn(px, -b.x), dy = __fadd_rn(py, -b.y), dz = __fadd_rn(pz, -b.z);
+    float r2 = __fmul_rn(dz, dz);
+    r2 = __fmaf_rn(dy, dy, r2);
+    r2 = __fmaf_rn(dx, dx, r2);
+    float ir = rsqrt_approx(r2);
+    if (!(r2 > 0.f)) ir = 0.f;
+    const float qir = __fmul_rn(b.w, ir);
+    const float q3 = __fmul_rn(__fmul_rn(qir, ir), ir);
+    // the FP64 terms of the pair
+    const double4 y = body64[pr.x];
+    double ex = yt.x - y.x, ey = yt.y - y.y, ez = yt.z - y.z;
+    if (cycle > 0.0) {
+      ex -= cycle * rint(ex / cycle);
+      ey -= cycle * rint(ey / cycle);
+      ez -= cycle * rint(ez / cycle);
+    }
+    const double rr = ex * ex + ey * ey + ez * ez;
+    const double jr = rr > 0.0 ? rsqrt_nr<2>(rr) : 0.0;
+    const double qjr = y.w * jr;
+    const double q3d = qjr * jr * jr;
+    P += qjr - (double)qir;
+    Gx += q3d * ex - (double)q3 * (double)dx;
+    Gy += q3d * ey - (double)q3 * (double)dy;
+    Gz += q3d * ez - (double)q3 * (double)dz;
+  }
+  phi[t] += P;
+  grad[3 * t + 0] -= Gx;
+  grad[3 * t + 1] -= Gy;
+  grad[3 * t + 2] -= Gz;
 }
 
 // ---------------------------------------------------------------------------
@@ -1420,6 +1539,33 @@ cudaError_t launch_p2p64(const double4* body64, const P2PItem32* items, int nite
   return cudaGetLastError();
 }
 
+cudaError_t launch_close_count(const float4* body32, const P2PItem32* items, int nitems, const int* list_off,
+                               const P2PSrc32* list, const LeafInfo* leaves, int* cnt, cudaStream_t st) {
+  if (nitems > 0)
+    k_close_scan<false><<<cdiv(nitems, 8), 256, 0, st>>>(body32, items, nitems, list_off, list, leaves, cnt,
+                                                         nullptr, nullptr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_close_emit(const float4* body32, const P2PItem32* items, int nitems, const int* list_off,
+                              const P2PSrc32* list, const LeafInfo* leaves, const int* off, int2* pairs,
+                              cudaStream_t st) {
+  if (nitems > 0)
+    k_close_scan<true><<<cdiv(nitems, 8), 256, 0, st>>>(body32, items, nitems, list_off, list, leaves, nullptr,
+                                                        off, pairs);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_close_fix(const double4* body64, const float4* body32, const P2PSrc32* list, const int* off,
+                             const int2* pairs, int n, double cycle, double* phi, double* grad, cudaStream_t st) {
+  if (n > 0) k_close_fix<<<cdiv(n, 256), 256, 0, st>>>(body64, body32, list, off, pairs, n, cycle, phi, grad);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_count_scan(const int* cnt, int* off, int n, void* tmp, size_t* tmp_bytes, cudaStream_t st) {
+  return cub::DeviceScan::ExclusiveSum(tmp, *tmp_bytes, cnt, off, n, st);
+}
+
 cudaError_t launch_p2m_check(const double4* body64, const LeafInfo* leaves, int nleaf,
                              const double* surf_unit, int ns, double* out, cudaStream_t st, int newton) {
   if (nleaf > 0) {
@@ -1457,15 +1603,16 @@ cudaError_t launch_apply(const ApplyBatch& b, cudaStream_t st) {
   if (b.max_rows > 0 && b.groups > 0) {
 #if APPLY_TC
     if (b.ns % 2 != 0) return cudaErrorInvalidValue;  // 16-byte copies need an even ns
-    // the shared-memory opt-in is per function and device
-    static bool attr_set[64] = {};
+    // the shared-memory opt-in is per function and device; set once per
+    // device, safely when several host threads make their first call at once
+    static std::atomic<bool> attr_set[64];
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+    if (dev < 0 || dev >= 64 || !attr_set[dev].load(std::memory_order_acquire)) {
       e = cudaFuncSetAttribute(k_apply_f64_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGSmem);
       if (e != cudaSuccess) return e;
-      if (dev >= 0 && dev < 64) attr_set[dev] = true;
+      if (dev >= 0 && dev < 64) attr_set[dev].store(true, std::memory_order_release);
     }
     dim3 grid(cdiv(b.ns, kGN), cdiv(b.max_rows, kGM), b.groups);
     k_apply_f64_tc<<<grid, kGThreads, kGSmem, st>>>(b);

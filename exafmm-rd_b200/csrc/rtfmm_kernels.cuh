@@ -63,6 +63,21 @@ cudaError_t launch_p2p32(const float4* body32, const P2PItem32* items, int nitem
                          const P2PSrc32* list, double* phi, double* grad, cudaStream_t st);
 cudaError_t launch_p2p64(const double4* body64, const P2PItem32* items, int nitems, const int* list_off,
                          const P2PSrc64* list, double* phi, double* grad, cudaStream_t st);
+// Close-pair refinement of the FP32 P2P: per-target counts of the pairs
+// closer than a fraction of their leaves (cnt[t], tree order), their list
+// (source body, list entry) at pairs[off[t]...], and the per-pass fix that
+// replaces their FP32 terms in phi / grad (P2P outputs) by FP64 ones.
+cudaError_t launch_close_count(const float4* body32, const P2PItem32* items, int nitems, const int* list_off,
+                               const P2PSrc32* list, const LeafInfo* leaves, int* cnt, cudaStream_t st);
+cudaError_t launch_close_emit(const float4* body32, const P2PItem32* items, int nitems, const int* list_off,
+                              const P2PSrc32* list, const LeafInfo* leaves, const int* off, int2* pairs,
+                              cudaStream_t st);
+// cycle > 0: periodic (nearest image); 0: free space
+cudaError_t launch_close_fix(const double4* body64, const float4* body32, const P2PSrc32* list, const int* off,
+                             const int2* pairs, int n, double cycle, double* phi, double* grad, cudaStream_t st);
+// off = exclusive prefix sum of cnt (n values); tmp == nullptr: *tmp_bytes
+// = the scratch it needs
+cudaError_t launch_count_scan(const int* cnt, int* off, int n, void* tmp, size_t* tmp_bytes, cudaStream_t st);
 // newton: Newton steps of the FP64 reciprocal square root (1: ~1e-13, for
 // the FP32-mixed form; 2: full FP64)
 cudaError_t launch_p2m_check(const double4* body64, const LeafInfo* leaves, int nleaf,

@@ -308,10 +308,10 @@ class LaplaceFMM:
         return dict(zip(("tree", "lists", "operators", "tables", "total", "upload"), v.tolist()))
 
     def info(self):
-        v = np.zeros(12, dtype=np.int64)
-        lib().rtfmm_b200_info(self._h, _ptr(v, _lp), 12)
+        v = np.zeros(13, dtype=np.int64)
+        lib().rtfmm_b200_info(self._h, _ptr(v, _lp), 13)
         keys = ("ncell", "nleaf", "depth_min", "depth_max", "n_p2p", "n_m2l_parents", "n_m2l", "num_surf",
-                "p2p_pairs", "m2l8_pairs", "m2l8_sources", "m2l8_targets")
+                "p2p_pairs", "m2l8_pairs", "m2l8_sources", "m2l8_targets", "close_pairs")
         return dict(zip(keys, v.tolist()))
 
     def cells(self):

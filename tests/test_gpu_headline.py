@@ -1,0 +1,232 @@
+"""The headline workload at full size, pinned to the reference's own output,
+and the adjoint's gradients at full size by central finite differences.
+
+C2: N = 2^20 uniform bodies (numpy default_rng(2)), P = 8, ncrit = 256,
+3 image levels, cycle 1, 1/(4 pi r), no dipole correction.  The reference's
+LaplaceFMM::solve (3dpp/src/fmm.cpp:13-81) ran on all bodies and its outputs
+at 4096 sampled bodies are the fixture tests/golden/golden_c2_sampled.npz
+(made by tests/golden/make_golden_c2.py).  Errors are the relative L2 norm
+of compare (3dpp/src/body.cpp:131-175) over the sampled bodies; periodic
+potentials are compared with the mean difference removed (rounding in the
+ill-conditioned equivalent densities leaves a near-constant shift that
+differs between any two FP64 implementations).
+
+C4: the same bodies with the hand-written adjoint, L = sum w phi with
+w ~ N(0,1) (default_rng(4)) and L = 1/2 sum q phi.  dL/dx and dL/dq are
+checked on 64 random bodies against central differences of L computed with
+the FP64 form (h = 1e-4, each perturbed body set set up again on the GPU).
+At N = 2^20 a body's nearest neighbour is ~5e-3 away, so the O(h^2)
+truncation of the central difference is ~(h/d)^2 ~ 4e-4; Richardson's
+extrapolation (4 D(h/2) - D(h)) / 3 removes it, and the gradients are
+checked against the extrapolated differences.
+"""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "golden_c2_sampled.npz")
+
+
+def c2_bodies(n=1 << 20, seed=2):
+    rng = np.random.default_rng(seed)
+    x = rng.random((n, 3))
+    q = rng.random(n) * 2 - 1
+    return x, q - q.mean()
+
+
+def c2_args(pkg, precision):
+    return pkg.Argument(P=8, ncrit=256, images=3, cycle=1.0, x=(0.5, 0.5, 0.5), dipole_correction=0,
+                        divide_4pi=1, precision=precision)
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def rel_mr(a, b):
+    d = a - b
+    return float(np.linalg.norm(d - d.mean()) / np.linalg.norm(b - b.mean()))
+
+
+@pytest.fixture(scope="module")
+def c2(pkg):
+    g = np.load(GOLDEN)
+    x, q = c2_bodies()
+    assert np.array_equal(x[:4], g["x_head"]), "bodies regenerated from the seed differ from the fixture's"
+    out = {}
+    for prec in (pkg.FP64, pkg.FP32_MIXED):
+        f = pkg.LaplaceFMM(x, q, c2_args(pkg, prec))
+        out[prec] = f.solve()
+        f.close()
+    return g, x, q, out
+
+
+def test_c2_fp64_matches_reference(pkg, c2):
+    g, _, _, out = c2
+    phi, grad = out[pkg.FP64]
+    idx = g["idx"]
+    eg = rel(grad[idx], g["grad"])
+    ep = rel_mr(phi[idx], g["phi"])
+    print("C2 FP64 vs reference: grad %.3e  phi (mean removed) %.3e" % (eg, ep))
+    assert eg < 1e-9 and ep < 1e-8, (eg, ep)
+    # whole-array sums of the reference's output
+    assert abs(np.linalg.norm(grad) / float(g["grad_norm"]) - 1) < 1e-10
+    assert abs(np.linalg.norm(phi - phi.mean()) / float(g["phi_norm_mr"]) - 1) < 1e-8
+
+
+def test_c2_mixed_within_north_star_bound(pkg, c2):
+    """The FP32-mixed form well within the 1e-5 bound of the reference
+    (sampled) and of the FP64 form (all bodies), potential and gradient
+    (measured: gradient 1.6e-7, potential 6.6e-7 against the FP64 form; the
+    potential's share is the FP32 FFT-M2L, the gradient's the FP32 P2P after
+    its closest pairs are refined in FP64)."""
+    g, _, _, out = c2
+    phi, grad = out[pkg.FP32_MIXED]
+    phi64, grad64 = out[pkg.FP64]
+    idx = g["idx"]
+    eg_ref = rel(grad[idx], g["grad"])
+    ep_ref = rel_mr(phi[idx], g["phi"])
+    eg = rel(grad, grad64)
+    ep = rel_mr(phi, phi64)
+    print("C2 mixed: vs reference grad %.3e phi %.3e; vs FP64 (all bodies) grad %.3e phi %.3e"
+          % (eg_ref, ep_ref, eg, ep))
+    assert eg_ref < 1e-6 and ep_ref < 2e-6, (eg_ref, ep_ref)
+    assert eg < 1e-6 and ep < 2e-6, (eg, ep)
+
+
+def away_from_faces(x, h, depth=8):
+    """bodies at least 3h from every cell face down to `depth` levels."""
+    ok = np.ones(len(x), bool)
+    for d in range(1, depth + 1):
+        s = x * (1 << d)
+        ok &= np.all(np.abs(s - np.round(s)) > 3 * h * (1 << d), axis=1)
+    return np.nonzero(ok)[0]
+
+
+@pytest.fixture(scope="module")
+def c4(pkg):
+    """Central differences of both losses with the FP64 form, at h and h/2,
+    for the positions and charges of 64 random bodies."""
+    import torch
+    x, q = c2_bodies()
+    n = len(q)
+    w = np.random.default_rng(4).standard_normal(n)
+    h = 1e-4
+    rng = np.random.default_rng(41)
+    pick = rng.choice(away_from_faces(x, h), size=64, replace=False)
+    dev = torch.device("cuda", 0)
+    xd = torch.from_numpy(x).to(dev)
+    qd = torch.from_numpy(q).to(dev)
+    wd = torch.from_numpy(w).to(dev)
+    phi = torch.empty(n, dtype=torch.float64, device=dev)
+    grad = torch.empty((n, 3), dtype=torch.float64, device=dev)
+    f = pkg.LaplaceFMM(x, q, c2_args(pkg, pkg.FP64))
+
+    def losses(qq=None):
+        f.forward_device(0 if qq is None else qq.data_ptr(), phi.data_ptr(), grad.data_ptr())
+        qv = qd if qq is None else qq
+        return float(wd @ phi), 0.5 * float(qv @ phi)
+
+    def dx_central(step):
+        fd = np.zeros((2, 64, 3))
+        for r, i in enumerate(pick):
+            for k in range(3):
+                v = []
+                for sgn in (1.0, -1.0):
+                    xp = xd.clone()
+                    xp[i, k] += sgn * step
+                    f.setup_device(xp.data_ptr(), qd.data_ptr(), n)
+                    v.append(losses())
+                fd[0, r, k] = (v[0][0] - v[1][0]) / (2 * step)
+                fd[1, r, k] = (v[0][1] - v[1][1]) / (2 * step)
+        return fd
+
+    fd_h = dx_central(h)
+    fd_h2 = dx_central(h / 2)
+    # charges: both losses are at most quadratic in q, so the central
+    # difference is exact up to rounding
+    f.setup_device(xd.data_ptr(), qd.data_ptr(), n)
+    fdq = np.zeros((2, 64))
+    for r, i in enumerate(pick):
+        v = []
+        for sgn in (1.0, -1.0):
+            qp = qd.clone()
+            qp[i] += sgn * h
+            v.append(losses(qp))
+        fdq[0, r] = (v[0][0] - v[1][0]) / (2 * h)
+        fdq[1, r] = (v[0][1] - v[1][1]) / (2 * h)
+    f.close()
+    rich = (4 * fd_h2 - fd_h) / 3
+    return dict(x=x, q=q, w=w, pick=pick, fd_h=fd_h, rich=rich, fdq=fdq)
+
+
+def adjoint_full(pkg, c4, precision):
+    """dL/dq, dL/dx at the picked bodies for both losses from the adjoint,
+    device-resident (forward pass, then the adjoint reusing its gradient)."""
+    import torch
+    x, q, w, pick = c4["x"], c4["q"], c4["w"], c4["pick"]
+    n = len(q)
+    dev = torch.device("cuda", 0)
+    xd, qd = torch.from_numpy(x).to(dev), torch.from_numpy(q).to(dev)
+    f = pkg.LaplaceFMM(x, q, c2_args(pkg, precision))
+    f.setup_device(xd.data_ptr(), qd.data_ptr(), n)
+    phi = torch.empty(n, dtype=torch.float64, device=dev)
+    grad = torch.empty((n, 3), dtype=torch.float64, device=dev)
+    dq = torch.empty(n, dtype=torch.float64, device=dev)
+    dx = torch.empty((n, 3), dtype=torch.float64, device=dev)
+    out = []
+    for wt in (torch.from_numpy(w).to(dev), 0.5 * qd):
+        f.forward_device(0, phi.data_ptr(), grad.data_ptr())
+        f.adjoint_device(wt.data_ptr(), dq.data_ptr(), dx.data_ptr())
+        dqn = dq.cpu().numpy()[pick]
+        if len(out) == 1:
+            # L = 1/2 q.K q: the adjoint with w = q/2 held fixed gives K^T q/2;
+            # the explicit dependence through w adds phi/2
+            dqn = dqn + 0.5 * phi.cpu().numpy()[pick]
+        out.append((dqn, dx.cpu().numpy()[pick]))
+    f.close()
+    return out
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_c4_gradients_by_finite_differences(pkg, c4, precision):
+    # measured: FP64 dL/dx 3e-7 / 5e-8 (the Richardson remainder), dL/dq
+    # 7e-10 / 1.3e-8; mixed dL/dx 7e-7, dL/dq 4e-9 / 6e-7
+    tol_x = 1e-6 if precision == 0 else 3e-6
+    tol_q = 1e-7 if precision == 0 else 2e-6
+    res = adjoint_full(pkg, c4, precision)
+    for loss, (dq, dx) in enumerate(res):
+        ex = rel(dx, c4["rich"][loss])
+        ex_h = rel(dx, c4["fd_h"][loss])
+        eq = rel(dq, c4["fdq"][loss])
+        print("C4 precision %d loss %d: dL/dx vs Richardson %.3e (vs D(h) %.3e), dL/dq %.3e"
+              % (precision, loss, ex, ex_h, eq))
+        assert ex < tol_x and eq < tol_q, (loss, ex, eq)
+
+
+def test_c4_half_energy_matches_reference_force(pkg, c4):
+    """For L = 1/2 sum q phi the mixed adjoint's dL/dx is q times the
+    reference's gradient output (sampled fixture), up to the FMM's asymmetry
+    and the mixed form's rounding."""
+    import torch
+    g = np.load(GOLDEN)
+    x, q = c4["x"], c4["q"]
+    idx = g["idx"]
+    n = len(q)
+    dev = torch.device("cuda", 0)
+    f = pkg.LaplaceFMM(x, q, c2_args(pkg, pkg.FP32_MIXED))
+    f.setup()
+    f.upload()
+    f.evaluate_device()
+    wt = torch.from_numpy(0.5 * q).to(dev)
+    dq = torch.empty(n, dtype=torch.float64, device=dev)
+    dx = torch.empty((n, 3), dtype=torch.float64, device=dev)
+    f.adjoint_device(wt.data_ptr(), dq.data_ptr(), dx.data_ptr())
+    f.close()
+    ref = q[idx][:, None] * g["grad"]
+    e = rel(dx.cpu().numpy()[idx], ref)
+    print("C4 mixed dL/dx (L = 1/2 q phi) vs q * reference gradient: %.3e" % e)
+    assert e < 2e-6, e
