@@ -229,8 +229,12 @@ def equal_error(pkg, mk, x, q, ref, w_dev, dq_dev, dx_dev, adj_ref, bound, steps
     """Both forms timed over a grid of expansion orders and leaf sizes, each
     setting's error taken against the FP64 form at the workload's own settings
     (P=8, ncrit=256: the reference's FP64 FMM on the same input, to 1e-13).
-    For each error bound the fastest FP64 setting and the fastest FP32-mixed
-    setting within it are compared, on the pass and on forward + adjoint."""
+    Every setting is timed on the pass and on forward + adjoint (the adjoint
+    reusing the forward gradient), and its adjoint's dL/dx and dL/dq are
+    compared with the FP64 adjoint at the workload's settings.  For each error
+    bound the fastest FP64 and FP32-mixed settings within it are compared:
+    on the pass by the pass's error, on forward + adjoint by the larger of the
+    pass's and the adjoint's errors."""
     import torch
     phi_ref, grad_ref = ref
     grid = []
@@ -247,64 +251,35 @@ def equal_error(pkg, mk, x, q, ref, w_dev, dq_dev, dx_dev, adj_ref, bound, steps
                     f.flush_l2()
                     ms.append(f.evaluate_device())
                 eg, ep = pass_error(*f.download(), phi_ref, grad_ref)
+                fa = []
+                for k in range(2 + steps):
+                    f.flush_l2()
+                    t = f.evaluate_device() + f.adjoint_device(w_dev.data_ptr(), dq_dev.data_ptr(),
+                                                                dx_dev.data_ptr())
+                    if k >= 2:
+                        fa.append(t)
+                ax, aq = pass_error(dq_dev.cpu().numpy(), dx_dev.cpu().numpy(), adj_ref[0], adj_ref[1])
                 grid.append({"form": "fp64" if prec == pkg.FP64 else "mixed", "P": P, "ncrit": ncrit,
-                             "ms": float(np.median(ms)), "err_grad": eg, "err_phi_mr": ep, "err": max(eg, ep)})
+                             "ms": float(np.median(ms)), "err_grad": eg, "err_phi_mr": ep, "err": max(eg, ep),
+                             "fwd_adj_ms": float(np.median(fa)), "adj_err_dLdx": ax, "adj_err_dLdq_mr": aq,
+                             "fwd_adj_err": max(eg, ep, ax, aq)})
                 f.close()
 
-    def fastest(form, e):
-        ok = [g for g in grid if g["form"] == form and g["err"] <= e]
-        return min(ok, key=lambda g: g["ms"]) if ok else None
-
-    def fwd_adj(g):
-        """forward + adjoint of one setting: device time, and the adjoint's
-        errors against the FP64 adjoint at the workload's settings"""
-        f = pkg.LaplaceFMM(x, q, mk(pkg.FP64 if g["form"] == "fp64" else pkg.FP32_MIXED, P=g["P"],
-                                    ncrit=g["ncrit"]))
-        f.setup()
-        f.upload()
-        ts = []
-        for k in range(2 + steps):
-            f.flush_l2()
-            t = f.evaluate_device() + f.adjoint_device(w_dev.data_ptr(), dq_dev.data_ptr(), dx_dev.data_ptr())
-            if k >= 2:
-                ts.append(t)
-        dq, dx = dq_dev.cpu().numpy(), dx_dev.cpu().numpy()
-        f.close()
-        egx, eqm = pass_error(dq, dx, adj_ref[0], adj_ref[1])
-        return float(np.median(ts)), {"dLdx": egx, "dLdq_mean_removed": eqm}
+    def fastest(form, key_err, key_ms, e):
+        ok = [g for g in grid if g["form"] == form and g[key_err] <= e]
+        return min(ok, key=lambda g: g[key_ms]) if ok else None
 
     out = []
     for name, e in bound:
-        a, b = fastest("fp64", e), fastest("mixed", e)
-        row = {"bound": name, "err_bound": e, "fp64": a, "mixed": b}
-        if a and b:
-            row["pass_speedup"] = a["ms"] / b["ms"]
-            fa_a, ea = fwd_adj(a)
-            fa_b, eb = fwd_adj(b)
-            row.update({"fwd_adj_ms_fp64": fa_a, "fwd_adj_ms_mixed": fa_b, "fwd_adj_speedup": fa_a / fa_b,
-                        "fwd_adj_err_fp64": ea, "fwd_adj_err_mixed": eb})
+        row = {"bound": name, "err_bound": e}
+        a, b = fastest("fp64", "err", "ms", e), fastest("mixed", "err", "ms", e)
+        row.update({"pass_fp64": a, "pass_mixed": b, "pass_speedup": a["ms"] / b["ms"] if a and b else None})
+        a, b = fastest("fp64", "fwd_adj_err", "fwd_adj_ms", e), fastest("mixed", "fwd_adj_err", "fwd_adj_ms", e)
+        row.update({"fwd_adj_fp64": a, "fwd_adj_mixed": b,
+                    "fwd_adj_speedup": a["fwd_adj_ms"] / b["fwd_adj_ms"] if a and b else None})
         out.append(row)
     torch.cuda.synchronize()
     return {"reference_form": "FP64 P=8 ncrit=256, the workload's settings", "grid": grid, "targets": out}
-
-
-def max_over_ranks(vals, world, device):
-    """The timings of every rank replaced by their maximum over ranks (one
-    all-reduce on the process group); unchanged on one rank.  Every rank
-    calls it at the same point."""
-    if world <= 1:
-        return [float(v) for v in vals]
-    import torch
-    import torch.distributed as dist
-    v = torch.tensor([float(x) for x in vals], dtype=torch.float64, device=device)
-    dist.all_reduce(v, op=dist.ReduceOp.MAX)
-    return v.tolist()
-
-
-def replica_value(n_per_rank, world, ms_max):
-    """Whole-job throughput of N independent replicas: all ranks' bodies over
-    the slowest rank's pass time."""
-    return world * n_per_rank / (ms_max * 1e-3)
 
 
 def run_ours(args):
