@@ -539,6 +539,97 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+# ----------------------------------------------------------------------------
+# the other large configurations (one JSON line each; the headline is C2)
+# ----------------------------------------------------------------------------
+def config_bodies(name):
+    """C3: 2^22 bodies in 64 Gaussian blobs (centres U[0,1)^3, sigma 0.02,
+    wrapped mod 1), charges +-1 balanced to net zero, seed 3.  C5: the 200^3
+    rock-salt lattice of spacing 1/200, each site jittered by U(+-0.1
+    spacing) per axis, charges (-1)^(i+j+k), seed 5."""
+    if name == "c3":
+        rng = np.random.default_rng(3)
+        n, nb = 1 << 22, 64
+        c = rng.random((nb, 3))
+        x = np.mod(c[rng.integers(0, nb, n)] + 0.02 * rng.standard_normal((n, 3)), 1.0)
+        q = np.where(rng.random(n) < 0.5, -1.0, 1.0)
+        return x, q - q.mean(), dict(P=10, ncrit=128, images=3)
+    m = 200
+    a = 1.0 / m
+    g = (np.arange(m) + 0.5) * a
+    X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
+    x = np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1)
+    x = np.mod(x + np.random.default_rng(5).uniform(-0.1 * a, 0.1 * a, x.shape), 1.0)
+    i, j, k = np.meshgrid(np.arange(m), np.arange(m), np.arange(m), indexing="ij")
+    q = np.where((i + j + k).ravel() % 2 == 0, 1.0, -1.0)
+    return x, q, dict(P=10, ncrit=256, images=4)
+
+
+CONFIG_DATA = {
+    "c3": "synthetic: 2^22 bodies in 64 Gaussian blobs (sigma 0.02, wrapped), q=+-1 net zero, seed 3",
+    "c5": "synthetic: 200^3 rock-salt lattice jittered by U(+-0.1 spacing), q=(-1)^(i+j+k), seed 5",
+}
+
+
+def run_config(args):
+    """One configuration other than the headline: both forms' pass and
+    forward + adjoint times (device-resident, CUDA events, L2 flushed between
+    steps) and the mixed form's errors against the FP64 form."""
+    import torch
+    torch.cuda.set_device(0)
+    pkg = load_pkg()
+    x, q, c = config_bodies(args.config)
+    n = len(q)
+    mk = lambda prec: pkg.Argument(P=c["P"], ncrit=c["ncrit"], images=c["images"], cycle=1.0, x=(0.5, 0.5, 0.5),
+                                   dipole_correction=0, divide_4pi=1, precision=prec, device=0)
+    w_dev = torch.from_numpy(np.random.default_rng(4).standard_normal(n)).cuda()
+    dq_dev = torch.empty(n, dtype=torch.float64, device="cuda")
+    dx_dev = torch.empty((n, 3), dtype=torch.float64, device="cuda")
+    res = {}
+    with ClockSampler(0) as clk:
+        for prec in (pkg.FP64, pkg.FP32_MIXED):
+            f = pkg.LaplaceFMM(x, q, mk(prec))
+            t0 = time.perf_counter()
+            f.setup()
+            f.upload()
+            setup_s = time.perf_counter() - t0
+            for _ in range(args.warmup):
+                f.evaluate_device()
+            ms = []
+            for _ in range(args.steps):
+                f.flush_l2()
+                ms.append(f.evaluate_device())
+            phi, grad = f.download()
+            fa = []
+            for k in range(1 + max(2, args.steps // 2)):
+                f.flush_l2()
+                t = f.evaluate_device() + f.adjoint_device(w_dev.data_ptr(), dq_dev.data_ptr(), dx_dev.data_ptr())
+                if k:
+                    fa.append(t)
+            res[prec] = dict(ms=float(np.median(ms)), fwd_adj_ms=float(np.median(fa)), phi=phi, grad=grad,
+                             dq=dq_dev.cpu().numpy(), dx=dx_dev.cpu().numpy(), setup_s=setup_s, info=f.info())
+            f.close()
+    d, m = res[pkg.FP64], res[pkg.FP32_MIXED]
+    eg, ep = pass_error(m["phi"], m["grad"], d["phi"], d["grad"])
+    ax, aq = pass_error(m["dq"], m["dx"], d["dq"], d["dx"])
+    line = {"metric": METRIC.replace("N=1M P=8", "%s N=%d P=%d" % (args.config.upper(), n, c["P"])),
+            "value": n / (m["ms"] * 1e-3), "unit": "particles/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": m["ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32-mixed", "data": CONFIG_DATA[args.config],
+            "config": {"workload": "periodic KIFMM evaluation pass %s" % args.config.upper(), "N": n, **c,
+                       "l2": "256 MB flush between timed steps", "nleaf": m["info"]["nleaf"],
+                       "ncell": m["info"]["ncell"], "p2p_pairs": m["info"]["p2p_pairs"],
+                       "close_pairs": m["info"]["close_pairs"],
+                       "fp64_ms_per_step": d["ms"], "mixed_speedup_vs_fp64": d["ms"] / m["ms"],
+                       "mixed_err_vs_fp64": {"l2f": eg, "l2p_mean_removed": ep},
+                       "fwd_adj_ms_mixed": m["fwd_adj_ms"], "fwd_adj_ms_fp64": d["fwd_adj_ms"],
+                       "fwd_adj_mixed_speedup_vs_fp64": d["fwd_adj_ms"] / m["fwd_adj_ms"],
+                       "fwd_adj_mixed_err_vs_fp64": {"dLdx_l2": ax, "dLdq_l2_mean_removed": aq},
+                       "setup_s": {"fp64": d["setup_s"], "mixed": m["setup_s"]}},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -549,8 +640,12 @@ def main():
     ap.add_argument("--ref-n", type=int, default=WORKLOAD["N"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-equal-error", action="store_true")
+    ap.add_argument("--config", default="c2", choices=["c2", "c3", "c5"],
+                    help="c2: the headline workload (default); c3, c5: the clustered and lattice configurations")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.config != "c2":
+        run_config(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -81,7 +81,10 @@ struct ApplyCall {
 
 // Largest P at which the FP32-mixed form runs the 8x8 FFT-M2L in FP32 (its
 // gradient error stays below 1e-5 on uniform inputs up to P = 8; 3e-5 at 10).
-constexpr int kM2L32MaxP = 8;
+#ifndef M2L32_MAXP
+#define M2L32_MAXP 8
+#endif
+constexpr int kM2L32MaxP = M2L32_MAXP;
 
 enum BSel { B_P2M1 = 0, B_P2M2, B_L2P1, B_L2P2, B_M2MT, B_M2M, B_IMGSUMT, B_IMG13, B_ADJ_IMG_UP, B_ADJ_IMG_DOWN,
             B_NUM };
