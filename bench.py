@@ -282,6 +282,25 @@ def equal_error(pkg, mk, x, q, ref, w_dev, dq_dev, dx_dev, adj_ref, bound, steps
     return {"reference_form": "FP64 P=8 ncrit=256, the workload's settings", "grid": grid, "targets": out}
 
 
+def max_over_ranks(vals, world, device):
+    """The timings of every rank replaced by their maximum over ranks (one
+    all-reduce on the process group); unchanged on one rank.  Every rank
+    calls it at the same point."""
+    if world <= 1:
+        return [float(v) for v in vals]
+    import torch
+    import torch.distributed as dist
+    v = torch.tensor([float(x) for x in vals], dtype=torch.float64, device=device)
+    dist.all_reduce(v, op=dist.ReduceOp.MAX)
+    return v.tolist()
+
+
+def replica_value(n_per_rank, world, ms_max):
+    """Whole-job throughput of N independent replicas: all ranks' bodies over
+    the slowest rank's pass time."""
+    return world * n_per_rank / (ms_max * 1e-3)
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist

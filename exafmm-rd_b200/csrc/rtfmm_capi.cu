@@ -199,6 +199,17 @@ struct rtfmm_fmm {
   // mixed form: the P2P pairs much closer than their leaves (tree-order
   // target t: pairs d_close_pairs[d_close_off[t] .. d_close_off[t+1]]),
   // found once per set of device positions, refined to FP64 every pass
+  // sharding (rtfmm_b200_shard): this rank computes the bodies of the leaves
+  // whose first body lies in its share of the tree-order body range, and the
+  // cells above them; shard_n == 1 is the whole pass
+  int shard_rank = 0, shard_n = 1;
+  bool shard_up = false;  // the upward phase ran; the downward may follow
+  std::vector<char> cell_own;       // per cell (image cells too): computed here
+  std::vector<int> own_leaves;      // leaf-table indices of the leaves computed here
+  std::vector<LeafInfo> leaves_own;
+  LeafInfo* d_leaves_own = nullptr;  // == d_leaves without sharding
+  int* d_leaf_cells = nullptr;      // cell of every leaf (leaf-table order)
+  char* d_leaf_own = nullptr;
   int* d_close_cnt = nullptr;
   int* d_close_off = nullptr;
   int2* d_close_pairs = nullptr;
@@ -366,6 +377,23 @@ void build_tables(rtfmm_fmm* f, bool host_p2p = true) {
   for (int l = 0; l < nlf; ++l) dfs[l] = l;
   std::sort(dfs.begin(), dfs.end(), [&](int a, int b) { return f->leaves[a].boff < f->leaves[b].boff; });
   for (int i = 0; i < nlf; ++i) dfs_pos[dfs[i]] = i;
+  // ownership: leaf l belongs to rank floor(boff * R / n); a cell is
+  // computed by every rank that owns a leaf beneath it (image cells by all)
+  {
+    const int R = std::max(1, f->shard_n);
+    f->cell_own.assign(p.cells.size(), R == 1 ? 1 : 0);
+    f->own_leaves.clear();
+    for (int l = 0; l < nlf; ++l) {
+      const int owner = p.n > 0 ? (int)((int64_t)f->leaves[l].boff * R / p.n) : 0;
+      if (R > 1 && owner != f->shard_rank) continue;
+      f->own_leaves.push_back(l);
+      if (R > 1)
+        for (int a = f->leaves[l].cell; a >= 0 && !f->cell_own[a]; a = parent[a]) f->cell_own[a] = 1;
+    }
+    for (size_t c = p.ntree; c < p.cells.size(); ++c) f->cell_own[c] = 1;
+    f->leaves_own.clear();
+    for (int l : f->own_leaves) f->leaves_own.push_back(f->leaves[l]);
+  }
   f->p2p_on_device = !host_p2p;
   if (!host_p2p) {
     f->list_off.clear();
@@ -470,6 +498,15 @@ void build_tables(rtfmm_fmm* f, bool host_p2p = true) {
     }
   }
   f->p2p_pairs = pairs;
+  if (f->shard_n > 1) {  // this rank's targets only
+    std::vector<P2PItem32> mine;
+    std::vector<char> own(nlf, 0);
+    for (int l : f->own_leaves) own[l] = 1;
+    for (const P2PItem32& it : f->items2)
+      if (own[it.leaf]) mine.push_back(it);
+    f->items2.swap(mine);
+    f->n_items2 = (int)f->items2.size();
+  }
   build_pass_tables(f);
 }
 
@@ -516,15 +553,15 @@ void build_pass_tables(rtfmm_fmm* f) {
   f->l2l_calls.clear();
   f->l2p_call.clear();
   {
-    std::vector<int> in, out;
+    // rows of the leaf vectors are this rank's leaves (all without sharding)
+    std::vector<int> out;
     std::vector<double> sc;
-    for (int l = 0; l < (int)f->leaves.size(); ++l) {
-      in.push_back(l);
-      out.push_back(f->leaves[l].cell);
-      sc.push_back(f->leaves[l].scale);
+    for (const LeafInfo& L : f->leaves_own) {
+      out.push_back(L.cell);
+      sc.push_back(L.scale);
     }
-    std::vector<int> lid(f->leaves.size());
-    for (int l = 0; l < (int)f->leaves.size(); ++l) lid[l] = l;
+    std::vector<int> lid(f->leaves_own.size());
+    for (int l = 0; l < (int)lid.size(); ++l) lid[l] = l;
     add_call(f->p2m_call, 1, {lid}, {lid}, nullptr, B_P2M1, BUF_LEAF, BUF_LEAF2, 0);
     add_call(f->p2m_call, 1, {lid}, {out}, &sc, B_P2M2, BUF_LEAF2, BUF_QEQ, 0);
     add_call(f->l2p_call, 1, {out}, {lid}, nullptr, B_L2P1, BUF_PCHK, BUF_LEAF, 0);
@@ -569,7 +606,7 @@ void build_pass_tables(rtfmm_fmm* f) {
     std::vector<int> in1, out1;
     for (int c = 0; c < (int)p.cells.size(); ++c) {
       const Cell& cl = p.cells[c];
-      if (cl.depth != depth || cl.cnum == 0) continue;
+      if (cl.depth != depth || cl.cnum == 0 || !f->cell_own[c]) continue;
       if (depth >= 0) {
         for (int k = 0; k < cl.cnum; ++k) {
           const int ch = cl.coff + k;
@@ -597,6 +634,7 @@ void build_pass_tables(rtfmm_fmm* f) {
   std::vector<int> s8(ncell, -1), s27(ncell, -1);
   std::vector<int> t8cells, t27cells;
   for (const auto& kv : p.m2l) {
+    if (!f->cell_own[kv.first]) continue;  // another rank's targets
     bool single = false, normal = false;
     for (const M2LEntry& e : kv.second) (e.single ? single : normal) = true;
     if (normal) t8cells.push_back(kv.first);
@@ -794,6 +832,20 @@ int upload_plan(rtfmm_fmm* f) {
   RC(dalloc(f, &f->d_xin, 3 * n));
   RC(dalloc(f, &f->d_qin, n));
   RC(dupload(f, &f->d_leaves, f->leaves));
+  {
+    // the exchange of a two-phase pass: every leaf's cell, and which leaves
+    // this rank computes
+    std::vector<int> lc(nleaf);
+    std::vector<char> lo(nleaf, 0);
+    for (size_t l = 0; l < nleaf; ++l) lc[l] = f->leaves[l].cell;
+    for (int l : f->own_leaves) lo[l] = 1;
+    RC(dupload(f, &f->d_leaf_cells, lc));
+    RC(dupload(f, &f->d_leaf_own, lo));
+  }
+  if (f->shard_n > 1)
+    RC(dupload(f, &f->d_leaves_own, f->leaves_own));
+  else
+    f->d_leaves_own = f->d_leaves;
   RC(dalloc(f, &f->d_qeq, ncell * ns));
   RC(dalloc(f, &f->d_pchk, ncell * ns));
   RC(dalloc(f, &f->d_leafvec, nleaf * ns));
@@ -912,18 +964,35 @@ int run_apply(rtfmm_fmm* f, const ApplyCall& c, bool adjoint = false) {
 // charges (which then hold the weights w): P2P, M2L and the tree-level
 // M2M/L2L and P2M/L2P pairs are their own transposes on the symmetric lists,
 // only the image-level operators swap; no dipole correction.
-int enqueue_pass(rtfmm_fmm* f, bool adjoint = false, bool no_dipole = false) {
+//
+// phase 0 is the whole pass.  A sharded pass runs in two phases around the
+// caller's exchange: phase 1 (upward) runs P2P and P2M for this rank's
+// leaves and gathers every leaf's q_equiv row into xbuf (rows of other
+// ranks' leaves zero); phase 2 (downward) takes xbuf summed over the ranks
+// back into the leaf rows and runs M2M on the whole tree, then M2L, L2L and
+// L2P for this rank's cells and the post-processing.
+int enqueue_pass(rtfmm_fmm* f, bool adjoint = false, bool no_dipole = false, int phase = 0,
+                 double* xbuf = nullptr) {
   const Plan& p = f->plan;
   const Operators& o = f->ops;
   const int n = (int)p.n, ns = o.ns, Nf = o.Nf, P = o.P;
-  const int nleaf = (int)f->leaves.size();
+  const int nleaf = (int)f->leaves_own.size();  // the leaves whose P2M / L2P run here
   const bool mixed = f->args.precision == RTFMM_FP32_MIXED;
   const unsigned stages = f->args.stages;
   const bool near = stages & RTFMM_STAGE_NEAR, far = stages & RTFMM_STAGE_FAR;
   const bool serial = stages & RTFMM_STAGE_SERIAL;
   cudaStream_t s0 = f->s0, s1 = serial ? f->s0 : f->s1;
+  const bool up = phase != 2, down = phase != 1;
   f->launches = 0;
-  CK(cudaEventRecord(f->ev_start, s0));
+  if (phase == 1) {
+    // the bodies of other ranks' leaves get no P2P or L2P here: zero outputs
+    // (before ev_start, which the P2P stream waits for)
+    CK(cudaMemsetAsync(f->d_near_phi, 0, sizeof(double) * n, s0));
+    CK(cudaMemsetAsync(f->d_near_grad, 0, sizeof(double) * 3 * n, s0));
+    CK(cudaMemsetAsync(f->d_far_phi, 0, sizeof(double) * n, s0));
+    CK(cudaMemsetAsync(f->d_far_grad, 0, sizeof(double) * 3 * n, s0));
+  }
+  if (up) CK(cudaEventRecord(f->ev_start, s0));
   auto near_field = [&]() -> int {
     if (!serial) CK(cudaStreamWaitEvent(s1, f->ev_start, 0));
     if (mixed) {
@@ -948,20 +1017,38 @@ int enqueue_pass(rtfmm_fmm* f, bool adjoint = false, bool no_dipole = false) {
     CK(cudaEventRecord(f->ev_near, s1));
     return RTFMM_OK;
   };
-  if (near && !serial) {
+  if (near && !serial && up) {
     int rc = near_field();
     if (rc) return rc;
   }
-  CK(cudaEventRecord(f->ev_st[ST_PREP], s0));
-  if (far) {
-    CK(cudaMemsetAsync(f->d_pchk, 0, sizeof(double) * p.cells.size() * ns, s0));
-    CK(launch_p2m_check(f->d_body64, f->d_leaves, nleaf, f->d_surf_unit, ns, f->d_leafvec, s0, mixed ? 1 : 2));
+  if (up) CK(cudaEventRecord(f->ev_st[ST_PREP], s0));
+  if (far && phase == 0) CK(cudaMemsetAsync(f->d_pchk, 0, sizeof(double) * p.cells.size() * ns, s0));
+  if (far && up) {
+    CK(launch_p2m_check(f->d_body64, f->d_leaves_own, nleaf, f->d_surf_unit, ns, f->d_leafvec, s0,
+                        mixed ? 1 : 2));
     f->launches++;
     for (auto& c : f->p2m_call) {
       int rc = run_apply(f, c);
       if (rc) return rc;
     }
     CK(cudaEventRecord(f->ev_st[ST_P2M], s0));
+  }
+  if (phase == 1) {
+    // every leaf's q_equiv row into the exchange buffer (others' rows zero)
+    if (far) {
+      CK(launch_leaf_rows(f->d_qeq, (int)p.cells.size(), f->d_leaf_cells, f->d_leaf_own, (int)f->leaves.size(), ns,
+                            xbuf, false, s0));
+      f->launches++;
+    }
+    return RTFMM_OK;
+  }
+  if (phase == 2 && far) {
+    CK(launch_leaf_rows(f->d_qeq, (int)p.cells.size(), f->d_leaf_cells, nullptr, (int)f->leaves.size(), ns, xbuf,
+                            true, s0));
+    f->launches++;
+  }
+  if (far && down) {
+    if (phase == 2) CK(cudaMemsetAsync(f->d_pchk, 0, sizeof(double) * p.cells.size() * ns, s0));
     for (auto& c : f->m2m_calls) {
       int rc = run_apply(f, c, adjoint);
       if (rc) return rc;
@@ -1010,7 +1097,7 @@ int enqueue_pass(rtfmm_fmm* f, bool adjoint = false, bool no_dipole = false) {
       int rc = run_apply(f, c);
       if (rc) return rc;
     }
-    CK(launch_l2p_eval(f->d_body64, f->d_leaves, nleaf, f->d_surf_unit, ns, f->d_leafvec2, f->d_far_phi,
+    CK(launch_l2p_eval(f->d_body64, f->d_leaves_own, nleaf, f->d_surf_unit, ns, f->d_leafvec2, f->d_far_phi,
                        f->d_far_grad, s0, mixed ? 1 : 2));
     f->launches++;
     CK(cudaEventRecord(f->ev_st[ST_L2P], s0));
@@ -1408,6 +1495,7 @@ int rtfmm_b200_setup(rtfmm_fmm* f, int64_t n, const double* x, const double* q) 
 
 int rtfmm_b200_setup_device(rtfmm_fmm* f, int64_t n, const double* x_dev, const double* q_dev) {
   if (!f) return fail(RTFMM_EINVAL, "null handle");
+  if (f->shard_n > 1) return fail(RTFMM_ENOTSUP, "sharded handles are set up from host bodies (rtfmm_b200_setup)");
   if (n < 0 || n > (int64_t)1 << 30) return fail(RTFMM_EINVAL, "n out of range");
   if (n > 0 && (!x_dev || !q_dev)) return fail(RTFMM_EINVAL, "null body arrays");
   const double t0 = wall_s();
@@ -1504,6 +1592,7 @@ int rtfmm_b200_upload(rtfmm_fmm* f) {
 
 int rtfmm_b200_evaluate_device(rtfmm_fmm* f, float* ms) {
   if (!f) return fail(RTFMM_EINVAL, "null handle");
+  if (f->shard_n > 1) return fail(RTFMM_ESTATE, "sharded handle: run the pass with rtfmm_b200_shard_upward/_downward");
   if (!f->setup_done || !f->device_ready) return fail(RTFMM_ESTATE, "upload has not run");
   CK(cudaSetDevice(f->dev));
   if (f->plan.n == 0) {
@@ -1523,6 +1612,7 @@ int rtfmm_b200_evaluate_device(rtfmm_fmm* f, float* ms) {
 
 int rtfmm_b200_forward_device(rtfmm_fmm* f, const double* q_dev, double* phi_dev, double* grad_dev, float* ms) {
   if (!f) return fail(RTFMM_EINVAL, "null handle");
+  if (f->shard_n > 1) return fail(RTFMM_ESTATE, "sharded handle: run the pass with rtfmm_b200_shard_upward/_downward");
   if (!f->setup_done || !f->device_ready || !f->pos_on_device)
     return fail(RTFMM_ESTATE, "upload (or an evaluate) has not run");
   if (ms) *ms = 0;
@@ -1558,6 +1648,7 @@ int rtfmm_b200_download(rtfmm_fmm* f, double* phi, double* grad) {
 
 int rtfmm_b200_evaluate(rtfmm_fmm* f, const double* q, double* phi, double* grad) {
   if (!f) return fail(RTFMM_EINVAL, "null handle");
+  if (f->shard_n > 1) return fail(RTFMM_ESTATE, "sharded handle: run the pass with rtfmm_b200_shard_upward/_downward");
   if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");
   const int64_t n = f->plan.n;
   if (n == 0) return RTFMM_OK;
@@ -1654,6 +1745,7 @@ int adjoint_core(rtfmm_fmm* f, const double* w, double* dq, double* dx) {
 
 int rtfmm_b200_adjoint(rtfmm_fmm* f, const double* w, double* dLdq, double* dLdx) {
   if (!f) return fail(RTFMM_EINVAL, "null handle");
+  if (f->shard_n > 1) return fail(RTFMM_ESTATE, "sharded handle: run the pass with rtfmm_b200_shard_upward/_downward");
   if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");
   const int64_t n = f->plan.n;
   if (n == 0) return RTFMM_OK;
@@ -1687,6 +1779,7 @@ int rtfmm_b200_adjoint(rtfmm_fmm* f, const double* w, double* dLdq, double* dLdx
 
 int rtfmm_b200_adjoint_device(rtfmm_fmm* f, const double* w_dev, double* dLdq_dev, double* dLdx_dev, float* ms) {
   if (!f) return fail(RTFMM_EINVAL, "null handle");
+  if (f->shard_n > 1) return fail(RTFMM_ESTATE, "sharded handle: run the pass with rtfmm_b200_shard_upward/_downward");
   if (!f->setup_done || !f->device_ready) return fail(RTFMM_ESTATE, "upload has not run");
   if (ms) *ms = 0;
   if (f->plan.n == 0) return RTFMM_OK;
@@ -1701,6 +1794,83 @@ int rtfmm_b200_adjoint_device(rtfmm_fmm* f, const double* w_dev, double* dLdq_de
   float t = 0;
   CK(cudaEventElapsedTime(&t, f->ev_adj0, f->ev_adj1));
   if (ms) *ms = t;
+  f->pass_done = true;
+  return RTFMM_OK;
+}
+
+int rtfmm_b200_shard(rtfmm_fmm* f, int rank, int nranks) {
+  if (!f) return fail(RTFMM_EINVAL, "null handle");
+  if (nranks < 1 || rank < 0 || rank >= nranks) return fail(RTFMM_EINVAL, "shard: need 0 <= rank < nranks");
+  f->shard_rank = rank;
+  f->shard_n = nranks;
+  // the ownership is part of the plan: set up again
+  f->setup_done = false;
+  f->device_ready = false;
+  drop_graph(f);
+  return RTFMM_OK;
+}
+
+int rtfmm_b200_shard_sizes(rtfmm_fmm* f, int64_t* nbodies, int64_t* xbuf_doubles) {
+  if (!f) return fail(RTFMM_EINVAL, "null handle");
+  if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");
+  int64_t nb = 0;
+  for (const LeafInfo& L : f->leaves_own) nb += L.bnum;
+  if (nbodies) *nbodies = nb;
+  if (xbuf_doubles) *xbuf_doubles = (int64_t)f->leaves.size() * f->ops.ns;
+  return RTFMM_OK;
+}
+
+int rtfmm_b200_shard_bodies(rtfmm_fmm* f, int64_t* idx, int64_t cap) {
+  if (!f || !idx) return fail(RTFMM_EINVAL, "null argument");
+  if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");
+  int rc = ensure_host_bodies(f);
+  if (rc) return rc;
+  std::vector<int64_t> v;
+  for (const LeafInfo& L : f->leaves_own)
+    for (int b = 0; b < L.bnum; ++b) v.push_back(f->plan.perm[L.boff + b]);
+  std::sort(v.begin(), v.end());
+  if ((int64_t)v.size() > cap) return fail(RTFMM_EINVAL, "shard_bodies: cap too small");
+  std::copy(v.begin(), v.end(), idx);
+  return RTFMM_OK;
+}
+
+int rtfmm_b200_shard_upward(rtfmm_fmm* f, double* xbuf_dev) {
+  if (!f || !xbuf_dev) return fail(RTFMM_EINVAL, "null argument");
+  if (!f->setup_done || !f->device_ready || !f->pos_on_device)
+    return fail(RTFMM_ESTATE, "upload (or an evaluate) has not run");
+  if (f->plan.n == 0) return RTFMM_OK;
+  CK(cudaSetDevice(f->dev));
+  int rc = ensure_close_pairs(f);
+  if (rc) return rc;
+  rc = enqueue_pass(f, false, false, 1, xbuf_dev);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(f->s0));  // the buffer is complete; P2P may still run
+  CK(cudaGetLastError());
+  f->shard_up = true;
+  return RTFMM_OK;
+}
+
+int rtfmm_b200_shard_downward(rtfmm_fmm* f, const double* xbuf_dev, double* phi_dev, double* grad_dev, float* ms) {
+  if (!f || !xbuf_dev) return fail(RTFMM_EINVAL, "null argument");
+  if (!f->shard_up) return fail(RTFMM_ESTATE, "shard_upward has not run");
+  if (ms) *ms = 0;
+  const int64_t n = f->plan.n;
+  if (n == 0) return RTFMM_OK;
+  CK(cudaSetDevice(f->dev));
+  CK(cudaEventRecord(f->ev_g0, f->s0));
+  int rc = enqueue_pass(f, false, false, 2, const_cast<double*>(xbuf_dev));
+  if (rc) return rc;
+  if (phi_dev) CK(cudaMemcpyAsync(phi_dev, f->d_out_phi, sizeof(double) * n, cudaMemcpyDeviceToDevice, f->s0));
+  if (grad_dev)
+    CK(cudaMemcpyAsync(grad_dev, f->d_out_grad, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, f->s0));
+  CK(cudaEventRecord(f->ev_g1, f->s0));
+  CK(cudaEventSynchronize(f->ev_g1));
+  CK(cudaGetLastError());
+  float t = 0;
+  CK(cudaEventElapsedTime(&t, f->ev_g0, f->ev_g1));
+  if (ms) *ms = t;
+  f->shard_up = false;
+  f->grad_q_valid = false;
   f->pass_done = true;
   return RTFMM_OK;
 }

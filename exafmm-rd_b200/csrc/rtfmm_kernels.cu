@@ -1759,6 +1759,32 @@ cudaError_t launch_adj_combine(const int64_t* perm, const double* w, const doubl
   return cudaGetLastError();
 }
 
+// Leaf rows of the cell vectors <-> a leaf-ordered buffer (the exchange of
+// a sharded pass): gather writes buf[l] = own[l] ? v[cell[l]] : 0 (own null:
+// every row), scatter writes v[cell[l]] = buf[l].
+__global__ void k_leaf_rows(double* __restrict__ v, int nrow, const int* __restrict__ cells,
+                            const char* __restrict__ own, int nleaf, int ns, double* __restrict__ buf, int scatter) {
+  const int l = blockIdx.x;
+  if (l >= nleaf) return;
+  const int c = cells[l];
+  if (c < 0 || c >= nrow) return;  // not a row of v
+  double* row = v + (size_t)c * ns;
+  double* b = buf + (size_t)l * ns;
+  if (scatter) {
+    for (int i = threadIdx.x; i < ns; i += blockDim.x) row[i] = b[i];
+  } else {
+    const bool keep = own == nullptr || own[l];
+    for (int i = threadIdx.x; i < ns; i += blockDim.x) b[i] = keep ? row[i] : 0.0;
+  }
+}
+
+cudaError_t launch_leaf_rows(double* v, int nrow, const int* cells, const char* own, int nleaf, int ns,
+                             double* buf, bool scatter, cudaStream_t st) {
+  if (nleaf > 0 && (!v || !cells || !buf)) return cudaErrorInvalidValue;
+  if (nleaf > 0) k_leaf_rows<<<nleaf, 128, 0, st>>>(v, nrow, cells, own, nleaf, ns, buf, scatter ? 1 : 0);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_post(const double* phi_far, const double* grad_far, const double* phi_near,
                         const double* grad_near, const double4* body64, const int64_t* perm, int n,
                         const double* dipole_partial, double coef, int dipole, const double* centre,

@@ -124,6 +124,11 @@ cudaError_t launch_restore_charges(double4* body64, const double* qsave, int n, 
 cudaError_t launch_set_charges(double4* body64, const double* q, const int64_t* perm, int n, cudaStream_t st);
 cudaError_t launch_adj_combine(const int64_t* perm, const double* w, const double* qsave, const double* grad_q,
                                const double* grad_w, int n, double* dLdx, cudaStream_t st);
+// a sharded pass's exchange: leaf rows of v (nrow rows, stride ns) into a
+// leaf-ordered buffer (scatter = false; rows of leaves with own[l] == 0 are
+// zero, own null keeps all) or back (scatter = true)
+cudaError_t launch_leaf_rows(double* v, int nrow, const int* cells, const char* own, int nleaf, int ns,
+                             double* buf, bool scatter, cudaStream_t st);
 // dipole: 0 none, 1 the reference's per-body form, 2 the surface term's
 // potential; centre: the box centre (3), the dipole's origin
 cudaError_t launch_post(const double* phi_far, const double* grad_far, const double* phi_near,

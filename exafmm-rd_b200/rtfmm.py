@@ -42,6 +42,8 @@ EXPORTS = (
     "rtfmm_b200_last_error", "rtfmm_b200_version", "rtfmm_b200_clear_operator_cache",
     "rtfmm_b200_save_operators", "rtfmm_b200_load_operators", "rtfmm_b200_p2m_noalloc",
     "rtfmm_b200_ewald_sampled", "rtfmm_b200_direct_sampled",
+    "rtfmm_b200_shard", "rtfmm_b200_shard_sizes", "rtfmm_b200_shard_bodies", "rtfmm_b200_shard_upward",
+    "rtfmm_b200_shard_downward",
 )
 
 
@@ -108,6 +110,11 @@ def lib():
         "rtfmm_b200_get_cell_vectors": (ctypes.c_int, [_vp, ctypes.c_int, _dp]),
         "rtfmm_b200_get_operator": (ctypes.c_int, [_vp, ctypes.c_int, _dp, ctypes.c_int64]),
         "rtfmm_b200_get_leaf_lists": (ctypes.c_int, [_vp, _ip, _ip, _dp, ctypes.c_int64]),
+        "rtfmm_b200_shard": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
+        "rtfmm_b200_shard_sizes": (ctypes.c_int, [_vp, _lp, _lp]),
+        "rtfmm_b200_shard_bodies": (ctypes.c_int, [_vp, _lp, ctypes.c_int64]),
+        "rtfmm_b200_shard_upward": (ctypes.c_int, [_vp, _vp]),
+        "rtfmm_b200_shard_downward": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_float)]),
         "rtfmm_b200_last_error": (ctypes.c_char_p, []),
         "rtfmm_b200_version": (ctypes.c_char_p, []),
     }
@@ -292,6 +299,40 @@ class LaplaceFMM:
         ms = ctypes.c_float(0)
         _check(lib().rtfmm_b200_adjoint_device(self._h, _vp(w_ptr), _vp(dq_ptr or None), _vp(dx_ptr or None),
                                                ctypes.byref(ms)))
+        return ms.value
+
+    # -- the pass sharded over ranks ------------------------------------------------
+    def shard(self, rank, nranks):
+        """This handle computes rank `rank` of `nranks` shares of the pass
+        (before setup(); see rtfmm_b200_shard in include/rtfmm_b200.h)."""
+        _check(lib().rtfmm_b200_shard(self._h, int(rank), int(nranks)))
+        self._set_up = False
+
+    def shard_sizes(self):
+        """(bodies computed by this rank, doubles of the exchange buffer)."""
+        nb, nx = ctypes.c_int64(0), ctypes.c_int64(0)
+        _check(lib().rtfmm_b200_shard_sizes(self._h, ctypes.byref(nb), ctypes.byref(nx)))
+        return nb.value, nx.value
+
+    def shard_bodies(self):
+        """Input indices of the bodies whose outputs this rank computes."""
+        nb, _ = self.shard_sizes()
+        idx = np.zeros(max(nb, 1), dtype=np.int64)
+        _check(lib().rtfmm_b200_shard_bodies(self._h, _ptr(idx, _lp), nb))
+        return idx[:nb]
+
+    def shard_upward(self, xbuf_ptr):
+        """P2M of this rank's leaves; every leaf's q_equiv row into the device
+        buffer at xbuf_ptr (others' rows zero), to be summed over the ranks."""
+        _check(lib().rtfmm_b200_shard_upward(self._h, _vp(xbuf_ptr)))
+
+    def shard_downward(self, xbuf_ptr, phi_ptr, grad_ptr):
+        """The rest of the pass from the summed buffer; this rank's outputs
+        into the device arrays at phi_ptr (n) and grad_ptr (n, 3).  Returns
+        the device time of this phase in ms."""
+        ms = ctypes.c_float(0)
+        _check(lib().rtfmm_b200_shard_downward(self._h, _vp(xbuf_ptr), _vp(phi_ptr or None),
+                                               _vp(grad_ptr or None), ctypes.byref(ms)))
         return ms.value
 
     # -- introspection ------------------------------------------------------------

@@ -193,6 +193,41 @@ int rtfmm_b200_adjoint(rtfmm_fmm* fmm, const double* w, double* dLdq, double* dL
 int rtfmm_b200_adjoint_device(rtfmm_fmm* fmm, const double* w_dev, double* dLdq_dev, double* dLdx_dev,
                               float* ms);
 
+/* ---- The pass sharded over ranks (one process per GPU) ----
+ *
+ * No counterpart in the reference (it runs on one node with OpenMP; the
+ * pass it shards is LaplaceFMM::solve's hot block, fmm.cpp:51-60).  Every
+ * rank sets up the same bodies; rank r then computes the outputs of the
+ * leaves whose first body (in tree order) lies in its share
+ * [r n / R, (r + 1) n / R) of the bodies, and the cells above them:
+ *
+ *   rtfmm_b200_shard(h, r, R);              before rtfmm_b200_setup (host
+ *                                           bodies; setup_device is refused)
+ *   rtfmm_b200_setup(...); rtfmm_b200_upload(h);
+ *   per pass:
+ *     rtfmm_b200_shard_upward(h, xbuf);     P2M of this rank's leaves, every
+ *                                           leaf's q_equiv row into xbuf
+ *                                           (rows of other ranks' leaves 0);
+ *                                           P2P starts, on its own stream
+ *     all-reduce (sum) xbuf over the ranks  the one exchange (NCCL / gloo)
+ *     rtfmm_b200_shard_downward(h, xbuf, phi, grad, &ms);
+ *                                           M2M on the whole tree, M2L, L2L,
+ *                                           L2P of this rank's cells, post
+ *
+ * xbuf is device memory of nleaf * num_surf doubles
+ * (rtfmm_b200_shard_sizes).  phi / grad (device, input order, n and 3n)
+ * hold this rank's bodies (rtfmm_b200_shard_bodies gives their input
+ * indices); other entries are not computed.  The outputs of a body equal
+ * the unsharded pass's bit for bit.  The whole-pass entry points and the
+ * adjoint return RTFMM_ESTATE on a sharded handle; rtfmm_b200_shard(h, 0,
+ * 1) undoes sharding (at the next set-up). */
+int rtfmm_b200_shard(rtfmm_fmm* fmm, int rank, int nranks);
+int rtfmm_b200_shard_sizes(rtfmm_fmm* fmm, int64_t* nbodies, int64_t* xbuf_doubles);
+int rtfmm_b200_shard_bodies(rtfmm_fmm* fmm, int64_t* idx, int64_t cap);
+int rtfmm_b200_shard_upward(rtfmm_fmm* fmm, double* xbuf_dev);
+int rtfmm_b200_shard_downward(rtfmm_fmm* fmm, const double* xbuf_dev, double* phi_dev, double* grad_dev,
+                              float* ms);
+
 /*
  * Accuracy references on sampled targets, FP64 on the GPU (device `device`),
  * for sizes where a CPU sum would take hours.  x is n*3, q is n (host),

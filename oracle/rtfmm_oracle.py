@@ -529,12 +529,13 @@ class FMM:
     def depth_range(self):
         return min(self.cells.depth), max(self.cells.depth)
 
-    def p2m(self, charges=None):
-        """``p2m_precompute`` (``kernel.cpp:332-371``)."""
+    def p2m(self, charges=None, leaves=None):
+        """``p2m_precompute`` (``kernel.cpp:332-371``); `leaves` restricts it
+        (a sharded pass)."""
         c = self.cells
         q = self.q if charges is None else charges
         o = self.ops
-        for leaf in self.leaves():
+        for leaf in (self.leaves() if leaves is None else leaves):
             b0, nb = c.boff[leaf], c.bnum[leaf]
             xc = surface_points(self.P, c.r[leaf] * 2.95, c.x[leaf])
             pc = p2p_matrix(self.x[b0:b0 + nb], xc) @ q[b0:b0 + nb]
@@ -557,9 +558,10 @@ class FMM:
                     for k in range(27):
                         self.q_equiv[par] += o.m2m_img[k] @ self.q_equiv[ch]
 
-    def m2l(self):
+    def m2l(self, targets=None):
         """``m2l_fft_precompute_t`` (``kernel.cpp:1140-1397``) with the 8x8 and
-        1x27 Hadamard stages (``1012-1138``)."""
+        1x27 Hadamard stages (``1012-1138``); `targets` restricts the target
+        parents (a sharded pass)."""
         c = self.cells
         o = self.ops
         N = o.grid.N
@@ -574,6 +576,8 @@ class FMM:
                 grid[slot][o.up_idx] = self.q_equiv[ch]
             qk[s] = np.fft.rfftn(grid, axes=(1, 2, 3))
         for t in sorted(self.trav.m2l_parent):
+            if targets is not None and t not in targets:
+                continue
             lst = self.trav.m2l_parent[t]
             bydir = {}
             for (s, off, single) in lst:
@@ -593,14 +597,17 @@ class FMM:
                 g = np.fft.irfftn(pk[slot], s=(N, N, N))
                 self.p_check[ch] += g[o.down_idx] * scale
 
-    def l2l(self):
+    def l2l(self, parents=None):
         """``LaplaceFMM::L2L`` (``fmm.cpp:195-229``) with ``l2l_precompute``
-        (``kernel.cpp:1419-1428``) / ``l2l_img_precompute`` (``1430-1435``)."""
+        (``kernel.cpp:1419-1428``) / ``l2l_img_precompute`` (``1430-1435``);
+        `parents` restricts it (a sharded pass)."""
         c = self.cells
         o = self.ops
         dmin, dmax = self.depth_range()
         for depth in range(dmin, dmax):
             for par in self.nonleaf_at(depth):
+                if parents is not None and par not in parents:
+                    continue
                 if depth >= 0:
                     for k in range(c.cnum[par]):
                         ch = c.coff[par] + k
@@ -609,11 +616,11 @@ class FMM:
                     ch = c.coff[par]
                     self.p_check[ch] += o.l2l_img @ self.p_check[par]
 
-    def l2p(self):
-        """``l2p_precompute`` (``kernel.cpp:1458-1511``)."""
+    def l2p(self, leaves=None):
+        """``l2p_precompute`` (``kernel.cpp:1458-1511``); `leaves` restricts it."""
         c = self.cells
         o = self.ops
-        for leaf in self.leaves():
+        for leaf in (self.leaves() if leaves is None else leaves):
             b0, nb = c.boff[leaf], c.bnum[leaf]
             qd = (0.5 ** c.depth[leaf]) * (o.VSinv_l2p @ (o.UT_l2p @ self.p_check[leaf]))
             xe = surface_points(self.P, c.r[leaf] * 2.95, c.x[leaf])
@@ -622,12 +629,14 @@ class FMM:
             self.phi[b0:b0 + nb] += ir @ qd
             self.grad[b0:b0 + nb] -= np.einsum("ts,tsk->tk", (ir ** 3) * qd[None, :], d)
 
-    def p2p(self, charges=None):
+    def p2p(self, charges=None, targets=None):
         """``p2p_1toN_256`` (``kernel.cpp:258-311``) over ``P2P_map``
-        (``fmm.cpp:259-294``)."""
+        (``fmm.cpp:259-294``); `targets` restricts the target cells."""
         c = self.cells
         q = self.q if charges is None else charges
         for t, lst in self.trav.p2p.items():
+            if targets is not None and t not in targets:
+                continue
             b0, nb = c.boff[t], c.bnum[t]
             xt = self.x[b0:b0 + nb]
             for (s, off) in lst:
@@ -679,6 +688,65 @@ class FMM:
         out_phi[self.perm] = phi
         out_grad[self.perm] = grad
         return out_phi, out_grad
+
+
+    # -- the pass sharded over ranks (test model of rtfmm_b200_shard) ---------
+    def shard_owned(self, rank, nranks):
+        """The leaves rank `rank` of `nranks` computes (those whose first body
+        in tree order lies in [rank n / R, (rank + 1) n / R)) and the cells it
+        computes: those leaves' ancestors, and every image cell."""
+        c = self.cells
+        n = len(self.q)
+        parent = [-1] * len(c)
+        for i in range(len(c)):
+            if c.depth[i] >= 0:
+                for k in range(c.cnum[i]):
+                    parent[c.coff[i] + k] = i
+        leaves = [l for l in self.leaves() if (c.boff[l] * nranks) // max(n, 1) == rank]
+        cells = {i for i in range(len(c)) if c.depth[i] < 0}
+        for l in leaves:
+            a = l
+            while a >= 0 and a not in cells:
+                cells.add(a)
+                a = parent[a]
+        return leaves, cells
+
+    def solve_sharded(self, rank, nranks, allreduce):
+        """One rank's share of the pass: P2M of its leaves, the exchange
+        (`allreduce` sums the leaf q_equiv rows over the ranks in place), M2M
+        on the whole tree, M2L / L2L of its cells, L2P and P2P of its leaves.
+        Returns (phi, grad) in input order and the mask of the bodies it
+        computed (no dipole correction)."""
+        leaves, cells = self.shard_owned(rank, nranks)
+        self.p2m(leaves=leaves)
+        lv = self.leaves()
+        buf = np.zeros((len(lv), self.ops.ns))
+        own = set(leaves)
+        for i, l in enumerate(lv):
+            if l in own:
+                buf[i] = self.q_equiv[l]
+        allreduce(buf)
+        for i, l in enumerate(lv):
+            self.q_equiv[l] = buf[i]
+        self.m2m()
+        self.m2l(targets=cells)
+        self.l2l(parents=cells)
+        self.l2p(leaves=leaves)
+        self.p2p(targets=own)
+        mask = np.zeros(len(self.q), bool)
+        for l in leaves:
+            mask[self.cells.boff[l]:self.cells.boff[l] + self.cells.bnum[l]] = True
+        phi, grad = self.phi.copy(), self.grad.copy()
+        if self.divide_4pi:
+            phi *= INV4PI
+            grad *= INV4PI
+        out_phi = np.empty_like(phi)
+        out_grad = np.empty_like(grad)
+        out_mask = np.empty_like(mask)
+        out_phi[self.perm] = phi
+        out_grad[self.perm] = grad
+        out_mask[self.perm] = mask
+        return out_phi, out_grad, out_mask
 
 
 def solve(x, q, P, ncrit, images, cycle, **kw):
