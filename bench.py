@@ -20,9 +20,10 @@ reference:  the reference's own CPU FMM (compiled from its sources into
             host threads: its tree, lists and tables built once, then one
             run of its hot block per step.
 
-Multi-GPU (torchrun): the pass does not shard in this build, so each rank
-runs an independent replica on its own GPU; value = all ranks' bodies /
-max-over-ranks time.
+Multi-GPU (torchrun): by default each rank runs an independent replica on
+its own GPU; value = all ranks' bodies / max-over-ranks time.  With --shard
+the ranks split one pass (rtfmm_b200_shard: each computes its share of the
+bodies; one NCCL all-reduce of the leaf q_equiv rows per pass).
 """
 import argparse
 import json
@@ -584,6 +585,77 @@ def config_bodies(name):
     return x, q, dict(P=10, ncrit=256, images=4)
 
 
+def run_shard(args):
+    """The pass sharded over the ranks (rtfmm_b200_shard): every rank sets up
+    the headline workload, computes its share of the bodies, and the ranks
+    exchange once per pass (an NCCL all-reduce of the leaf q_equiv rows, 43 MB
+    at N=2^20, P=8).  Total work is fixed: strong scaling.  A step is the
+    upward phase, the all-reduce and the downward phase, bracketed by device
+    synchronisations on every rank and timed with CUDA events on the current
+    stream (the library's phases synchronise their own streams); the max over
+    ranks is reported."""
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    pkg = load_pkg()
+    W = WORKLOAD
+    x, q = make_bodies(args.n, W["seed"])
+    n = len(q)
+    a = pkg.Argument(P=W["P"], ncrit=W["ncrit"], images=W["images"], cycle=W["cycle"], x=(0.5, 0.5, 0.5),
+                     dipole_correction=0, divide_4pi=1, precision=pkg.FP32_MIXED, device=local)
+    f = pkg.LaplaceFMM(x, q, a)
+    f.shard(rank, world)
+    f.setup()
+    f.upload()
+    nb, nx = f.shard_sizes()
+    xbuf = torch.empty(nx, dtype=torch.float64, device="cuda")
+    phi = torch.empty(n, dtype=torch.float64, device="cuda")
+    grad = torch.empty((n, 3), dtype=torch.float64, device="cuda")
+
+    def step():
+        f.shard_upward(xbuf.data_ptr())
+        if world > 1:
+            dist.all_reduce(xbuf)
+            torch.cuda.synchronize()
+        f.shard_downward(xbuf.data_ptr(), phi.data_ptr(), grad.data_ptr())
+
+    for _ in range(args.warmup):
+        step()
+    ms = []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            f.flush_l2()
+            if world > 1:
+                dist.barrier()
+            torch.cuda.synchronize()
+            e0.record()
+            step()
+            torch.cuda.synchronize()
+            e1.record()
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+    t = max_over_ranks([float(np.mean(ms))], world, "cuda")[0]
+    f.close()
+    if rank == 0:
+        line = {"metric": METRIC, "value": n / (t * 1e-3), "unit": "particles/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": t, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "f32-mixed",
+                "data": "synthetic: uniform [0,1)^3, q~U[-1,1] net zero, seed 2",
+                "config": {"workload": "periodic KIFMM evaluation pass N=%d P=8 ncrit=256 images=3, sharded" % n,
+                           "N": n, "parallelism": "shard%d" % world, "bodies_rank0": nb,
+                           "exchange_bytes": 8 * nx, "l2": "256 MB flush between timed steps"},
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
 CONFIG_DATA = {
     "c3": "synthetic: 2^22 bodies in 64 Gaussian blobs (sigma 0.02, wrapped), q=+-1 net zero, seed 3",
     "c5": "synthetic: 200^3 rock-salt lattice jittered by U(+-0.1 spacing), q=(-1)^(i+j+k), seed 5",
@@ -659,11 +731,15 @@ def main():
     ap.add_argument("--ref-n", type=int, default=WORKLOAD["N"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-equal-error", action="store_true")
+    ap.add_argument("--shard", action="store_true",
+                    help="the pass sharded over the ranks (one all-reduce per pass) instead of replicas")
     ap.add_argument("--config", default="c2", choices=["c2", "c3", "c5"],
                     help="c2: the headline workload (default); c3, c5: the clustered and lattice configurations")
     args = ap.parse_args()
     if args.config != "c2":
         run_config(args)
+    elif args.shard and args.impl == "ours":
+        run_shard(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
