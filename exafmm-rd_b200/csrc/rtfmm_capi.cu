@@ -153,6 +153,7 @@ struct rtfmm_fmm {
   int* d_body_leaf = nullptr;
   int64_t* d_perm = nullptr;
   double *d_xin = nullptr, *d_qin = nullptr;
+  double *d_stage_x = nullptr, *d_stage_q = nullptr;  // rtfmm_b200_solve's host bodies on their way in
   LeafInfo* d_leaves = nullptr;
   double *d_qeq = nullptr, *d_pchk = nullptr, *d_leafvec = nullptr, *d_leafvec2 = nullptr, *d_y = nullptr;
   double *d_far_phi = nullptr, *d_far_grad = nullptr, *d_near_phi = nullptr, *d_near_grad = nullptr;
@@ -1657,19 +1658,31 @@ int rtfmm_b200_evaluate(rtfmm_fmm* f, const double* q, double* phi, double* grad
     if (rc) return rc;
   }
   CK(cudaSetDevice(f->dev));
-  int rc0 = ensure_host_bodies(f);
-  if (rc0) return rc0;
+  // New charges for positions already on the device go through a staging
+  // buffer, so d_qin keeps the set-up charges (which a later host-buffer
+  // call may fetch); otherwise the set-up charges or the first move of the
+  // positions need the host copies of the set-up bodies (fetched here after
+  // a device set-up, before d_qin is overwritten).
+  const bool staged = q && f->pos_on_device;
+  if (!staged) {
+    int rc0 = ensure_host_bodies(f);
+    if (rc0) return rc0;
+  } else {
+    int rc0 = dalloc(f, &f->d_stage_q, (size_t)n);
+    if (rc0) return rc0;
+  }
   // host -> device (input order), then into tree order on the device; the
   // positions move only on the first call after set-up.  The charges are
-  // checked on the host while they are copied; nothing reads d_qin before
-  // the check passes.
-  CK(cudaMemcpyAsync(f->d_qin, q ? q : f->q_in.data(), sizeof(double) * n, cudaMemcpyHostToDevice, f->s0));
+  // checked on the host while they are copied; nothing reads them before the
+  // check passes.
+  double* qdst = staged ? f->d_stage_q : f->d_qin;
+  CK(cudaMemcpyAsync(qdst, q ? q : f->q_in.data(), sizeof(double) * n, cudaMemcpyHostToDevice, f->s0));
   if (q && !finite_all(q, n)) {
     CK(cudaStreamSynchronize(f->s0));
     return fail(RTFMM_EINVAL, "non-finite charge");
   }
   if (f->pos_on_device) {
-    CK(launch_set_charges(f->d_body64, f->d_qin, f->d_perm, (int)n, f->s0));
+    CK(launch_set_charges(f->d_body64, qdst, f->d_perm, (int)n, f->s0));
   } else {
     CK(cudaMemcpyAsync(f->d_xin, f->h_xin, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, f->s0));
     CK(launch_gather_bodies(f->d_xin, f->d_qin, f->d_perm, (int)n, f->d_body64, f->s0));
@@ -1688,9 +1701,27 @@ int rtfmm_b200_evaluate(rtfmm_fmm* f, const double* q, double* phi, double* grad
   return RTFMM_OK;
 }
 
+// Bodies from which rtfmm_b200_solve builds the tree, lists and P2P tables on
+// the GPU (rtfmm_b200_setup_device, the same plan bit for bit); below it the
+// host set-up is quicker than the copies and launches.
+constexpr int64_t kSolveDeviceSetupMin = 1 << 16;
+
 int rtfmm_b200_solve(rtfmm_fmm* f, int64_t n, const double* x, const double* q, double* phi, double* grad) {
-  int rc = rtfmm_b200_setup(f, n, x, q);
-  if (rc) return rc;
+  if (!f) return fail(RTFMM_EINVAL, "null handle");
+  if (n >= kSolveDeviceSetupMin && f->shard_n == 1 && x && q) {
+    int rc = ensure_device(f);
+    if (rc) return rc;
+    // the input bodies through pooled staging buffers to the device set-up
+    if ((rc = dalloc(f, &f->d_stage_x, 3 * (size_t)n)) || (rc = dalloc(f, &f->d_stage_q, (size_t)n))) return rc;
+    CK(cudaMemcpyAsync(f->d_stage_x, x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, f->s0));
+    CK(cudaMemcpyAsync(f->d_stage_q, q, sizeof(double) * n, cudaMemcpyHostToDevice, f->s0));
+    CK(cudaStreamSynchronize(f->s0));
+    rc = rtfmm_b200_setup_device(f, n, f->d_stage_x, f->d_stage_q);
+    if (rc) return rc;
+  } else {
+    int rc = rtfmm_b200_setup(f, n, x, q);
+    if (rc) return rc;
+  }
   return rtfmm_b200_evaluate(f, q, phi, grad);
 }
 

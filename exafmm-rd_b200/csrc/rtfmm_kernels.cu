@@ -485,11 +485,19 @@ __global__ void __launch_bounds__(256)
   int pos = EMIT ? off[t] : 0;
   const int pend = EMIT ? off[t + 1] : 0;  // the count pass's total for t bounds the writes
   const int e1 = list_off[it.leaf + 1];
+  const unsigned mask = __activemask();
   for (int e = list_off[it.leaf]; e < e1; ++e) {
     const P2PSrc32 s = list[e];
-    const float rc = kCloseFrac * fmaxf(rt, (float)leaves[s.leaf].r);
+    const float rs = (float)leaves[s.leaf].r;
+    const float rc = kCloseFrac * fmaxf(rt, rs);
     const float rc2 = rc * rc;
     const float px = xt.x - s.dx, py = xt.y - s.dy, pz = xt.z - s.dz;
+    // the source leaf's box (half edge rs, a little margin for the FP32
+    // rounding of the positions) is farther than rc from every target of
+    // this warp: no close pair in it
+    const float bx = fmaxf(fabsf(px) - 1.001f * rs, 0.f), by = fmaxf(fabsf(py) - 1.001f * rs, 0.f),
+                bz = fmaxf(fabsf(pz) - 1.001f * rs, 0.f);
+    if (!__any_sync(mask, bx * bx + by * by + bz * bz < rc2)) continue;
     for (int k = 0; k < s.bnum; ++k) {
       const float4 b = body32[s.boff + k];
       const float dx = px - b.x, dy = py - b.y, dz = pz - b.z;

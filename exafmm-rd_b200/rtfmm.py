@@ -244,9 +244,14 @@ class LaplaceFMM:
         return phi, grad
 
     def solve(self):
-        """``LaplaceFMM::solve`` (fmm.cpp:13-81)."""
-        self.setup()
-        return self.evaluate()
+        """``LaplaceFMM::solve`` (fmm.cpp:13-81): rtfmm_b200_solve (set-up on
+        the GPU from 65536 bodies, else on the host; the same plan), then the
+        pass."""
+        phi = np.empty(self.n)
+        grad = np.empty((self.n, 3))
+        _check(lib().rtfmm_b200_solve(self._h, self.n, _ptr(self.x), _ptr(self.q), _ptr(phi), _ptr(grad)))
+        self._set_up = True
+        return phi, grad
 
     # -- device-resident timing -------------------------------------------------
     def upload(self):

@@ -138,7 +138,11 @@ int rtfmm_b200_setup_device(rtfmm_fmm* fmm, int64_t n, const double* x_dev, cons
  */
 int rtfmm_b200_evaluate(rtfmm_fmm* fmm, const double* q, double* phi, double* grad);
 
-/* setup + evaluate: replaces LaplaceFMM::solve() (3dpp/src/fmm.cpp:13-81). */
+/* setup + evaluate: replaces LaplaceFMM::solve() (3dpp/src/fmm.cpp:13-81).
+ * From 65536 bodies the set-up runs on the GPU (the bodies are copied to the
+ * device and rtfmm_b200_setup_device builds the tree, lists and P2P tables,
+ * the same plan bit for bit as rtfmm_b200_setup); below that, and on a
+ * sharded handle, on the host. */
 int rtfmm_b200_solve(rtfmm_fmm* fmm, int64_t n, const double* x, const double* q,
                      double* phi, double* grad);
 

@@ -214,3 +214,28 @@ def test_device_setup_at_c3_size(pkg):
     assert h.info() == d.info()
     h.close()
     d.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_solve_sets_up_on_the_gpu(pkg, precision):
+    """rtfmm_b200_solve (the drop-in for LaplaceFMM::solve) builds the tree,
+    lists and P2P tables on the GPU from 65536 bodies; its outputs equal the
+    host set-up's bit for bit, and the set-up's phases show the device build
+    (tree phase well under the host build's)."""
+    x, q = blobs(1 << 17, 4, 0.05, 80)
+    a = pkg.Argument(P=6, ncrit=64, images=3, cycle=1.0, x=(0.5, 0.5, 0.5), dipole_correction=0, divide_4pi=1,
+                     precision=precision)
+    f = pkg.LaplaceFMM(x, q, a)
+    phi, grad = f.solve()
+    g = pkg.LaplaceFMM(x, q, a)
+    g.setup()
+    rphi, rgrad = g.evaluate()
+    assert np.array_equal(phi, rphi) and np.array_equal(grad, rgrad)
+    # a second solve on the same handle with new charges
+    q2 = np.random.default_rng(81).standard_normal(len(q))
+    f.q = q2 - q2.mean()
+    phi2, grad2 = f.solve()
+    rphi2, rgrad2 = g.evaluate(f.q)
+    assert np.array_equal(phi2, rphi2) and np.array_equal(grad2, rgrad2)
+    f.close()
+    g.close()
