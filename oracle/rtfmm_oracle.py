@@ -594,7 +594,7 @@ class FMM:
             for k in range(c.cnum[t]):
                 ch = c.coff[t] + k
                 slot = 0 if c.octant[ch] == 13 else c.octant[ch]
-                g = np.fft.irfftn(pk[slot], s=(N, N, N))
+                g = np.fft.irfftn(pk[slot], s=(N, N, N), axes=(0, 1, 2))
                 self.p_check[ch] += g[o.down_idx] * scale
 
     def l2l(self, parents=None):
