@@ -503,9 +503,8 @@ def run_ours(args):
                   "peak_kind": "nominal 148 SM x 128 FMA/clk x 2 at the sampled SM clock"},
         "m2l_hadamard8": {"bound": "fp32", "work": had_flop, "ms": stage_serial["M2L_hadamard"],
                           "peak": fp32_peak, "unit": "TFLOP/s",
-                          "peak_kind": "nominal FP32 (the kernel is bound by L1 wavefronts of its coefficient "
-                                       "reads, 75% in ncu); against the measured HBM peak it moves %.0f MB"
-                                       % (had_bytes / 1e6)},
+                          "peak_kind": "nominal FP32 at the sampled SM clock; against the measured HBM peak "
+                                       "it moves %.0f MB" % (had_bytes / 1e6)},
     }
     for k, d in kern.items():
         scale = 1e12 if d["unit"] == "TFLOP/s" else 1e9
