@@ -189,7 +189,7 @@ struct rtfmm_fmm {
   // set-up wall times (s): tree, lists, operators (0 when cached), host
   // tables, the setup call, and the upload of the device tables (in the call
   // that did it)
-  double setup_s[6] = {0, 0, 0, 0, 0, 0};
+  double setup_s[12] = {};
   // the forward pass captured as a CUDA graph (launch_pass), dropped with
   // the device tables
   cudaGraphExec_t pass_graph = nullptr;
@@ -776,26 +776,34 @@ int upload_operators(rtfmm_fmm* f) {
   // y = (sum of M2M_img)^T x (B[j][n] = sum[j][n])
   RC(dupload(f, &f->d_B[B_ADJ_IMG_UP], o.l2l_img));
   RC(dupload(f, &f->d_B[B_ADJ_IMG_DOWN], o.m2m_img_sum));
-  // M2L: kernel spectra re-laid frequency-major, G[f][d][pair]
-  std::vector<double> g64(o.cc8.size());
-  for (int d = 0; d < 26; ++d)
-    for (int pr = 0; pr < 64; ++pr)
-      for (int fq = 0; fq < Nf; ++fq) {
-        const size_t from = (((size_t)d * 64 + pr) * Nf + fq) * 2;
-        const size_t to = (((size_t)fq * 26 + d) * 64 + pr) * 2;
-        g64[to] = o.cc8[from];
-        g64[to + 1] = o.cc8[from + 1];
+  // M2L: kernel spectra re-laid frequency-major, G[f][d][pair], on the GPU
+  // from a staging copy of cc8
+  {
+    double* stage = nullptr;
+    CK(cudaMalloc(&stage, sizeof(double) * std::max<size_t>(1, o.cc8.size())));
+    cudaError_t e = cudaMemcpy(stage, o.cc8.data(), sizeof(double) * o.cc8.size(), cudaMemcpyHostToDevice);
+    if (f->m2l32) {
+      float* gp = nullptr;
+      int rc = dalloc(f, &gp, o.cc8.size(), &f->d_G8);
+      if (rc) {
+        cudaFree(stage);
+        return rc;
       }
-  if (f->m2l32) {
-    std::vector<float> g(g64.size());
-    for (size_t i = 0; i < g.size(); ++i) g[i] = (float)g64[i];
-    float* gp;
-    RC(dupload(f, &gp, g, &f->d_G8));
-    f->d_G8 = gp;
-  } else {
-    double* gp;
-    RC(dupload(f, &gp, g64, &f->d_G8));
-    f->d_G8 = gp;
+      f->d_G8 = gp;
+      if (e == cudaSuccess) e = launch_g8_layout<float>(stage, Nf, gp, f->s0);
+    } else {
+      double* gp = nullptr;
+      int rc = dalloc(f, &gp, o.cc8.size(), &f->d_G8);
+      if (rc) {
+        cudaFree(stage);
+        return rc;
+      }
+      f->d_G8 = gp;
+      if (e == cudaSuccess) e = launch_g8_layout<double>(stage, Nf, gp, f->s0);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(f->s0);
+    cudaFree(stage);
+    CK(e);
   }
   RC(dupload(f, &f->d_G27, o.cc27sum));
 #undef RC
@@ -1369,9 +1377,6 @@ void ops_store(const Operators& o) {
 // 48..63.
 constexpr int kWalkSlots = 16;
 constexpr int kTableSlots = 48;
-// Surface points from which a device set-up builds its operators' dense
-// parts on the GPU (P >= 10).
-constexpr int kDenseGpuMinSurf = 480;
 
 // Lists (the P2P walk on the GPU with `gpu` scratch), operators (unless
 // cached for this P, images and radius) and host tables of the plan whose
@@ -1402,12 +1407,11 @@ void finish_setup(rtfmm_fmm* f, const TreeScratchFn* gpu = nullptr) {
     if (std::shared_ptr<const Operators> c = ops_lookup(f->args.P, f->args.images, f->plan.r0)) {
       f->ops = *c;
     } else {
-      // with a device set-up at P >= 10, the SVD sweeps and the M2M products
-      // run on the GPU (the same tables, bit for bit); below that the host's
-      // 16-core build is as fast
+      // with a device set-up, the SVD sweeps, the M2M products and the kernel
+      // spectra run on the GPU (the same tables, bit for bit)
       const DenseBackend be = gpu_dense_backend(f->s0);
-      const bool dense_gpu = gpu && surface_point_num(f->args.P) >= kDenseGpuMinSurf;
-      build_operators(f->ops, f->args.P, f->plan.r0, f->args.images, dense_gpu ? &be : nullptr);
+      build_operators(f->ops, f->args.P, f->plan.r0, f->args.images, gpu ? &be : nullptr);
+      for (int k = 0; k < 6; ++k) st[6 + k] = f->ops.build_s[k];
       ops_store(f->ops);
     }
     f->ops_valid = true;
@@ -1454,7 +1458,7 @@ void begin_setup(rtfmm_fmm* f, int64_t n) {
   f->plan = Plan();
   f->plan.args = f->args;
   f->plan.n = n;
-  for (int k = 0; k < 6; ++k) f->setup_s[k] = 0;
+  for (int k = 0; k < 12; ++k) f->setup_s[k] = 0;
 }
 
 void end_setup(rtfmm_fmm* f, double t0) {
@@ -1937,7 +1941,7 @@ int rtfmm_b200_flush_l2(rtfmm_fmm* f) {
 int rtfmm_b200_setup_times(rtfmm_fmm* f, double* s, int cap) {
   if (!f || !s) return fail(RTFMM_EINVAL, "null argument");
   if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");
-  for (int k = 0; k < 6 && k < cap; ++k) s[k] = f->setup_s[k];
+  for (int k = 0; k < 12 && k < cap; ++k) s[k] = f->setup_s[k];
   return RTFMM_OK;
 }
 
@@ -2105,6 +2109,10 @@ int rtfmm_b200_get_operator(rtfmm_fmm* f, int which, double* out, int64_t cap) {
     v = o.U;
   } else if (which == 5) {
     v = o.VSinv;
+  } else if (which == 6) {
+    v = o.cc27sum;
+  } else if (which == 7) {
+    v = o.l2l_img;
   } else {
     return fail(RTFMM_EINVAL, "unknown operator");
   }

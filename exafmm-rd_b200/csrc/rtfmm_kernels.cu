@@ -1276,6 +1276,21 @@ __global__ void __launch_bounds__(HadCfg<T>::THREADS, HadCfg<T>::MINB)
   }
 }
 
+// The 8x8 kernel spectra re-laid frequency-major for the Hadamard:
+// G[(f * 26 + d) * 64 + pair] = cc8[(d * 64 + pair) * Nf + f] (complex), in the
+// pass's precision (FP32 by round to nearest).
+template <typename T>
+__global__ void k_g8_layout(const double2* __restrict__ cc8, int Nf, T* __restrict__ G) {
+  const size_t total = (size_t)26 * 64 * Nf;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+    const int pr = (int)(e % 64), d = (int)((e / 64) % 26);
+    const size_t f = e / (64 * 26);
+    const double2 v = cc8[((size_t)d * 64 + pr) * Nf + f];
+    G[2 * e] = (T)v.x;
+    G[2 * e + 1] = (T)v.y;
+  }
+}
+
 // Hadamard 1x27 (hadamard_1x27 + c2c_1x27x1_AVX, kernel.cpp:1084-1138) for the
 // image levels, FP64; the 27 image spectra of a direction are pre-summed.
 __global__ void k_m2l_hadamard27(const double* __restrict__ Q, const double* __restrict__ G27,
@@ -1704,6 +1719,17 @@ cudaError_t launch_m2l_hadamard8(const T* Q, const T* G, const int* tsrcT, int n
   }
   return cudaGetLastError();
 }
+
+template <typename T>
+cudaError_t launch_g8_layout(const double* cc8, int Nf, T* G, cudaStream_t st) {
+  const size_t total = (size_t)26 * 64 * Nf;
+  if (total > 0)
+    k_g8_layout<T><<<(int)std::min<size_t>((total + 255) / 256, 148 * 16), 256, 0, st>>>(
+        reinterpret_cast<const double2*>(cc8), Nf, G);
+  return cudaGetLastError();
+}
+template cudaError_t launch_g8_layout<float>(const double*, int, float*, cudaStream_t);
+template cudaError_t launch_g8_layout<double>(const double*, int, double*, cudaStream_t);
 
 cudaError_t launch_m2l_hadamard27(const double* Q, const double* G27, const int* tsrc, int ntar, int nsrc,
                                   int Nf, double* Pk, cudaStream_t st) {

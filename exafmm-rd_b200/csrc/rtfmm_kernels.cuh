@@ -101,6 +101,9 @@ cudaError_t launch_m2l_up(const double* q_equiv, const int* items, int nitems, c
 template <typename T>
 cudaError_t launch_m2l_hadamard8(const T* Q, const T* G, const int* tsrcT /*[26][ntar]*/, int ntar, int nsrc,
                                  int Nf, T* Pk, cudaStream_t st);
+// G (frequency-major, the Hadamard's layout) from cc8 [d][pair][f] (device)
+template <typename T>
+cudaError_t launch_g8_layout(const double* cc8, int Nf, T* G, cudaStream_t st);
 cudaError_t launch_m2l_hadamard27(const double* Q, const double* G27 /*[d][f]*/, const int* tsrc /*[ntar][26]*/,
                                   int ntar, int nsrc, int Nf, double* Pk, cudaStream_t st);
 template <typename T>

@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -24,6 +25,10 @@
 namespace rtfmm_b200 {
 
 static const int kMaxDepth = 40;
+
+static double wall_now() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 
 // ---------------------------------------------------------------------------
 // octree: Tree::build_nonuniform_octree (3dpp/src/tree.cpp:102-188)
@@ -486,6 +491,37 @@ std::vector<int> jacobi_pairs(int n) {
   return out;
 }
 
+// The three inner products of a column pair in the order of a 32-lane warp:
+// lane l sums the terms i = l, l + 32, ... in order, then the lanes are
+// combined by the butterfly of a warp reduction (partner l ^ 16, l ^ 8, ...,
+// l ^ 1; FP addition commutes, so every lane ends with the same sum).
+void jacobi_dots(int n, const double* wp, const double* wq, double& alpha, double& beta, double& gamma) {
+  double a[32] = {}, b[32] = {}, g[32] = {};
+  int i0 = 0;
+  for (; i0 + 32 <= n; i0 += 32)
+    for (int l = 0; l < 32; ++l) {
+      a[l] += wp[i0 + l] * wp[i0 + l];
+      b[l] += wq[i0 + l] * wq[i0 + l];
+      g[l] += wp[i0 + l] * wq[i0 + l];
+    }
+  for (int l = 0; i0 + l < n; ++l) {
+    a[l] += wp[i0 + l] * wp[i0 + l];
+    b[l] += wq[i0 + l] * wq[i0 + l];
+    g[l] += wp[i0 + l] * wq[i0 + l];
+  }
+  // lanes l and l ^ o hold equal sums after each step, so lanes 0..o-1 carry
+  // all of them
+  for (int o = 16; o >= 1; o >>= 1)
+    for (int l = 0; l < o; ++l) {
+      a[l] = a[l] + a[l + o];
+      b[l] = b[l] + b[l + o];
+      g[l] = g[l] + g[l + o];
+    }
+  alpha = a[0];
+  beta = b[0];
+  gamma = g[0];
+}
+
 void jacobi_sweeps_host(int n, std::vector<double>& W, std::vector<double>& Vc) {
   const int m = n + (n & 1);
   const std::vector<int> pairs = jacobi_pairs(n);
@@ -499,12 +535,8 @@ void jacobi_sweeps_host(int n, std::vector<double>& W, std::vector<double>& Vc) 
         if (q >= n) continue;  // padding column
         double* wp = &W[(size_t)p * n];
         double* wq = &W[(size_t)q * n];
-        double alpha = 0, beta = 0, gamma = 0;
-        for (int i = 0; i < n; ++i) {
-          alpha += wp[i] * wp[i];
-          beta += wq[i] * wq[i];
-          gamma += wp[i] * wq[i];
-        }
+        double alpha, beta, gamma;
+        jacobi_dots(n, wp, wq, alpha, beta, gamma);
         if (alpha == 0.0 || beta == 0.0) continue;
         const double rel = std::fabs(gamma) / std::sqrt(alpha * beta);
         off_max = std::max(off_max, rel);
@@ -531,8 +563,40 @@ void jacobi_sweeps_host(int n, std::vector<double>& W, std::vector<double>& Vc) 
   }
 }
 
+// Classical Gram-Schmidt, two passes, on the rows of Q (n x n) in order:
+// row k loses its components along rows 0..k-1, then is normalised (a zero
+// row stays zero).  Every inner product runs over its index in order.
+void reorthogonalize_host(int n, double* Q) {
+  std::vector<double> h(n);
+  for (int k = 0; k < n; ++k) {
+    double* u = &Q[(size_t)k * n];
+    double nrm = 0;
+    for (int i = 0; i < n; ++i) nrm += u[i] * u[i];
+    if (nrm == 0.0) continue;  // s_k = 0: not inverted
+    for (int pass = 0; pass < 2; ++pass) {
+#pragma omp parallel for schedule(static)
+      for (int j = 0; j < k; ++j) {
+        const double* qj = &Q[(size_t)j * n];
+        double d = 0;
+        for (int i = 0; i < n; ++i) d += qj[i] * u[i];
+        h[j] = d;
+      }
+#pragma omp parallel for schedule(static)
+      for (int i = 0; i < n; ++i) {
+        double acc = 0;
+        for (int j = 0; j < k; ++j) acc += h[j] * Q[(size_t)j * n + i];
+        u[i] -= acc;
+      }
+    }
+    nrm = 0;
+    for (int i = 0; i < n; ++i) nrm += u[i] * u[i];
+    nrm = std::sqrt(nrm);
+    for (int i = 0; i < n; ++i) u[i] = nrm > 0 ? u[i] / nrm : 0.0;
+  }
+}
+
 void jacobi_svd(int n, const double* A, std::vector<double>& U, std::vector<double>& s, std::vector<double>& V,
-                const DenseBackend* be) {
+                const DenseBackend* be, const std::function<void()>& after_sweeps) {
   const int m = n + (n & 1);
   std::vector<double> W((size_t)m * n, 0.0), Vc((size_t)m * m, 0.0);
   for (int j = 0; j < n; ++j)
@@ -542,6 +606,7 @@ void jacobi_svd(int n, const double* A, std::vector<double>& U, std::vector<doub
     be->jacobi_sweeps(n, W, Vc);
   else
     jacobi_sweeps_host(n, W, Vc);
+  if (after_sweeps) after_sweeps();
   std::vector<std::pair<double, int>> sv(n);
   for (int j = 0; j < n; ++j) {
     double nr = 0;
@@ -570,34 +635,13 @@ void jacobi_svd(int n, const double* A, std::vector<double>& U, std::vector<doub
   // dgesvd) returns an orthonormal U; re-orthogonalise the columns in order
   // of decreasing s (classical Gram-Schmidt, two passes) to the same effect.
   // At P <= 8 this changes U by ~1e-15.
-  std::vector<double> Q((size_t)n * n), h(n);
+  std::vector<double> Q((size_t)n * n);
   for (int k = 0; k < n; ++k)
     for (int i = 0; i < n; ++i) Q[(size_t)k * n + i] = U[(size_t)i * n + k];
-  for (int k = 0; k < n; ++k) {
-    double* u = &Q[(size_t)k * n];
-    double nrm = 0;
-    for (int i = 0; i < n; ++i) nrm += u[i] * u[i];
-    if (nrm == 0.0) continue;  // s_k = 0: not inverted
-    for (int pass = 0; pass < 2; ++pass) {
-#pragma omp parallel for schedule(static)
-      for (int j = 0; j < k; ++j) {
-        const double* qj = &Q[(size_t)j * n];
-        double d = 0;
-        for (int i = 0; i < n; ++i) d += qj[i] * u[i];
-        h[j] = d;
-      }
-#pragma omp parallel for schedule(static)
-      for (int i = 0; i < n; ++i) {
-        double acc = 0;
-        for (int j = 0; j < k; ++j) acc += h[j] * Q[(size_t)j * n + i];
-        u[i] -= acc;
-      }
-    }
-    nrm = 0;
-    for (int i = 0; i < n; ++i) nrm += u[i] * u[i];
-    nrm = std::sqrt(nrm);
-    for (int i = 0; i < n; ++i) u[i] = nrm > 0 ? u[i] / nrm : 0.0;
-  }
+  if (be && be->reorthogonalize)
+    be->reorthogonalize(n, Q.data());
+  else
+    reorthogonalize_host(n, Q.data());
   for (int k = 0; k < n; ++k)
     for (int i = 0; i < n; ++i) U[(size_t)i * n + k] = Q[(size_t)k * n + i];
 }
@@ -697,6 +741,28 @@ static int hash_rel(int i, int j, int k) {
   return std::abs(i) * 1000 + std::abs(j) * 100 + std::abs(k) * 10 + signs;
 }
 
+// Kernel spectra (kernel.cpp:1721-1769): for each offset n (in units of the
+// parent edge 2 r0), the R2C DFT (dft3_r2c) of 1/|p - rel_n| sampled on the
+// N^3 convolution grid p = -gsize + (i, j, k) delta (0 where p = rel_n).
+void kernel_spectra_host(int N, int noff, const int* offs, double r0, double delta, double gsize, double* gk) {
+  const size_t Nf = (size_t)N * N * (N / 2 + 1);
+#pragma omp parallel for schedule(dynamic)
+  for (int n = 0; n < noff; ++n) {
+    std::vector<double> g((size_t)N * N * N);
+    const double rel[3] = {offs[3 * n] * r0 * 2, offs[3 * n + 1] * r0 * 2, offs[3 * n + 2] * r0 * 2};
+    for (int k = 0; k < N; ++k)
+      for (int j = 0; j < N; ++j)
+        for (int i = 0; i < N; ++i) {
+          const double px = (-gsize + i * delta) - rel[0];
+          const double py = (-gsize + j * delta) - rel[1];
+          const double pz = (-gsize + k * delta) - rel[2];
+          const double r = std::sqrt(px * px + py * py + pz * pz);
+          g[((size_t)k * N + j) * N + i] = r == 0 ? 0.0 : 1.0 / r;
+        }
+    dft3_r2c(N, g.data(), &gk[(size_t)n * Nf * 2]);
+  }
+}
+
 void build_operators(Operators& o, int P, double r0, int images, const DenseBackend* be) {
   auto matmul = [be](int n, const double* A, const double* B, double* C) {
     if (be && be->matmul)
@@ -726,12 +792,18 @@ void build_operators(Operators& o, int P, double r0, int images, const DenseBack
           o.surf_unit.push_back(-1.0 + j * 2.0 / (P - 1));
           o.surf_unit.push_back(-1.0 + k * 2.0 / (P - 1));
         }
+  double tb = wall_now();
+  auto lap = [&](int k) {
+    const double t = wall_now();
+    o.build_s[k] = t - tb;
+    tb = t;
+  };
   std::vector<double> xc, xe, e2c;
   surface(o, r0 * 2.95, V3{0, 0, 0}, xc);
   surface(o, r0 * 1.05, V3{0, 0, 0}, xe);
   p2p_matrix(ns, xc.data(), ns, xe.data(), e2c);
   std::vector<double> U, s, V;
-  jacobi_svd(ns, e2c.data(), U, s, V, be);
+  jacobi_svd(ns, e2c.data(), U, s, V, be, [&]() { lap(0); });
   // pseudo_inverse: drop singular values <= 4e-16 * s_max (mathfunc.cpp:154-169)
   double smax = 0;
   for (double v : s) smax = std::max(smax, std::fabs(v));
@@ -752,6 +824,7 @@ void build_operators(Operators& o, int P, double r0, int images, const DenseBack
   o.pinv_down.assign((size_t)ns * ns, 0);
   for (int i = 0; i < ns; ++i)
     for (int j = 0; j < ns; ++j) o.pinv_down[(size_t)i * ns + j] = o.pinv_up[(size_t)j * ns + i];
+  lap(1);
   // out_k = VSinv (UT G_k) for a batch of child check matrices G_k
   auto chain = [&](std::vector<std::vector<double>>& Gs, std::vector<std::vector<double>>& outs) {
     outs.assign(Gs.size(), std::vector<double>((size_t)ns * ns, 0.0));
@@ -783,6 +856,7 @@ void build_operators(Operators& o, int P, double r0, int images, const DenseBack
     chain(Gs, outs);
     for (int oc = 0; oc < 8; ++oc) o.m2m[oc].swap(outs[oc]);
   }
+  lap(2);
   // image M2M over the 27 children of a 3x3x3 super-cell (kernel.cpp:1671-1683)
   o.m2m_img_sum.assign((size_t)ns * ns, 0);
   o.l2l_img.assign((size_t)ns * ns, 0);
@@ -804,6 +878,7 @@ void build_operators(Operators& o, int P, double r0, int images, const DenseBack
           for (int j = 0; j < ns; ++j) o.l2l_img[(size_t)i * ns + j] = mi[(size_t)j * ns + i];
     }
   }
+  lap(3);
   // kernel spectra over every non-adjacent child offset (kernel.cpp:1721-1769)
   const int rng = images >= 2 ? 4 : 3;
   std::vector<std::array<int, 3>> offs;
@@ -816,21 +891,14 @@ void build_operators(Operators& o, int P, double r0, int images, const DenseBack
   std::vector<double> gk(offs.size() * (size_t)Nf * 2);
   const double delta = 2 * r0 / (P - 1) * 1.05;
   const double gsize = r0 * 2 * 1.05;
-#pragma omp parallel for schedule(dynamic)
-  for (int n = 0; n < (int)offs.size(); ++n) {
-    std::vector<double> g((size_t)N * N * N);
-    const double rel[3] = {offs[n][0] * r0 * 2, offs[n][1] * r0 * 2, offs[n][2] * r0 * 2};
-    for (int k = 0; k < N; ++k)
-      for (int j = 0; j < N; ++j)
-        for (int i = 0; i < N; ++i) {
-          const double px = (-gsize + i * delta) - rel[0];
-          const double py = (-gsize + j * delta) - rel[1];
-          const double pz = (-gsize + k * delta) - rel[2];
-          const double r = std::sqrt(px * px + py * py + pz * pz);
-          g[((size_t)k * N + j) * N + i] = r == 0 ? 0.0 : 1.0 / r;
-        }
-    dft3_r2c(N, g.data(), &gk[(size_t)n * Nf * 2]);
-  }
+  std::vector<int> offv(offs.size() * 3);
+  for (size_t n = 0; n < offs.size(); ++n)
+    for (int k = 0; k < 3; ++k) offv[3 * n + k] = offs[n][k];
+  if (be && be->spectra)
+    be->spectra(N, (int)offs.size(), offv.data(), r0, delta, gsize, gk.data());
+  else
+    kernel_spectra_host(N, (int)offs.size(), offv.data(), r0, delta, gsize, gk.data());
+  lap(4);
   // 8x8 sibling blocks per parent direction (kernel.cpp:1783-1811), stored
   // [d][isrc][itar][f]; adjacent child pairs stay zero.
   o.cc8.assign((size_t)26 * 64 * Nf * 2, 0.0);
@@ -840,6 +908,7 @@ void build_operators(Operators& o, int P, double r0, int images, const DenseBack
     for (int j = -1; j <= 1; ++j)
       for (int i = -1; i <= 1; ++i)
         if (i || j || k) dirs.push_back({i, j, k});
+#pragma omp parallel for schedule(static)
   for (d = 0; d < 26; ++d) {
     for (int isrc = 0; isrc < 8; ++isrc)
       for (int itar = 0; itar < 8; ++itar) {
@@ -866,6 +935,7 @@ void build_operators(Operators& o, int P, double r0, int images, const DenseBack
             for (int f = 0; f < 2 * Nf; ++f) o.cc27sum[(size_t)d * Nf * 2 + f] += gk[(size_t)g * Nf * 2 + f];
           }
   }
+  lap(5);
 }
 
 // ---------------------------------------------------------------------------

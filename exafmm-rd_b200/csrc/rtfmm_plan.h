@@ -54,6 +54,10 @@ struct Operators {
   std::vector<double> cc27sum;     // [d][f] complex: sum of the 27 image spectra
   std::vector<double> surf_unit;   // ns x 3 unit-cube surface points
   std::vector<int> surf_ijk;       // ns x 3 lattice coordinates (x,y,z)
+  // wall seconds of the build: SVD (surfaces, e2c, sweeps), Gram-Schmidt and
+  // pseudo-inverse, M2M products, image products, kernel spectra, the 8x8 and
+  // 1x27 blocks
+  double build_s[6] = {0, 0, 0, 0, 0, 0};
 };
 
 // Per-cell lists indexed by cell: a vector of vectors that reads like the
@@ -155,6 +159,9 @@ struct DenseBackend {
   // out[k] = A (B G[k]) for k < nG, each product as matmul
   std::function<void(int n, const double* A, const double* B, int nG, const double* const* G, double* const* out)>
       chain;
+  // as kernel_spectra_host and reorthogonalize_host
+  std::function<void(int N, int noff, const int* offs, double r0, double delta, double gsize, double* gk)> spectra;
+  std::function<void(int n, double* Q)> reorthogonalize;
 };
 
 // Operator tables.
@@ -168,13 +175,22 @@ std::string load_operators(Operators& ops, const std::string& path);
 // tournament: jacobi_pairs lists (p, q), p < q, for each of the m - 1
 // rounds of a sweep (m/2 pairs a round; q >= n is the padding column);
 // sweeps end when every pair's |gamma|/sqrt(alpha beta) is below kJacobiTol
-// or after kJacobiMaxSweeps.
+// or after kJacobiMaxSweeps.  The inner products alpha, beta, gamma of a pair
+// are summed as a 32-lane warp sums them (jacobi_dots), so that the GPU
+// sweeps give the same rotations bit for bit.
 constexpr double kJacobiTol = 1e-15;
 constexpr int kJacobiMaxSweeps = 40;
 std::vector<int> jacobi_pairs(int n);
+void jacobi_dots(int n, const double* wp, const double* wq, double& alpha, double& beta, double& gamma);
 void jacobi_sweeps_host(int n, std::vector<double>& W, std::vector<double>& Vc);
+// Gram-Schmidt (two passes) of the rows of Q (n x n, row-major) in order
+void reorthogonalize_host(int n, double* Q);
+// gk[n] (N*N*(N/2+1) complex) = DFT of 1/|p - 2 r0 offs[n]| on the grid
+// p = -gsize + (i, j, k) delta, i, j, k < N
+void kernel_spectra_host(int N, int noff, const int* offs, double r0, double delta, double gsize, double* gk);
+// after_sweeps (if set) runs when the sweeps are done
 void jacobi_svd(int n, const double* A, std::vector<double>& U, std::vector<double>& s, std::vector<double>& V,
-                const DenseBackend* be = nullptr);
+                const DenseBackend* be = nullptr, const std::function<void()>& after_sweeps = nullptr);
 // C = A B, each C[i][j] summed over k in order (multiply, then add)
 void matmul_host(int n, const double* A, const double* B, double* C);
 void dft3_r2c(int N, const double* in, double* out);  // out: N*N*(N/2+1) complex

@@ -1,18 +1,22 @@
-// Dense kernels of the operator build on the GPU (LaplaceKernel::precompute,
-// 3dpp/src/kernel.cpp:1638-1683): the one-sided Jacobi sweeps of the SVD of
-// the equivalent-to-check operator and the products VSinv (UT G) of the M2M
-// and image-M2M operators.
+// Dense kernels of the operator build on the GPU (LaplaceKernel::precompute
+// and precompute_m2l, 3dpp/src/kernel.cpp:1638-1769): the one-sided Jacobi
+// sweeps of the SVD of the equivalent-to-check operator, the products
+// VSinv (UT G) of the M2M and image-M2M operators, and the kernel spectra of
+// the FFT-M2L.  (The Gram-Schmidt pass over the left singular vectors, a
+// chain of n dependent steps, stays on the host cores, which run it faster.)
 //
-// Both give the host's results bit for bit, so an operator set built here
+// All give the host's results bit for bit, so an operator set built here
 // equals one built by the host.  Every floating-point operation is the
 // host's, in the host's order, with rounding to nearest and no contraction
-// (__dmul_rn, __dadd_rn, __ddiv_rn, __dsqrt_rn): dot products and matrix
-// sums run sequentially over their index in one thread, and only
-// independent element updates are spread over threads.  The host code they
-// mirror is jacobi_sweeps_host and matmul_host (rtfmm_plan.cpp).
+// (__dmul_rn, __dadd_rn, __ddiv_rn, __dsqrt_rn): sums run sequentially over
+// their index in one thread, except the Jacobi inner products, which the host
+// sums in a warp's order (jacobi_dots), and only independent element updates
+// are spread over threads.  The host code they mirror is jacobi_sweeps_host,
+// matmul_host and kernel_spectra_host (rtfmm_plan.cpp).
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -20,71 +24,207 @@
 
 #include "rtfmm_precompute.h"
 
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
 namespace rtfmm_b200 {
 namespace {
 
-constexpr int kRoundThreads = 128;
+constexpr int kRoundWarps = 4;
 
-// One round of the tournament: block b rotates the column pair
-// (pairs[2b], pairs[2b+1]) of W (n rows) and Vc (m rows, first n updated).
-__global__ void __launch_bounds__(kRoundThreads) k_jacobi_round(double* __restrict__ W, double* __restrict__ Vc,
-                                                               int n, int m, const int* __restrict__ pairs,
-                                                               unsigned long long* __restrict__ off_bits) {
-  extern __shared__ double col[];  // 2n: columns p and q of W
-  __shared__ double cs[2];
-  __shared__ int go;
-  const int p = pairs[2 * blockIdx.x], q = pairs[2 * blockIdx.x + 1];
-  if (q >= n) return;  // the padding column
-  double* sp = col;
-  double* sq = col + n;
+// The rotation of column pair (p, q) of W (n rows) and Vc (m rows, first n
+// updated) by one warp.  Lane l sums the terms i = l, l + 32, ... of the three
+// inner products in order, then the butterfly combines the lanes
+// (jacobi_dots); every lane forms the same rotation.  The pair's
+// |gamma|/sqrt(alpha beta) goes into *off_bits (a maximum of non-negative
+// doubles taken on their bit patterns).
+__device__ __forceinline__ void jacobi_pair(double* __restrict__ W, double* __restrict__ Vc, int n, int m, int p,
+                                            int q, unsigned long long* __restrict__ off_bits) {
+  const int lane = threadIdx.x & 31;
   double* wp = W + (size_t)p * n;
   double* wq = W + (size_t)q * n;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    sp[i] = wp[i];
-    sq[i] = wq[i];
+  double alpha = 0, beta = 0, gamma = 0;
+  for (int i = lane; i < n; i += 32) {
+    const double a = wp[i], b = wq[i];
+    alpha = __dadd_rn(alpha, __dmul_rn(a, a));
+    beta = __dadd_rn(beta, __dmul_rn(b, b));
+    gamma = __dadd_rn(gamma, __dmul_rn(a, b));
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double alpha = 0, beta = 0, gamma = 0;
-    // in order over i (the host's sum); unrolled so the shared-memory loads
-    // run ahead of the three dependent chains of adds
-#pragma unroll 8
-    for (int i = 0; i < n; ++i) {
-      alpha = __dadd_rn(alpha, __dmul_rn(sp[i], sp[i]));
-      beta = __dadd_rn(beta, __dmul_rn(sq[i], sq[i]));
-      gamma = __dadd_rn(gamma, __dmul_rn(sp[i], sq[i]));
-    }
-    go = 0;
-    if (!(alpha == 0.0 || beta == 0.0)) {
-      const double rel = __ddiv_rn(fabs(gamma), __dsqrt_rn(__dmul_rn(alpha, beta)));
-      // rel >= 0, so its bit pattern orders as its value (a NaN, which the
-      // host's std::max would drop, is left out)
-      if (!isnan(rel)) atomicMax(off_bits, (unsigned long long)__double_as_longlong(rel));
-      if (!(rel < kJacobiTol)) {
-        const double zeta = __ddiv_rn(__dsub_rn(beta, alpha), __dmul_rn(2.0, gamma));
-        const double t = __ddiv_rn(zeta >= 0 ? 1.0 : -1.0,
-                                   __dadd_rn(fabs(zeta), __dsqrt_rn(__dadd_rn(1.0, __dmul_rn(zeta, zeta)))));
-        const double c = __ddiv_rn(1.0, __dsqrt_rn(__dadd_rn(1.0, __dmul_rn(t, t))));
-        cs[0] = c;
-        cs[1] = __dmul_rn(c, t);
-        go = 1;
-      }
-    }
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) {
+    alpha = __dadd_rn(alpha, __shfl_xor_sync(0xffffffffu, alpha, o));
+    beta = __dadd_rn(beta, __shfl_xor_sync(0xffffffffu, beta, o));
+    gamma = __dadd_rn(gamma, __shfl_xor_sync(0xffffffffu, gamma, o));
   }
-  __syncthreads();
-  if (!go) return;
-  const double c = cs[0], sn = cs[1];
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const double a1 = sp[i], b1 = sq[i];
+  if (alpha == 0.0 || beta == 0.0) return;
+  const double rel = __ddiv_rn(fabs(gamma), __dsqrt_rn(__dmul_rn(alpha, beta)));
+  // a NaN, which the host's std::max would drop, is left out
+  if (lane == 0 && !isnan(rel)) atomicMax(off_bits, (unsigned long long)__double_as_longlong(rel));
+  if (rel < kJacobiTol) return;
+  const double zeta = __ddiv_rn(__dsub_rn(beta, alpha), __dmul_rn(2.0, gamma));
+  const double t =
+      __ddiv_rn(zeta >= 0 ? 1.0 : -1.0, __dadd_rn(fabs(zeta), __dsqrt_rn(__dadd_rn(1.0, __dmul_rn(zeta, zeta)))));
+  const double c = __ddiv_rn(1.0, __dsqrt_rn(__dadd_rn(1.0, __dmul_rn(t, t))));
+  const double sn = __dmul_rn(c, t);
+  for (int i = lane; i < n; i += 32) {
+    const double a1 = wp[i], b1 = wq[i];
     wp[i] = __dsub_rn(__dmul_rn(c, a1), __dmul_rn(sn, b1));
     wq[i] = __dadd_rn(__dmul_rn(sn, a1), __dmul_rn(c, b1));
   }
   double* vp = Vc + (size_t)p * m;
   double* vq = Vc + (size_t)q * m;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+  for (int i = lane; i < n; i += 32) {
     const double a1 = vp[i], b1 = vq[i];
     vp[i] = __dsub_rn(__dmul_rn(c, a1), __dmul_rn(sn, b1));
     vq[i] = __dadd_rn(__dmul_rn(sn, a1), __dmul_rn(c, b1));
+  }
+}
+
+// One round of the tournament: warp w of block b rotates the pair
+// pairs[2k], pairs[2k+1], k = 4 b + w.
+__global__ void __launch_bounds__(32 * kRoundWarps) k_jacobi_round(double* __restrict__ W, double* __restrict__ Vc,
+                                                                  int n, int m, const int* __restrict__ pairs,
+                                                                  unsigned long long* __restrict__ off_bits) {
+  const int k = blockIdx.x * kRoundWarps + (threadIdx.x >> 5);
+  if (k >= m / 2) return;  // warp-uniform
+  const int p = pairs[2 * k], q = pairs[2 * k + 1];
+  if (q >= n) return;  // the padding column
+  jacobi_pair(W, Vc, n, m, p, q, off_bits);
+}
+
+// Spins of a block at the grid barrier before it gives up (the blocks of a
+// cooperative launch are all resident, so the barrier only gives up when
+// something else has gone wrong).
+constexpr long long kBarrierSpins = 1ll << 24;
+
+// Grid-wide barrier of a cooperative launch: bar[0] counts arrivals, bar[1]
+// is the generation.  A block that waits kBarrierSpins in vain sets *err and
+// leaves; returns false when *err is set.
+__device__ bool grid_barrier(unsigned* bar, int* err) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* gen = bar + 1;
+    const unsigned g = *gen;
+    __threadfence();
+    if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+      bar[0] = 0;
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      long long it = 0;
+      while (*gen == g)
+        if (++it > kBarrierSpins) {
+          atomicExch(err, 1);
+          break;
+        }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return *(volatile int*)err == 0;
+}
+
+// Every sweep in one cooperative launch: the warps of the grid take the
+// pairs of a round in turn, a grid barrier separates the rounds, and after a
+// sweep's last round every block reads the sweep's maximum and stops when it
+// is below the tolerance.  off_bits[s & 1] collects sweep s (the other slot
+// is cleared for the next sweep once all blocks have read it).  status[0] =
+// sweeps run, status[1] = 1 if a barrier gave up.
+__global__ void __launch_bounds__(32 * kRoundWarps) k_jacobi_sweeps(double* __restrict__ W, double* __restrict__ Vc,
+                                                                   int n, int m, const int* __restrict__ pairs,
+                                                                   unsigned long long* __restrict__ off_bits,
+                                                                   unsigned* __restrict__ bar, int* __restrict__ status) {
+  const int nw = gridDim.x * kRoundWarps;
+  const int w = blockIdx.x * kRoundWarps + (threadIdx.x >> 5);
+  int sweep = 0;
+  for (; sweep < kJacobiMaxSweeps; ++sweep) {
+    unsigned long long* ob = off_bits + (sweep & 1);
+    for (int round = 0; round < m - 1; ++round) {
+      const int* pr = pairs + (size_t)round * m;
+      for (int k = w; k < m / 2; k += nw) {
+        const int p = pr[2 * k], q = pr[2 * k + 1];
+        if (q < n) jacobi_pair(W, Vc, n, m, p, q, ob);
+      }
+      if (!grid_barrier(bar, status + 1)) return;
+    }
+    const unsigned long long bits = *(volatile unsigned long long*)ob;
+    if (blockIdx.x == 0 && threadIdx.x == 0) off_bits[(sweep + 1) & 1] = 0;
+    if (__longlong_as_double((long long)bits) < kJacobiTol) {
+      ++sweep;
+      break;
+    }
+    if (!grid_barrier(bar, status + 1)) return;  // every block has read the maximum
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) status[0] = sweep;
+}
+
+// Kernel spectra (kernel_spectra_host): block b takes offset b; the grid of
+// 1/r and the two intermediate passes of the separable DFT live in the
+// block's scratch (N^3 + 2 * 2 N^2 Nh doubles).  Thread per output, each sum
+// sequential over its index as in dft3_r2c; cs/sn are the host's twiddles.
+__global__ void __launch_bounds__(256) k_kernel_spectra(int N, const int* __restrict__ offs, double r0,
+                                                        double delta, double gsize, const double* __restrict__ cs,
+                                                        const double* __restrict__ sn, double* __restrict__ scratch,
+                                                        double* __restrict__ gk) {
+  const int Nh = N / 2 + 1;
+  const size_t N3 = (size_t)N * N * N, Nc = (size_t)N * N * Nh;
+  double* g = scratch + (size_t)blockIdx.x * (N3 + 4 * Nc);
+  double* a = g + N3;
+  double* b = a + 2 * Nc;
+  double* out = gk + (size_t)blockIdx.x * 2 * Nc;
+  const int* o = offs + 3 * blockIdx.x;
+  const double rel0 = __dmul_rn(__dmul_rn((double)o[0], r0), 2.0);
+  const double rel1 = __dmul_rn(__dmul_rn((double)o[1], r0), 2.0);
+  const double rel2 = __dmul_rn(__dmul_rn((double)o[2], r0), 2.0);
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (size_t e = tid; e < N3; e += nt) {
+    const int i = (int)(e % N), j = (int)((e / N) % N), k = (int)(e / ((size_t)N * N));
+    const double px = __dsub_rn(__dadd_rn(-gsize, __dmul_rn((double)i, delta)), rel0);
+    const double py = __dsub_rn(__dadd_rn(-gsize, __dmul_rn((double)j, delta)), rel1);
+    const double pz = __dsub_rn(__dadd_rn(-gsize, __dmul_rn((double)k, delta)), rel2);
+    const double r = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(px, px), __dmul_rn(py, py)), __dmul_rn(pz, pz)));
+    g[e] = r == 0 ? 0.0 : __ddiv_rn(1.0, r);
+  }
+  __syncthreads();
+  for (size_t e = tid; e < Nc; e += nt) {  // x -> kx: e = (z N + y) Nh + kx
+    const int kx = (int)(e % Nh);
+    const size_t zy = e / Nh;
+    double re = 0, im = 0;
+    for (int x = 0; x < N; ++x) {
+      const int t = (kx * x) % N;
+      const double v = g[zy * N + x];
+      re = __dadd_rn(re, __dmul_rn(v, cs[t]));
+      im = __dadd_rn(im, __dmul_rn(v, sn[t]));
+    }
+    a[2 * e] = re;
+    a[2 * e + 1] = im;
+  }
+  __syncthreads();
+  for (size_t e = tid; e < Nc; e += nt) {  // y -> ky: e = (z N + ky) Nh + kx
+    const int kx = (int)(e % Nh), ky = (int)((e / Nh) % N), z = (int)(e / ((size_t)N * Nh));
+    double re = 0, im = 0;
+    for (int y = 0; y < N; ++y) {
+      const int t = (ky * y) % N;
+      const size_t s = ((size_t)z * N + y) * Nh + kx;
+      re = __dadd_rn(re, __dsub_rn(__dmul_rn(a[2 * s], cs[t]), __dmul_rn(a[2 * s + 1], sn[t])));
+      im = __dadd_rn(im, __dadd_rn(__dmul_rn(a[2 * s], sn[t]), __dmul_rn(a[2 * s + 1], cs[t])));
+    }
+    b[2 * e] = re;
+    b[2 * e + 1] = im;
+  }
+  __syncthreads();
+  for (size_t e = tid; e < Nc; e += nt) {  // z -> kz: e = (kz N + ky) Nh + kx
+    const int kx = (int)(e % Nh), ky = (int)((e / Nh) % N), kz = (int)(e / ((size_t)N * Nh));
+    double re = 0, im = 0;
+    for (int z = 0; z < N; ++z) {
+      const int t = (kz * z) % N;
+      const size_t s = ((size_t)z * N + ky) * Nh + kx;
+      re = __dadd_rn(re, __dsub_rn(__dmul_rn(b[2 * s], cs[t]), __dmul_rn(b[2 * s + 1], sn[t])));
+      im = __dadd_rn(im, __dadd_rn(__dmul_rn(b[2 * s], sn[t]), __dmul_rn(b[2 * s + 1], cs[t])));
+    }
+    out[2 * e] = re;
+    out[2 * e + 1] = im;
   }
 }
 
@@ -132,12 +272,21 @@ void launch_matmul(int n, const double* A, const double* B, double* C, cudaStrea
 
 }  // namespace
 
-void jacobi_sweeps_gpu(int n, std::vector<double>& W, std::vector<double>& Vc, cudaStream_t st) {
+// A captured CUDA graph and its executable, released together.
+struct Graph {
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t x = nullptr;
+  ~Graph() {
+    if (x) cudaGraphExecDestroy(x);
+    if (g) cudaGraphDestroy(g);
+  }
+};
+
+int jacobi_sweeps_gpu(int n, std::vector<double>& W, std::vector<double>& Vc, cudaStream_t st) {
   const int m = n + (n & 1);
-  const size_t smem = sizeof(double) * 2 * (size_t)n;
-  if (n < 2 || smem > 48 * 1024) {  // beyond one block's default shared memory: the host sweeps
+  if (n < 2) {
     jacobi_sweeps_host(n, W, Vc);
-    return;
+    return -1;
   }
   const std::vector<int> pairs = jacobi_pairs(n);
   Buf bw, bv, bp, bo;
@@ -148,22 +297,98 @@ void jacobi_sweeps_gpu(int n, std::vector<double>& W, std::vector<double>& Vc, c
   check(cudaMemcpyAsync(dW, W.data(), sizeof(double) * W.size(), cudaMemcpyHostToDevice, st), "upload W");
   check(cudaMemcpyAsync(dV, Vc.data(), sizeof(double) * Vc.size(), cudaMemcpyHostToDevice, st), "upload V");
   check(cudaMemcpyAsync(dP, pairs.data(), sizeof(int) * pairs.size(), cudaMemcpyHostToDevice, st), "upload pairs");
-  for (int sweep = 0; sweep < kJacobiMaxSweeps; ++sweep) {
-    check(cudaMemsetAsync(dO, 0, sizeof(unsigned long long), st), "memset");
-    for (int round = 0; round < m - 1; ++round) {
-      k_jacobi_round<<<m / 2, kRoundThreads, smem, st>>>(dW, dV, n, m, dP + (size_t)round * m, dO);
-      check(cudaGetLastError(), "k_jacobi_round");
+  // all sweeps in one cooperative launch (its blocks all resident, so its
+  // grid barriers can wait); a launch that is refused or a barrier that gives
+  // up leaves it to the graph below, from the same inputs
+  bool done = false;
+  int sweeps_run = -1;
+  {
+    int dev = 0, nsm = 0, per = 0, coop = 0;
+    check(cudaGetDevice(&dev), "device");
+    check(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev), "attribute");
+    check(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "attribute");
+    check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_jacobi_sweeps, 32 * kRoundWarps, 0), "occupancy");
+    const int nblk = std::min((m / 2 + kRoundWarps - 1) / kRoundWarps, nsm * per);
+    if (coop && nblk >= 1) {
+      Buf baux;
+      unsigned long long* aux = baux.get<unsigned long long>(4);  // off_bits[2], bar[2], status[2]
+      check(cudaMemsetAsync(aux, 0, sizeof(unsigned long long) * 4, st), "memset");
+      unsigned long long* ob = aux;
+      unsigned* bar = reinterpret_cast<unsigned*>(aux + 2);
+      int* status = reinterpret_cast<int*>(aux + 3);
+      int nn = n, mm = m;
+      void* args[] = {&dW, &dV, &nn, &mm, &dP, &ob, &bar, &status};
+      cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_jacobi_sweeps, dim3(nblk), dim3(32 * kRoundWarps),
+                                                  args, 0, st);
+      int hs[2] = {0, 0};
+      if (e == cudaSuccess) e = cudaMemcpyAsync(hs, status, sizeof(hs), cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (e == cudaSuccess && hs[1] == 0) {
+        done = true;
+        sweeps_run = hs[0];
+      } else if (e == cudaErrorCooperativeLaunchTooLarge || e == cudaErrorNotSupported || e == cudaSuccess) {
+        cudaGetLastError();  // refused launch or a barrier that gave up: the graph path
+        check(cudaMemcpyAsync(dW, W.data(), sizeof(double) * W.size(), cudaMemcpyHostToDevice, st), "upload W");
+        check(cudaMemcpyAsync(dV, Vc.data(), sizeof(double) * Vc.size(), cudaMemcpyHostToDevice, st), "upload V");
+      } else {
+        check(e, "k_jacobi_sweeps");
+      }
     }
-    unsigned long long bits = 0;
-    check(cudaMemcpyAsync(&bits, dO, sizeof(bits), cudaMemcpyDeviceToHost, st), "off_max");
-    check(cudaStreamSynchronize(st), "sweep");
-    double off_max;
-    std::memcpy(&off_max, &bits, sizeof(off_max));
-    if (off_max < kJacobiTol) break;
+  }
+  if (!done) {
+    // one sweep (the off-diagonal maximum cleared, then m - 1 rounds) as a
+    // graph, replayed until the sweep leaves every pair below the tolerance
+    Graph sweep;
+    const int nblk = (m / 2 + kRoundWarps - 1) / kRoundWarps;
+    check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "capture");
+    cudaError_t e = cudaMemsetAsync(dO, 0, sizeof(unsigned long long), st);
+    for (int round = 0; round < m - 1 && e == cudaSuccess; ++round) {
+      k_jacobi_round<<<nblk, 32 * kRoundWarps, 0, st>>>(dW, dV, n, m, dP + (size_t)round * m, dO);
+      e = cudaGetLastError();
+    }
+    const cudaError_t ec = cudaStreamEndCapture(st, &sweep.g);
+    check(e, "k_jacobi_round");
+    check(ec, "end capture");
+    check(cudaGraphInstantiate(&sweep.x, sweep.g, 0), "instantiate");
+    for (int s = 0; s < kJacobiMaxSweeps; ++s) {
+      check(cudaGraphLaunch(sweep.x, st), "sweep");
+      unsigned long long bits = 0;
+      check(cudaMemcpyAsync(&bits, dO, sizeof(bits), cudaMemcpyDeviceToHost, st), "off_max");
+      check(cudaStreamSynchronize(st), "sweep");
+      double off_max;
+      std::memcpy(&off_max, &bits, sizeof(off_max));
+      if (off_max < kJacobiTol) break;
+    }
   }
   check(cudaMemcpyAsync(W.data(), dW, sizeof(double) * W.size(), cudaMemcpyDeviceToHost, st), "download W");
   check(cudaMemcpyAsync(Vc.data(), dV, sizeof(double) * Vc.size(), cudaMemcpyDeviceToHost, st), "download V");
   check(cudaStreamSynchronize(st), "download");
+  return sweeps_run;
+}
+
+void kernel_spectra_gpu(int N, int noff, const int* offs, double r0, double delta, double gsize, double* gk,
+                        cudaStream_t st) {
+  if (noff <= 0) return;
+  const size_t N3 = (size_t)N * N * N, Nc = (size_t)N * N * (N / 2 + 1);
+  // the host's twiddles (dft3_r2c)
+  std::vector<double> cs(N), sn(N);
+  for (int m = 0; m < N; ++m) {
+    cs[m] = std::cos(2.0 * M_PI * m / N);
+    sn[m] = -std::sin(2.0 * M_PI * m / N);
+  }
+  Buf bo, bc, bs, bw, bg;
+  int* dOff = bo.get<int>(3 * (size_t)noff);
+  double* dcs = bc.get<double>(N);
+  double* dsn = bs.get<double>(N);
+  double* dW = bw.get<double>((N3 + 4 * Nc) * noff);
+  double* dG = bg.get<double>(2 * Nc * noff);
+  check(cudaMemcpyAsync(dOff, offs, sizeof(int) * 3 * noff, cudaMemcpyHostToDevice, st), "upload offsets");
+  check(cudaMemcpyAsync(dcs, cs.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st), "upload twiddles");
+  check(cudaMemcpyAsync(dsn, sn.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st), "upload twiddles");
+  k_kernel_spectra<<<noff, 256, 0, st>>>(N, dOff, r0, delta, gsize, dcs, dsn, dW, dG);
+  check(cudaGetLastError(), "k_kernel_spectra");
+  check(cudaMemcpyAsync(gk, dG, sizeof(double) * 2 * Nc * noff, cudaMemcpyDeviceToHost, st), "download spectra");
+  check(cudaStreamSynchronize(st), "spectra");
 }
 
 void matmul_gpu(int n, const double* A, const double* B, double* C, cudaStream_t st) {
@@ -203,11 +428,17 @@ void chain_gpu(int n, const double* A, const double* B, int nG, const double* co
 
 DenseBackend gpu_dense_backend(cudaStream_t st) {
   DenseBackend be;
-  be.jacobi_sweeps = [st](int n, std::vector<double>& W, std::vector<double>& Vc) { jacobi_sweeps_gpu(n, W, Vc, st); };
+  be.jacobi_sweeps = [st](int n, std::vector<double>& W, std::vector<double>& Vc) {
+    (void)jacobi_sweeps_gpu(n, W, Vc, st);
+  };
   be.matmul = [st](int n, const double* A, const double* B, double* C) { matmul_gpu(n, A, B, C, st); };
   be.chain = [st](int n, const double* A, const double* B, int nG, const double* const* G, double* const* out) {
     chain_gpu(n, A, B, nG, G, out, st);
   };
+  be.spectra = [st](int N, int noff, const int* offs, double r0, double delta, double gsize, double* gk) {
+    kernel_spectra_gpu(N, noff, offs, r0, delta, gsize, gk, st);
+  };
+
   return be;
 }
 

@@ -348,10 +348,12 @@ class LaplaceFMM:
     def setup_times(self):
         """Wall seconds of the last set-up's phases: tree, lists, operators
         (0 when cached), host tables, the setup call, and the upload of the
-        device tables."""
-        v = np.zeros(6)
-        _check(lib().rtfmm_b200_setup_times(self._h, _ptr(v), 6))
-        return dict(zip(("tree", "lists", "operators", "tables", "total", "upload"), v.tolist()))
+        device tables; then the operator build's parts (0 when cached): SVD,
+        Gram-Schmidt, M2M products, image products, kernel spectra, blocks."""
+        v = np.zeros(12)
+        _check(lib().rtfmm_b200_setup_times(self._h, _ptr(v), 12))
+        return dict(zip(("tree", "lists", "operators", "tables", "total", "upload", "ops_svd", "ops_orth",
+                         "ops_m2m", "ops_img", "ops_spectra", "ops_blocks"), v.tolist()))
 
     def info(self):
         v = np.zeros(13, dtype=np.int64)

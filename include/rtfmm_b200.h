@@ -271,9 +271,12 @@ int rtfmm_b200_flush_l2(rtfmm_fmm* fmm);
  * interaction lists, s[2] operator tables (0 when the handle's cached tables
  * were reused), s[3] host tables of the pass, s[4] the whole setup call,
  * s[5] the upload of the device tables (done by rtfmm_b200_setup_device, or
- * by the first upload/evaluate after rtfmm_b200_setup).  The reference times
- * the same phases separately from the evaluation (3dpp/src/fmm.cpp:13-50).
- * Writes min(cap, 6) values. */
+ * by the first upload/evaluate after rtfmm_b200_setup).  s[6..11] split s[2]
+ * when the tables were built in this set-up (else 0): the SVD (surfaces,
+ * check matrix, Jacobi sweeps), the Gram-Schmidt pass and pseudo-inverse,
+ * the M2M products, the image products, the kernel spectra, and their 8x8
+ * and 1x27 blocks.  The reference times the same phases separately from the
+ * evaluation (3dpp/src/fmm.cpp:13-50).  Writes min(cap, 12) values. */
 int rtfmm_b200_setup_times(rtfmm_fmm* fmm, double* s, int cap);
 
 /* Tree and list sizes.  info[0..11] = ncell (incl. image cells), nleaf,
@@ -323,7 +326,9 @@ int rtfmm_b200_get_cell_vectors(rtfmm_fmm* fmm, int which, double* out);
  *            (ns*ns),  3: 8x8 kernel spectra (26*8*8*Nfreq complex, as
  *            interleaved re,im),  4: U and 5: V S^-1 of the SVD
  *            e2c = U S V^T with the pseudo-inverted S (UT_p2m_precompute^T
- *            and VSinv_p2m_precompute, kernel.h:197-200), row-major ns*ns. */
+ *            and VSinv_p2m_precompute, kernel.h:197-200), row-major ns*ns,
+ *         6: 1x27 image kernel spectra summed over the 27 copies
+ *            (26*Nfreq complex),  7: the centre image L2L (ns*ns). */
 int rtfmm_b200_get_operator(rtfmm_fmm* fmm, int which, double* out, int64_t cap);
 
 /* ---- P2M that allocates no device memory ----

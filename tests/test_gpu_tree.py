@@ -173,11 +173,11 @@ def test_resetup_reuses_buffers(pkg, precision):
     f.close()
 
 
-@pytest.mark.parametrize("P,images", [(4, 2), (8, 3), (10, 3), (12, 1)])
+@pytest.mark.parametrize("P,images", [(4, 2), (6, 0), (8, 3), (10, 3), (12, 1)])
 def test_gpu_operators_equal_host(pkg, P, images):
-    """A device set-up at P >= 10 builds its operators with the SVD sweeps
-    and the M2M products on the GPU (below that on the host); either way the
-    tables equal the host set-up's bit for bit."""
+    """A device set-up builds its operators on the GPU (the SVD sweeps, the
+    M2M and image products and the kernel spectra); the tables equal the host
+    set-up's bit for bit."""
     x, q = uniform01(500, 70 + P)
     a = pkg.Argument(P=P, ncrit=32, images=images, cycle=1.0, x=(0.5, 0.5, 0.5), dipole_correction=0)
     pkg.clear_operator_cache()  # each handle builds its own tables
@@ -193,7 +193,7 @@ def test_gpu_operators_equal_host(pkg, P, images):
     N = 2 * P - 1
     nf = N * N * (N // 2 + 1)
     for which, size in [(0, ns * ns), (1, 8 * ns * ns), (2, ns * ns), (3, 26 * 64 * nf * 2), (4, ns * ns),
-                        (5, ns * ns)]:
+                        (5, ns * ns), (6, 26 * nf * 2), (7, ns * ns)]:
         assert np.array_equal(h.operator(which, size), d.operator(which, size)), which
     h.close()
     d.close()
