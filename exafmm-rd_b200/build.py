@@ -50,7 +50,8 @@ def build(force=False, verbose=False):
     with ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 1)) as ex:
         list(ex.map(compile_one, range(len(SOURCES))))
     tmp = LIB + ".tmp"
-    cmd = [NVCC] + FLAGS + ["-shared", "-o", tmp] + objs + ["-lgomp"]
+    # every symbol resolved at link time, so a missing definition fails here
+    cmd = [NVCC] + FLAGS + ["-shared", "-o", tmp] + objs + ["-lgomp", "-Xlinker", "--no-undefined"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

@@ -113,6 +113,8 @@ struct rtfmm_fmm {
   // the P2P lists, offsets and items were built on the GPU (device set-up):
   // the host vectors above are empty
   bool p2p_on_device = false;
+  // plan.p2p is empty and the walk's pairs are on the device (f->dwalk)
+  bool p2p_lists_on_device = false;
   std::vector<int> h_parent, h_dfs, h_dfs_pos;  // inputs of the device build
   DeviceWalk dwalk;                             // the GPU walk's device output
   std::vector<P2PSrc32> list32;
@@ -346,10 +348,15 @@ void build_tables(rtfmm_fmm* f, bool host_p2p = true) {
     L.bnum = cl.bnum;
     f->leaves.push_back(L);
   }
-  f->body_leaf.assign(p.n, 0);
+  // each body's leaf (a device set-up fills it on the GPU, k_body_leaf)
+  if (host_p2p) {
+    f->body_leaf.assign(p.n, 0);
 #pragma omp parallel for schedule(dynamic, 64)
-  for (int l = 0; l < (int)f->leaves.size(); ++l)
-    for (int b = 0; b < f->leaves[l].bnum; ++b) f->body_leaf[f->leaves[l].boff + b] = l;
+    for (int l = 0; l < (int)f->leaves.size(); ++l)
+      for (int b = 0; b < f->leaves[l].bnum; ++b) f->body_leaf[f->leaves[l].boff + b] = l;
+  } else {
+    f->body_leaf.clear();
+  }
 
   // P2P lists in CSR by target leaf; work items of 32 / 64 targets.  The
   // reference's M2P/P2L-to-P2P conversions (traverser.cpp:75-86) can pair a
@@ -375,9 +382,26 @@ void build_tables(rtfmm_fmm* f, bool host_p2p = true) {
   std::vector<int>& dfs_pos = f->h_dfs_pos;
   dfs.resize(nlf);
   dfs_pos.resize(nlf);
-  for (int l = 0; l < nlf; ++l) dfs[l] = l;
-  std::sort(dfs.begin(), dfs.end(), [&](int a, int b) { return f->leaves[a].boff < f->leaves[b].boff; });
-  for (int i = 0; i < nlf; ++i) dfs_pos[dfs[i]] = i;
+  {
+    // leaves by first body: the tree's depth-first order (children in
+    // octant order own consecutive body ranges), walked without a sort
+    std::vector<int> leaf_of(p.ntree, -1);
+    for (int l = 0; l < nlf; ++l) leaf_of[f->leaves[l].cell] = l;
+    std::vector<int> stack;
+    int k = 0;
+    if (p.ntree > 0) stack.push_back(0);
+    while (!stack.empty()) {
+      const int c = stack.back();
+      stack.pop_back();
+      const Cell& cl = p.cells[c];
+      if (cl.cnum == 0) {
+        if (leaf_of[c] >= 0) dfs[k++] = leaf_of[c];
+        continue;
+      }
+      for (int j = cl.cnum - 1; j >= 0; --j) stack.push_back(cl.coff + j);
+    }
+    for (int i = 0; i < nlf; ++i) dfs_pos[dfs[i]] = i;
+  }
   // ownership: leaf l belongs to rank floor(boff * R / n); a cell is
   // computed by every rank that owns a leaf beneath it (image cells by all)
   {
@@ -568,6 +592,10 @@ void build_pass_tables(rtfmm_fmm* f) {
     add_call(f->l2p_call, 1, {out}, {lid}, nullptr, B_L2P1, BUF_PCHK, BUF_LEAF, 0);
     add_call(f->l2p_call, 1, {lid}, {lid}, &sc, B_L2P2, BUF_LEAF, BUF_LEAF2, 0);
   }
+  // the non-leaf cells of each depth, in cell order
+  std::vector<std::vector<int>> by_depth(p.dmax - p.dmin + 1);
+  for (int c = 0; c < (int)p.cells.size(); ++c)
+    if (p.cells[c].cnum != 0) by_depth[p.cells[c].depth - p.dmin].push_back(c);
   // M2M bottom-up (fmm.cpp:111-150): depth = dmax .. dmin+1.  For depth >= 0
   // each child's contribution M2M[octant] q_child is one row of a batched
   // apply grouped by octant (into the Y scratch), then each parent sums its
@@ -575,9 +603,8 @@ void build_pass_tables(rtfmm_fmm* f) {
   for (int depth = p.dmax; depth > p.dmin; --depth) {
     std::vector<std::vector<int>> in(8), out(8);
     std::vector<int> in1, out1, sums;
-    for (int c = 0; c < (int)p.cells.size(); ++c) {
+    for (int c : by_depth[depth - p.dmin]) {
       const Cell& cl = p.cells[c];
-      if (cl.depth != depth || cl.cnum == 0) continue;
       if (depth >= 0) {
         for (int k = 0; k < cl.cnum; ++k) {
           const int ch = cl.coff + k;
@@ -605,9 +632,9 @@ void build_pass_tables(rtfmm_fmm* f) {
   for (int depth = p.dmin; depth < p.dmax; ++depth) {
     std::vector<std::vector<int>> in(8), out(8);
     std::vector<int> in1, out1;
-    for (int c = 0; c < (int)p.cells.size(); ++c) {
+    for (int c : by_depth[depth - p.dmin]) {
       const Cell& cl = p.cells[c];
-      if (cl.depth != depth || cl.cnum == 0 || !f->cell_own[c]) continue;
+      if (!f->cell_own[c]) continue;
       if (depth >= 0) {
         for (int k = 0; k < cl.cnum; ++k) {
           const int ch = cl.coff + k;
@@ -833,7 +860,11 @@ int upload_plan(rtfmm_fmm* f) {
   } while (0)
   RC(dalloc(f, &f->d_body64, n));
   RC(dalloc(f, &f->d_body32, n));
-  RC(dupload(f, &f->d_body_leaf, f->body_leaf));
+  if (f->body_leaf.empty() && n > 0) {
+    RC(dalloc(f, &f->d_body_leaf, n));  // filled below from the leaf table
+  } else {
+    RC(dupload(f, &f->d_body_leaf, f->body_leaf));
+  }
   if (f->host_bodies)
     RC(dupload(f, &f->d_perm, p.perm));
   else
@@ -841,6 +872,7 @@ int upload_plan(rtfmm_fmm* f) {
   RC(dalloc(f, &f->d_xin, 3 * n));
   RC(dalloc(f, &f->d_qin, n));
   RC(dupload(f, &f->d_leaves, f->leaves));
+  if (f->body_leaf.empty() && n > 0) CK(launch_body_leaf(f->d_leaves, (int)nleaf, (int)n, f->d_body_leaf, f->s0));
   {
     // the exchange of a two-phase pass: every leaf's cell, and which leaves
     // this rank computes
@@ -1390,15 +1422,22 @@ void finish_setup(rtfmm_fmm* f, const TreeScratchFn* gpu = nullptr) {
     const std::vector<WalkRoot> roots = traverse_begin(f->plan);
     std::string msg;
     f->dwalk = DeviceWalk();
-    const int rc = device_p2p_walk(f->plan, roots, f->s0, *gpu, kWalkSlots, &f->dwalk, msg);
+    // the lists stay on the device when the GPU builds the P2P tables from
+    // them (the host copy is fetched only on request, rtfmm_b200_get_p2p)
+    const int rc = device_p2p_walk(f->plan, roots, f->s0, *gpu, kWalkSlots, &f->dwalk, msg, false);
     if (rc == kTreeError) throw std::runtime_error(msg);
     if (rc == kTreeTooDeep) {
       f->plan.p2p.clear();
       traverse_p2p(f->plan, roots);
     }
     device_tables = rc == kTreeOk && f->plan.n > 0 && f->dwalk.npairs > 0;
+    if (rc == kTreeOk && !device_tables && device_walk_host_lists(f->dwalk, f->plan, f->s0, msg) != kTreeOk)
+      throw std::runtime_error(msg);
+    f->p2p_lists_on_device = device_tables;
     traverse_finish(f->plan);
+    if (device_tables) f->plan.n_p2p = f->dwalk.npairs;
   } else {
+    f->p2p_lists_on_device = false;
     traverse(f->plan);
   }
   st[1] = wall_s() - t;
@@ -1996,6 +2035,11 @@ int rtfmm_b200_get_perm(rtfmm_fmm* f, int64_t* perm) {
 int rtfmm_b200_get_p2p(rtfmm_fmm* f, int32_t* ints, double* off) {
   if (!f) return fail(RTFMM_EINVAL, "null handle");
   if (!f->setup_done) return fail(RTFMM_ESTATE, "setup has not run");
+  if (f->p2p_lists_on_device) {
+    std::string msg;
+    if (device_walk_host_lists(f->dwalk, f->plan, f->s0, msg) != kTreeOk) return fail(RTFMM_ECUDA, msg);
+    f->p2p_lists_on_device = false;
+  }
   size_t e = 0;
   for (const auto& kv : f->plan.p2p)
     for (const P2PEntry& s : kv.second) {

@@ -147,6 +147,15 @@ __global__ void k_prep32(const double4* __restrict__ body64, const int* __restri
   body32[i] = make_float4((float)(b.x - L.cx), (float)(b.y - L.cy), (float)(b.z - L.cz), (float)b.w);
 }
 
+// body_leaf[b] = the leaf holding tree-order body b (block per leaf)
+__global__ void k_body_leaf(const LeafInfo* __restrict__ leaves, int nleaf, int n, int* __restrict__ body_leaf) {
+  const int l = blockIdx.x;
+  if (l >= nleaf) return;
+  const LeafInfo L = leaves[l];
+  for (int b = threadIdx.x; b < L.bnum; b += blockDim.x)
+    if (L.boff + b >= 0 && L.boff + b < n) body_leaf[L.boff + b] = l;
+}
+
 // ---------------------------------------------------------------------------
 // P2P: one warp per work item (up to 32 targets of one leaf); sources staged
 // 32 at a time in a per-warp shared-memory slot and read as broadcasts, the
@@ -1730,6 +1739,11 @@ cudaError_t launch_g8_layout(const double* cc8, int Nf, T* G, cudaStream_t st) {
 }
 template cudaError_t launch_g8_layout<float>(const double*, int, float*, cudaStream_t);
 template cudaError_t launch_g8_layout<double>(const double*, int, double*, cudaStream_t);
+
+cudaError_t launch_body_leaf(const LeafInfo* leaves, int nleaf, int n, int* body_leaf, cudaStream_t st) {
+  if (nleaf > 0) k_body_leaf<<<nleaf, 128, 0, st>>>(leaves, nleaf, n, body_leaf);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_m2l_hadamard27(const double* Q, const double* G27, const int* tsrc, int ntar, int nsrc,
                                   int Nf, double* Pk, cudaStream_t st) {

@@ -57,6 +57,8 @@ struct ApplyBatch {
 };
 
 // Launch helpers (all asynchronous on `st`; return cudaGetLastError()).
+// body_leaf[b] = leaf of tree-order body b (the leaves partition [0, n))
+cudaError_t launch_body_leaf(const LeafInfo* leaves, int nleaf, int n, int* body_leaf, cudaStream_t st);
 cudaError_t launch_prep32(const double4* body64, const int* body_leaf, const LeafInfo* leaves,
                           float4* body32, int n, cudaStream_t st);
 cudaError_t launch_p2p32(const float4* body32, const P2PItem32* items, int nitems, const int* list_off,

@@ -144,8 +144,43 @@ struct Scratch {
     }                                                           \
   } while (0)
 
+namespace {
+// plan.p2p from the sorted pairs: each target's run becomes its list
+void pairs_to_lists(const std::vector<unsigned long long>& out, const std::vector<V3>& offs, int nc, Plan& plan) {
+  const int H = (int)out.size();
+  std::vector<int> run_start;
+  for (int i = 0; i < H; ++i)
+    if (i == 0 || (out[i] >> (kCellBits + 5)) != (out[i - 1] >> (kCellBits + 5))) run_start.push_back(i);
+  run_start.push_back(H);
+  plan.p2p.v.assign(nc, {});
+  const unsigned long long cmask = (1ull << kCellBits) - 1;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int r = 0; r < (int)run_start.size() - 1; ++r) {
+    const int a = run_start[r], b = run_start[r + 1];
+    const int tc = (int)(out[a] >> (kCellBits + 5));
+    std::vector<P2PEntry>& L = plan.p2p.v[tc];
+    L.resize(b - a);
+    for (int i = a; i < b; ++i) {
+      const int sc = (int)((out[i] >> 5) & cmask);
+      const int w = (int)(out[i] & 31);
+      L[i - a] = P2PEntry{sc, offs[w]};
+    }
+  }
+}
+}  // namespace
+
+int device_walk_host_lists(const DeviceWalk& dw, Plan& plan, cudaStream_t st, std::string& msg) {
+  std::vector<unsigned long long> out(dw.npairs);
+  if (dw.npairs > 0) {
+    LCK(cudaMemcpyAsync(out.data(), dw.pairs, sizeof(unsigned long long) * dw.npairs, cudaMemcpyDeviceToHost, st));
+    LCK(cudaStreamSynchronize(st));
+  }
+  pairs_to_lists(out, dw.host_offs, dw.ncell, plan);
+  return kTreeOk;
+}
+
 int device_p2p_walk(Plan& plan, const std::vector<WalkRoot>& roots, cudaStream_t st, const TreeScratchFn& scratch,
-                    int slot_base, DeviceWalk* dw, std::string& msg) {
+                    int slot_base, DeviceWalk* dw, std::string& msg, bool host_lists) {
   const int nc = (int)plan.cells.size();
   if (nc >= (1 << kCellBits) || roots.size() > 31) return kTreeTooDeep;
   Scratch S{scratch, slot_base};
@@ -323,40 +358,30 @@ int device_p2p_walk(Plan& plan, const std::vector<WalkRoot>& roots, cudaStream_t
     k_gather<<<cdiv(H, 256), 256, 0, st>>>(hv[hset], idx0, H, g0);
     LCK(cudaGetLastError());
     LCK(cub::DeviceRadixSort::SortKeys(tmp, tb, g0, g1, H, kCellBits + 5, 2 * kCellBits + 5, st));
-    LCK(cudaMemcpyAsync(out.data(), g1, sizeof(unsigned long long) * H, cudaMemcpyDeviceToHost, st));
-    LCK(cudaStreamSynchronize(st));
+    if (host_lists || !dw) {
+      LCK(cudaMemcpyAsync(out.data(), g1, sizeof(unsigned long long) * H, cudaMemcpyDeviceToHost, st));
+      LCK(cudaStreamSynchronize(st));
+    }
     if (dw) {
       dw->pairs = g1;
       dw->npairs = H;
     }
   }
+  std::vector<V3> offs(nw);
+  for (int w = 0; w < nw; ++w) offs[w] = roots[w].off;
   if (dw) {
     dw->offs = doff;
     dw->nwalk = nw;
     dw->ncell = nc;
     dw->cboff = dcb;
     dw->cbnum = dcm;
+    dw->host_offs = offs;
+    if (H == 0) dw->npairs = 0;
   }
-
-  // each target's run becomes its list
-  std::vector<int> run_start;
-  for (int i = 0; i < H; ++i)
-    if (i == 0 || (out[i] >> (kCellBits + 5)) != (out[i - 1] >> (kCellBits + 5))) run_start.push_back(i);
-  run_start.push_back(H);
-  plan.p2p.v.assign(nc, {});
-  const unsigned long long cmask = (1ull << kCellBits) - 1;
-#pragma omp parallel for schedule(dynamic, 64)
-  for (int r = 0; r < (int)run_start.size() - 1; ++r) {
-    const int a = run_start[r], b = run_start[r + 1];
-    const int tc = (int)(out[a] >> (kCellBits + 5));
-    std::vector<P2PEntry>& L = plan.p2p.v[tc];
-    L.resize(b - a);
-    for (int i = a; i < b; ++i) {
-      const int sc = (int)((out[i] >> 5) & cmask);
-      const int w = (int)(out[i] & 31);
-      L[i - a] = P2PEntry{sc, roots[w].off};
-    }
-  }
+  if (host_lists || !dw)
+    pairs_to_lists(out, offs, nc, plan);
+  else
+    plan.p2p.v.assign(nc, {});
   return kTreeOk;
 }
 

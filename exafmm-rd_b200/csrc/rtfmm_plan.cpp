@@ -372,21 +372,36 @@ void traverse_finish(Plan& plan) {
   // M2L parent map over the tree cells (make_M2L_parent_map and the
   // periodic part of make_M2L_parent_map_i1, traverser.cpp:234-282).  The
   // reference tests every cell pair; same-depth cells sit on a lattice of
-  // spacing 2r, so the same predicate is evaluated here through a hash of
-  // lattice coordinates: a source at lattice displacement v in {-1,0,1}^3
-  // (wrapped periodically when images >= 1) with offset p * cycle.
-  std::unordered_map<uint64_t, int> lattice;
-  auto key = [](int depth, int64_t i, int64_t j, int64_t k) {
-    return ((uint64_t)depth << 57) ^ ((uint64_t)i << 38) ^ ((uint64_t)j << 19) ^ (uint64_t)k;
-  };
+  // spacing 2r, so the same predicate is evaluated here for the cell at each
+  // lattice displacement v in {-1,0,1}^3 (wrapped periodically when images
+  // >= 1, with offset p * cycle).  A cell at depth d and lattice coordinate m
+  // is found by descending from the root along the bits of m (bit d - l of
+  // each axis gives the octant at level l).
   const V3 lo{a.x[0] - plan.r0, a.x[1] - plan.r0, a.x[2] - plan.r0};
   std::vector<std::array<int64_t, 3>> coord(plan.ntree);
+#pragma omp parallel for schedule(static)
   for (int c = 0; c < plan.ntree; ++c) {
     const Cell& cl = plan.cells[c];
     for (int k = 0; k < 3; ++k)
       coord[c][k] = (int64_t)std::llround((cl.x[k] - lo[k]) / (2 * cl.r) - 0.5);
-    if (cl.cnum > 0) lattice[key(cl.depth, coord[c][0], coord[c][1], coord[c][2])] = c;
   }
+  // each tree cell's child by octant (-1: none)
+  std::vector<std::array<int, 8>> child(plan.ntree);
+#pragma omp parallel for schedule(static)
+  for (int c = 0; c < plan.ntree; ++c) {
+    const Cell& cl = plan.cells[c];
+    child[c].fill(-1);
+    for (int k = 0; k < cl.cnum; ++k) child[c][plan.cells[cl.coff + k].octant & 7] = cl.coff + k;
+  }
+  // the non-leaf tree cell at (depth, m), or -1
+  auto lattice_cell = [&](int depth, const int64_t m[3]) {
+    int c = 0;
+    for (int l = 1; l <= depth && c >= 0; ++l) {
+      const int sh = depth - l;
+      c = child[c][(((m[0] >> sh) & 1) << 2) | (((m[1] >> sh) & 1) << 1) | ((m[2] >> sh) & 1)];
+    }
+    return c >= 0 && plan.cells[c].cnum > 0 ? c : -1;
+  };
   // each parent's list is written by one thread (lists sized up front; the
   // lattice is only read)
   if ((int)plan.m2l.v.size() < plan.ntree) plan.m2l.v.resize(plan.ntree);
@@ -395,7 +410,8 @@ void traverse_finish(Plan& plan) {
     const Cell& T = plan.cells[j];
     if (T.cnum == 0) continue;
     const int64_t nside = (int64_t)1 << T.depth;
-    std::vector<M2LEntry> near, far;
+    M2LEntry near[26], far[26];
+    int nn = 0, nf = 0;
     for (int vz = -1; vz <= 1; ++vz)
       for (int vy = -1; vy <= 1; ++vy)
         for (int vx = -1; vx <= 1; ++vx) {
@@ -409,17 +425,21 @@ void traverse_finish(Plan& plan) {
             if (pw[k] != 0) inside = false;
           }
           if (!inside && a.images == 0) continue;
-          auto it = lattice.find(key(T.depth, m[0], m[1], m[2]));
-          if (it == lattice.end()) continue;
+          const int src = lattice_cell(T.depth, m);
+          if (src < 0) continue;
           V3 off{pw[0] * cycle, pw[1] * cycle, pw[2] * cycle};
           // confirm with the reference's own predicate
-          if (!w.neighbour(j, it->second, off)) continue;
-          (inside ? near : far).push_back({it->second, off, 0});
+          if (!w.neighbour(j, src, off)) continue;
+          if (inside)
+            near[nn++] = {src, off, 0};
+          else
+            far[nf++] = {src, off, 0};
         }
-    if (!near.empty() || !far.empty()) {
+    if (nn + nf > 0) {
       auto& lst = plan.m2l.v[(size_t)j];
-      lst.insert(lst.end(), near.begin(), near.end());
-      lst.insert(lst.end(), far.begin(), far.end());
+      lst.reserve(lst.size() + nn + nf);
+      lst.insert(lst.end(), near, near + nn);
+      lst.insert(lst.end(), far, far + nf);
     }
   }
 

@@ -30,10 +30,11 @@ int device_build_tree(const double* x_dev, const double* q_dev, int64_t n, cudaS
                       int64_t* d_perm, const TreeScratchFn& scratch, std::string& msg);
 
 // The P2P lists of the dual-tree walk from `roots` (traverse_begin) on the
-// GPU, into plan.p2p: the same entries in the same order as traverse_p2p.
-// Scratch slots slot_base .. slot_base + 27.  kTreeTooDeep: the walk is
-// deeper than 40 divisions or the tree has 2^25 cells or more (use
-// traverse_p2p).
+// GPU: the same entries in the same order as traverse_p2p, into plan.p2p
+// when host_lists (else left on the device, plan.p2p empty: see
+// device_walk_host_lists).  Scratch slots slot_base .. slot_base + 27.
+// kTreeTooDeep: the walk is deeper than 40 divisions or the tree has 2^25
+// cells or more (use traverse_p2p).
 // What the GPU walk leaves on the device (in its scratch slots, valid until
 // they are reused): the pairs sorted by target cell, depth-first within one
 // (target << 30 | source << 5 | walk), the walks' offsets, the cells' body
@@ -45,9 +46,12 @@ struct DeviceWalk {
   int nwalk = 0, ncell = 0;
   const int* cboff = nullptr;
   const int* cbnum = nullptr;
+  std::vector<V3> host_offs;  // the walks' offsets (roots' order)
 };
 int device_p2p_walk(Plan& plan, const std::vector<WalkRoot>& roots, cudaStream_t st, const TreeScratchFn& scratch,
-                    int slot_base, DeviceWalk* dw, std::string& msg);
+                    int slot_base, DeviceWalk* dw, std::string& msg, bool host_lists = true);
+// plan.p2p from a walk left on the device (its pairs copied back).
+int device_walk_host_lists(const DeviceWalk& dw, Plan& plan, cudaStream_t st, std::string& msg);
 
 // The pass's P2P tables built on the GPU from the walk's pairs: list
 // offsets by target leaf, the list entries (FP32 or FP64 form) and the work
