@@ -263,9 +263,15 @@ def test_operator_tables_shared_between_handles(pkg):
     f2.setup()
     t2 = f2.setup_times()["operators"]
     ns = 152
-    for which, size in [(0, ns * ns), (1, 8 * ns * ns), (2, ns * ns), (4, ns * ns), (5, ns * ns)]:
+    for which, size in [(0, ns * ns), (1, 8 * ns * ns), (2, ns * ns), (4, ns * ns), (5, ns * ns), (7, ns * ns)]:
         assert np.array_equal(f1.operator(which, size), f2.operator(which, size))
     assert t2 < t1 / 3, (t1, t2)
+    # the build's parts add up to the operator phase; a cached set reports none
+    st1, st2 = f1.setup_times(), f2.setup_times()
+    parts = ("ops_svd", "ops_orth", "ops_m2m", "ops_img", "ops_spectra", "ops_blocks")
+    assert all(st1[k] >= 0 for k in parts) and st1["ops_svd"] > 0
+    assert 0.5 * t1 <= sum(st1[k] for k in parts) <= t1 * 1.01 + 1e-4, st1
+    assert all(st2[k] == 0 for k in parts), st2
     pkg.clear_operator_cache()
     f3 = pkg.LaplaceFMM(x, q, a)
     f3.setup()
