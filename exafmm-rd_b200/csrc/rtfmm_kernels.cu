@@ -48,6 +48,10 @@
 #ifndef P2P_TILE
 #define P2P_TILE 32
 #endif
+// register-blocked FFT-M2L up: resident blocks per SM
+#ifndef UP_RB_MINB
+#define UP_RB_MINB 2
+#endif
 // FP32 Hadamard: targets per thread, directions per FP32 partial sum,
 // resident blocks per SM
 #ifndef HAD_TT
@@ -1111,6 +1115,240 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// The up and down kernels above with register blocking, for the orders P
+// fixed at compile time: the sp children of a block go through each DFT pass
+// together, and a thread keeps one input line of the pass (the values along
+// the transformed axis) in registers and forms every output of that line, the
+// twiddles read as shared-memory broadcasts.  Each output sums its terms in
+// the same order as k_m2l_up / k_m2l_down, so the results are the same bit
+// for bit; the shared-memory traffic per multiply-add falls from two loads
+// to about one broadcast.
+template <typename T, int PP>
+__global__ void __launch_bounds__(256, UP_RB_MINB)
+    k_m2l_up_rb(const double* __restrict__ q_equiv, const int* __restrict__ items, const int* __restrict__ surf_ijk,
+                const double* __restrict__ twiddle, int ns, int nsrc, int sp, T* __restrict__ Q) {
+  constexpr int P = PP, N = 2 * P - 1, P3 = P * P * P, PNP = P * N * P;
+  constexpr int SPM = 32 / (2 * (int)sizeof(T));  // largest slot group (m2l_up_slots)
+  constexpr int KC = (256 / (N * P)) < 1 ? 1 : ((256 / (N * P)) > N ? N : 256 / (N * P));
+  constexpr int KH = (N + KC - 1) / KC;
+  extern __shared__ unsigned char smem_raw[];
+  T* W = reinterpret_cast<T*>(smem_raw);  // N*N complex: W[k][n] = w^(k n mod N)
+  T* A = W + 2 * N * N;                   // sp * P^3 complex: [slot][z][y][kx]
+  T* cube = A + 2 * (size_t)sp * P3;      // sp * P^3, read by the first pass only
+  T* Bm = cube;                           // sp * P*N*P complex: [slot][z][ky][kx], after it
+  const int* it = items + 10 * blockIdx.x;
+  const int src = it[0], slot0 = it[1];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int e = tid; e < N * N; e += nt) {
+    const int m = ((e / N) * (e % N)) % N;
+    W[2 * e] = (T)twiddle[2 * m];
+    W[2 * e + 1] = (T)twiddle[2 * m + 1];
+  }
+  for (int e = tid; e < sp * P3; e += nt) cube[e] = T(0);
+  __syncthreads();
+  for (int e = tid; e < sp * ns; e += nt) {
+    const int j = e / ns, i = e - j * ns;
+    const int child = it[2 + j];
+    if (child < 0) continue;  // an absent child: zero spectra
+    const int x = surf_ijk[3 * i], y = surf_ijk[3 * i + 1], z = surf_ijk[3 * i + 2];
+    cube[(size_t)j * P3 + (z * P + y) * P + x] = (T)q_equiv[(size_t)child * ns + i];
+  }
+  __syncthreads();
+  // x -> kx: a thread per (slot, z, y)
+  for (int e = tid; e < sp * P * P; e += nt) {
+    const int j = e / (P * P), zy = e - j * P * P;
+    const T* row = cube + (size_t)j * P3 + zy * P;
+    T r[P];
+#pragma unroll
+    for (int x = 0; x < P; ++x) r[x] = row[x];
+    T* a = A + 2 * ((size_t)j * P3 + zy * P);
+#pragma unroll
+    for (int kx = 0; kx < P; ++kx) {
+      const T* wk = W + 2 * kx * N;
+      T re = 0, im = 0;
+#pragma unroll
+      for (int x = 0; x < P; ++x) {
+        re = fma(r[x], wk[2 * x], re);
+        im = fma(r[x], wk[2 * x + 1], im);
+      }
+      a[2 * kx] = re;
+      a[2 * kx + 1] = im;
+    }
+  }
+  __syncthreads();
+  // y -> ky: a thread per (slot, z, kx)
+  for (int e = tid; e < sp * P * P; e += nt) {
+    const int j = e / (P * P), z = (e / P) % P, kx = e % P;
+    T ar[P], ai[P];
+#pragma unroll
+    for (int y = 0; y < P; ++y) {
+      const T* q = A + 2 * ((size_t)j * P3 + (z * P + y) * P + kx);
+      ar[y] = q[0];
+      ai[y] = q[1];
+    }
+    T* b = Bm + 2 * ((size_t)j * PNP + z * N * P + kx);
+#pragma unroll
+    for (int ky = 0; ky < N; ++ky) {
+      const T* wk = W + 2 * ky * N;
+      T re = 0, im = 0;
+#pragma unroll
+      for (int y = 0; y < P; ++y) cmad(re, im, ar[y], ai[y], wk[2 * y], wk[2 * y + 1]);
+      b[2 * ky * P] = re;
+      b[2 * ky * P + 1] = im;
+    }
+  }
+  __syncthreads();
+  // z -> kz: a thread per (ky, kx, range of kz), every slot; two slots of a
+  // frequency written together as in k_m2l_up
+  using V2 = typename Cplx2<T>::type;
+  for (int e = tid; e < N * P * KC; e += nt) {
+    const int c = e / (N * P), ky = (e / P) % N, kx = e % P;
+    T br[SPM][P], bi[SPM][P];
+#pragma unroll
+    for (int j = 0; j < SPM; ++j)
+#pragma unroll
+      for (int z = 0; z < P; ++z) {
+        if (j < sp) {
+          const T* q = Bm + 2 * ((size_t)j * PNP + (z * N + ky) * P + kx);
+          br[j][z] = q[0];
+          bi[j][z] = q[1];
+        } else {
+          br[j][z] = bi[j][z] = T(0);
+        }
+      }
+    const int kz1 = (c + 1) * KH < N ? (c + 1) * KH : N;
+    for (int kz = c * KH; kz < kz1; ++kz) {
+      const T* wk = W + 2 * kz * N;
+      const int f = (kz * N + ky) * P + kx;
+      T* out = Q + (((size_t)f * nsrc + src) * 8 + slot0) * 2;
+#pragma unroll
+      for (int j = 0; j < SPM; j += 2) {
+        if (j >= sp) break;
+        T re0 = 0, im0 = 0, re1 = 0, im1 = 0;
+#pragma unroll
+        for (int z = 0; z < P; ++z) {
+          cmad(re0, im0, br[j][z], bi[j][z], wk[2 * z], wk[2 * z + 1]);
+          if (j + 1 < sp) cmad(re1, im1, br[j + 1][z], bi[j + 1][z], wk[2 * z], wk[2 * z + 1]);
+        }
+        if (j + 1 < sp) {
+          V2 v;
+          v.x = re0;
+          v.y = im0;
+          v.z = re1;
+          v.w = im1;
+          *reinterpret_cast<V2*>(out + 2 * j) = v;
+        } else {
+          out[2 * j] = re0;
+          out[2 * j + 1] = im0;
+        }
+      }
+    }
+  }
+}
+
+template <typename T, int PP>
+__global__ void __launch_bounds__(256)
+    k_m2l_down_rb(const T* __restrict__ Pk, const int* __restrict__ items, const double* __restrict__ tscale,
+                  const int* __restrict__ surf_ijk, const double* __restrict__ twiddle, int ns, int ntar, int sp,
+                  double* __restrict__ p_check) {
+  constexpr int P = PP, N = 2 * P - 1, P3 = P * P * P, PNP = P * N * P, Nf = N * N * P;
+  extern __shared__ unsigned char smem_raw[];
+  T* W = reinterpret_cast<T*>(smem_raw);  // P*N complex: W[o][k] = conj(w)^(k (P-1+o) mod N)
+  T* Y1 = W + 2 * P * N;                  // sp * P*N*P complex: [slot][zo][ky][kx]
+  T* X = Y1 + 2 * (size_t)sp * PNP;       // sp * Nf complex: [slot][f]; later Y2
+  T* Y2 = X;                              // sp * P^3 complex: [slot][zo][yo][kx]
+  const int* it = items + 10 * blockIdx.x;
+  const int tar = it[0], slot0 = it[1];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int e = tid; e < P * N; e += nt) {
+    const int o = e / N, k = e % N;
+    const int m = (k * (P - 1 + o)) % N;
+    W[2 * e] = (T)twiddle[2 * m];
+    W[2 * e + 1] = -(T)twiddle[2 * m + 1];
+  }
+  if (sp >= 2) {
+    using V2 = typename Cplx2<T>::type;
+    const int hp = sp / 2;
+    for (int e = tid; e < Nf * hp; e += nt) {
+      const int f = e / hp, j = 2 * (e % hp);
+      const V2 v = *reinterpret_cast<const V2*>(Pk + (((size_t)f * ntar + tar) * 8 + slot0 + j) * 2);
+      X[2 * ((size_t)j * Nf + f)] = v.x;
+      X[2 * ((size_t)j * Nf + f) + 1] = v.y;
+      X[2 * ((size_t)(j + 1) * Nf + f)] = v.z;
+      X[2 * ((size_t)(j + 1) * Nf + f) + 1] = v.w;
+    }
+  } else {
+    for (int f = tid; f < Nf; f += nt) {
+      const T* in = Pk + (((size_t)f * ntar + tar) * 8 + slot0) * 2;
+      X[2 * f] = in[0];
+      X[2 * f + 1] = in[1];
+    }
+  }
+  __syncthreads();
+  // kz -> zo (zo < P only): a thread per (slot, ky, kx)
+  for (int e = tid; e < sp * N * P; e += nt) {
+    const int j = e / (N * P), ky = (e / P) % N, kx = e % P;
+    T xr[N], xi[N];
+#pragma unroll
+    for (int kz = 0; kz < N; ++kz) {
+      const T* q = X + 2 * ((size_t)j * Nf + (kz * N + ky) * P + kx);
+      xr[kz] = q[0];
+      xi[kz] = q[1];
+    }
+#pragma unroll
+    for (int zo = 0; zo < P; ++zo) {
+      const T* wo = W + 2 * zo * N;
+      T re = 0, im = 0;
+#pragma unroll
+      for (int kz = 0; kz < N; ++kz) cmad(re, im, xr[kz], xi[kz], wo[2 * kz], wo[2 * kz + 1]);
+      T* y1 = Y1 + 2 * ((size_t)j * PNP + (zo * N + ky) * P + kx);
+      y1[0] = re;
+      y1[1] = im;
+    }
+  }
+  __syncthreads();  // X is read: its space becomes Y2
+  // ky -> yo (yo < P): a thread per (slot, zo, kx)
+  for (int e = tid; e < sp * P * P; e += nt) {
+    const int j = e / (P * P), zo = (e / P) % P, kx = e % P;
+    T yr[N], yi[N];
+#pragma unroll
+    for (int ky = 0; ky < N; ++ky) {
+      const T* q = Y1 + 2 * ((size_t)j * PNP + (zo * N + ky) * P + kx);
+      yr[ky] = q[0];
+      yi[ky] = q[1];
+    }
+#pragma unroll
+    for (int yo = 0; yo < P; ++yo) {
+      const T* wo = W + 2 * yo * N;
+      T re = 0, im = 0;
+#pragma unroll
+      for (int ky = 0; ky < N; ++ky) cmad(re, im, yr[ky], yi[ky], wo[2 * ky], wo[2 * ky + 1]);
+      T* y2 = Y2 + 2 * ((size_t)j * P3 + (zo * P + yo) * P + kx);
+      y2[0] = re;
+      y2[1] = im;
+    }
+  }
+  __syncthreads();
+  // kx -> xo at the check-surface points, real part; p_check += value * scale
+  const double sc = tscale[tar];
+  for (int e = tid; e < sp * ns; e += nt) {
+    const int j = e / ns, i = e - j * ns;
+    const int child = it[2 + j];
+    if (child < 0) continue;
+    const int xo = surf_ijk[3 * i], yo = surf_ijk[3 * i + 1], zo = surf_ijk[3 * i + 2];
+    const T* row = Y2 + 2 * ((size_t)j * P3 + (zo * P + yo) * P);
+    const T* wo = W + 2 * xo * N;
+    T acc = 0;
+    // Re(Y * conj(w)^m) summed over kx >= 1, doubled for the missing half
+    for (int kx = 1; kx < P; ++kx) {
+      acc = fma(row[2 * kx], wo[2 * kx], acc);
+      acc = fma(-row[2 * kx + 1], wo[2 * kx + 1], acc);
+    }
+    const T v = row[0] + T(2) * acc;
+    p_check[(size_t)child * ns + i] += (double)v * sc;
+  }
+}
+
 // Hadamard 8x8 (hadamard_8x8 + c2c_8x8x2_avx, kernel.cpp:1012-1082, c2c.h:201-296):
 //   Pk[f][t][itar] = sum_d sum_isrc G[f][d][isrc][itar] * Q[f][src(t,d)][isrc]
 // A block holds one frequency's 26x64 kernel coefficients in shared memory
@@ -1665,16 +1903,19 @@ cudaError_t launch_sum_children(const int* list, int nparents, const double* Y, 
   return cudaGetLastError();
 }
 
+// orders with a compile-time instance (the register-blocked kernels)
+static bool fixed_p(int P) { return P == 4 || P == 6 || P == 8 || P == 10; }
 template <typename T>
 static size_t up_smem(int P, int sp) {
-  const int N = 2 * P - 1;
-  return sizeof(T) * ((size_t)2 * N * N + 3 * (size_t)P * P * P + 2 * (size_t)sp * P * N * P);
+  const size_t N = 2 * P - 1, P3 = (size_t)P * P * P;
+  if (fixed_p(P)) return sizeof(T) * (2 * N * N + 2 * (size_t)sp * P3 + std::max((size_t)sp * P3, 2 * (size_t)sp * P * N * P));
+  return sizeof(T) * (2 * N * N + 3 * P3 + 2 * (size_t)sp * P * N * P);
 }
 template <typename T>
 static size_t down_smem(int P, int sp) {
-  const int N = 2 * P - 1;
-  return sizeof(T) * (2 * (size_t)P * N + 2 * (size_t)P * N * P + 2 * (size_t)P * P * P +
-                      2 * (size_t)sp * N * N * P);
+  const size_t N = 2 * P - 1, P3 = (size_t)P * P * P;
+  if (fixed_p(P)) return sizeof(T) * (2 * (size_t)P * N + 2 * (size_t)sp * P * N * P + 2 * (size_t)sp * N * N * P);
+  return sizeof(T) * (2 * (size_t)P * N + 2 * (size_t)P * N * P + 2 * P3 + 2 * (size_t)sp * N * N * P);
 }
 
 // Largest slot group (8, 4, 2, 1) whose working set fits in shared memory.
@@ -1702,9 +1943,15 @@ template <typename T, int PP>
 static cudaError_t up_p(const double* q_equiv, const int* items, int nitems, const int* surf_ijk,
                         const double* twiddle, int P, int ns, int nsrc, int sp, T* Q, cudaStream_t st) {
   const size_t sm = up_smem<T>(P, sp);
-  cudaError_t e = cudaFuncSetAttribute(k_m2l_up<T, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  if (e != cudaSuccess) return e;
-  k_m2l_up<T, PP><<<nitems, 256, sm, st>>>(q_equiv, items, surf_ijk, twiddle, P, ns, nsrc, sp, Q);
+  if constexpr (PP > 0) {
+    cudaError_t e = cudaFuncSetAttribute(k_m2l_up_rb<T, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    k_m2l_up_rb<T, PP><<<nitems, 256, sm, st>>>(q_equiv, items, surf_ijk, twiddle, ns, nsrc, sp, Q);
+  } else {
+    cudaError_t e = cudaFuncSetAttribute(k_m2l_up<T, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    k_m2l_up<T, PP><<<nitems, 256, sm, st>>>(q_equiv, items, surf_ijk, twiddle, P, ns, nsrc, sp, Q);
+  }
   return cudaGetLastError();
 }
 
@@ -1762,9 +2009,16 @@ static cudaError_t down_p(const T* Pk, const int* items, const double* tscale, i
                           const double* twiddle, int P, int ns, int ntar, int sp, double* p_check,
                           cudaStream_t st) {
   const size_t sm = down_smem<T>(P, sp);
-  cudaError_t e = cudaFuncSetAttribute(k_m2l_down<T, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  if (e != cudaSuccess) return e;
-  k_m2l_down<T, PP><<<nitems, 256, sm, st>>>(Pk, items, tscale, surf_ijk, twiddle, P, ns, ntar, sp, p_check);
+  if constexpr (PP > 0) {
+    cudaError_t e =
+        cudaFuncSetAttribute(k_m2l_down_rb<T, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    k_m2l_down_rb<T, PP><<<nitems, 256, sm, st>>>(Pk, items, tscale, surf_ijk, twiddle, ns, ntar, sp, p_check);
+  } else {
+    cudaError_t e = cudaFuncSetAttribute(k_m2l_down<T, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    k_m2l_down<T, PP><<<nitems, 256, sm, st>>>(Pk, items, tscale, surf_ijk, twiddle, P, ns, ntar, sp, p_check);
+  }
   return cudaGetLastError();
 }
 
