@@ -656,8 +656,12 @@ void build_pass_tables(rtfmm_fmm* f) {
   }
 
   // FFT-M2L lists (m2l_fft_precompute_t, kernel.cpp:1153-1245).  Source
-  // parents are numbered in ascending cell index (s8/s27: cell -> number,
-  // -1 for none).
+  // and target parents of the 8x8 products are numbered level by level in
+  // row-major order of their lattice coordinates (x fastest): a warp of the
+  // Hadamard takes consecutive targets, and the sources of consecutive
+  // targets in one direction are then mostly consecutive rows of the
+  // spectra.  The 1x27 image-level ones in ascending cell index (s8/s27:
+  // cell -> number, -1 for none).
   const int ncell = (int)p.cells.size();
   std::vector<int> s8(ncell, -1), s27(ncell, -1);
   std::vector<int> t8cells, t27cells;
@@ -669,9 +673,29 @@ void build_pass_tables(rtfmm_fmm* f) {
     if (single) t27cells.push_back(kv.first);
     for (const M2LEntry& e : kv.second) (e.single ? s27 : s8)[e.src] = 0;
   }
+  {
+    const V3 lo{p.args.x[0] - p.r0, p.args.x[1] - p.r0, p.args.x[2] - p.r0};
+    auto lattice_key = [&](int c) {
+      const Cell& cl = p.cells[c];
+      int64_t m[3];
+      for (int k = 0; k < 3; ++k) m[k] = (int64_t)std::llround((cl.x[k] - lo[k]) / (2 * cl.r) - 0.5);
+      const int64_t side = c < p.ntree && cl.depth >= 0 ? (int64_t)1 << cl.depth : 1;
+      const int64_t lin = c < p.ntree ? (m[2] * side + m[1]) * side + m[0] : c;
+      return std::make_pair((int64_t)cl.depth + (c < p.ntree ? 0 : 1000), lin);
+    };
+    std::vector<std::pair<std::pair<int64_t, int64_t>, int>> key8;
+    for (int c = 0; c < ncell; ++c)
+      if (s8[c] >= 0) key8.push_back({lattice_key(c), c});
+    std::sort(key8.begin(), key8.end());
+    for (int k = 0; k < (int)key8.size(); ++k) s8[key8[k].second] = k;
+    std::vector<std::pair<std::pair<int64_t, int64_t>, int>> keyt;
+    for (int c : t8cells) keyt.push_back({lattice_key(c), c});
+    std::sort(keyt.begin(), keyt.end());
+    for (int k = 0; k < (int)keyt.size(); ++k) t8cells[k] = keyt[k].second;
+  }
   int k8 = 0, k27 = 0;
   for (int c = 0; c < ncell; ++c) {
-    if (s8[c] >= 0) s8[c] = k8++;
+    if (s8[c] >= 0) ++k8;
     if (s27[c] >= 0) s27[c] = k27++;
   }
   f->nS8 = k8;
