@@ -282,7 +282,7 @@ struct Graph {
   }
 };
 
-int jacobi_sweeps_gpu(int n, std::vector<double>& W, std::vector<double>& Vc, cudaStream_t st) {
+int jacobi_sweeps_gpu(int n, std::vector<double>& W, std::vector<double>& Vc, cudaStream_t st, bool one_launch) {
   const int m = n + (n & 1);
   if (n < 2) {
     jacobi_sweeps_host(n, W, Vc);
@@ -309,7 +309,7 @@ int jacobi_sweeps_gpu(int n, std::vector<double>& W, std::vector<double>& Vc, cu
     check(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "attribute");
     check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_jacobi_sweeps, 32 * kRoundWarps, 0), "occupancy");
     const int nblk = std::min((m / 2 + kRoundWarps - 1) / kRoundWarps, nsm * per);
-    if (coop && nblk >= 1) {
+    if (one_launch && coop && nblk >= 1) {
       Buf baux;
       unsigned long long* aux = baux.get<unsigned long long>(4);  // off_bits[2], bar[2], status[2]
       check(cudaMemsetAsync(aux, 0, sizeof(unsigned long long) * 4, st), "memset");

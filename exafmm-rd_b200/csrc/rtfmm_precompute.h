@@ -11,8 +11,10 @@
 namespace rtfmm_b200 {
 
 // returns the sweeps run by the one-launch (cooperative) form, -1 when the
-// per-sweep graph (or the host, n < 2) ran them
-int jacobi_sweeps_gpu(int n, std::vector<double>& W, std::vector<double>& Vc, cudaStream_t st);
+// per-sweep graph (or the host, n < 2) ran them; one_launch = false asks for
+// the graph form
+int jacobi_sweeps_gpu(int n, std::vector<double>& W, std::vector<double>& Vc, cudaStream_t st,
+                      bool one_launch = true);
 void matmul_gpu(int n, const double* A, const double* B, double* C, cudaStream_t st);
 void chain_gpu(int n, const double* A, const double* B, int nG, const double* const* G, double* const* out,
                cudaStream_t st);
