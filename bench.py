@@ -53,6 +53,43 @@ def load_pkg():
     return mod
 
 
+def pass_roofline(info, n, Nf, had_flop, had_bytes, fp32_peak, sm_mhz, hbm, hbm_kind, pass_ms):
+    """The whole pass against its roofline: each stage's algorithmic work
+    (flops and bytes per unit as the scope table counts them) gives the time
+    its bound allows, max(flops / compute peak, bytes / HBM peak); their sum
+    over the measured pass time is the fraction of the roofline the pass
+    reaches.  P2P and the Hadamard count against FP32, the operator stages
+    against FP64 (nominal 148 SM x 64 FMA/clk x 2 at the sampled clock)."""
+    ns, nl, N = info["num_surf"], info["nleaf"], n
+    nch = max(info["ncell"] - 1, 0)  # every cell but the root is a child
+    nsrc, ntar = info["m2l8_sources"], info["m2l8_targets"]
+    fp64_peak = 148 * 64 * 2 * sm_mhz * 1e6 / 1e12
+    bw = hbm * 1e9
+
+    def bound(flop, peak_tf, nbytes):
+        return max(flop / (peak_tf * 1e12), nbytes / bw)
+
+    st = {
+        # 20 flop per body pair; bodies read (16 B) and phi, grad written (32 B)
+        "P2P": bound(20.0 * info["p2p_pairs"], fp32_peak, 48.0 * N),
+        # 11 flop per body x check point, two ns x ns products per leaf
+        "P2M": bound(11.0 * N * ns + 4.0 * ns * ns * nl, fp64_peak, 16.0 * N + 8.0 * ns * nl),
+        "M2M": bound(2.0 * ns * ns * nch, fp64_peak, 16.0 * ns * nch),
+        "M2L_up": bound(0.0, fp32_peak, (8.0 * ns * 8 + 8.0 * Nf * 8) * nsrc),
+        "M2L_hadamard": bound(had_flop, fp32_peak, had_bytes),
+        "M2L_down": bound(0.0, fp32_peak, (8.0 * ns * 8 + 8.0 * Nf * 8) * ntar),
+        "L2L": bound(2.0 * ns * ns * nch, fp64_peak, 16.0 * ns * nch),
+        # 20 flop per body x equivalent point, two products per leaf; bodies
+        # read, phi and grad written
+        "L2P": bound(20.0 * N * ns + 4.0 * ns * ns * nl, fp64_peak, 48.0 * N + 8.0 * ns * nl),
+    }
+    total = sum(st.values())
+    return {"bound_ms": total * 1e3, "pass_ms": pass_ms, "frac": total * 1e3 / pass_ms,
+            "stages_bound_ms": {k: v * 1e3 for k, v in st.items()},
+            "peaks": {"fp32_tflops": fp32_peak, "fp64_tflops": fp64_peak, "hbm_gbs": hbm,
+                      "kind": "FP32/FP64 nominal at the sampled SM clock; HBM " + hbm_kind}}
+
+
 def make_bodies(n, seed):
     rng = np.random.default_rng(seed)
     x = rng.random((n, 3))
@@ -518,6 +555,7 @@ def run_ours(args):
                 "work_per_launch": K["work"], "launch_ms": K["ms"],
                 "others": {k: {"achieved": d["achieved"], "peak": d["peak"], "unit": d["unit"],
                                "frac": d["frac"], "launch_ms": d["ms"]} for k, d in kern.items() if k != top}}
+    pass_roof = pass_roofline(info, n, Nf, had_flop, had_bytes, fp32_peak, sm_mhz, hbm, hbm_kind, t_m)
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         try:
@@ -555,6 +593,7 @@ def run_ours(args):
                    "ms_per_step_direct_launches": float(np.median(ms_direct)),
                    "stage_ms_overlapped": st_mixed, "stage_ms_serial": stage_serial},
         "roofline": roofline,
+        "pass_roofline": pass_roof,
         "cpu_baseline": cpu,
         "e2e": {"value": world * n / t_e, "unit": "particles/s", "h2d_bytes_per_step": 8 * n,
                 "d2h_bytes_per_step": 8 * n + 24 * n, "ms_per_step": 1000 * t_e},

@@ -1,7 +1,8 @@
-"""The multi-GPU path of bench.py is replicas only (the pass does not shard
-in this build): each rank runs its own pass and rank 0 reports all ranks'
-bodies over the slowest rank's time.  Checked here with two gloo ranks on
-CPU: the max-over-ranks reduction and the aggregate value."""
+"""bench.py's multi-GPU bookkeeping.  By default each rank runs its own
+pass (replicas; --shard splits one pass instead) and rank 0 reports all
+ranks' bodies over the slowest rank's time: the max-over-ranks reduction and
+the aggregate value, with two gloo ranks on CPU.  Also the whole-pass
+roofline helper, on the headline workload's counts."""
 import importlib.util
 import os
 
@@ -54,3 +55,23 @@ def test_single_rank_is_unchanged():
     bench = load_bench()
     assert bench.max_over_ranks([1.5, 2.5], 1, "cpu") == [1.5, 2.5]
     assert bench.replica_value(1 << 20, 1, 7.0) == pytest.approx((1 << 20) / 7.0e-3)
+
+
+def test_pass_roofline_sums_stage_bounds():
+    bench = load_bench()
+    # counts of the headline workload (N = 2^20, P = 8, ncrit = 256)
+    info = {"num_surf": 296, "nleaf": 18075, "ncell": 20660, "p2p_pairs": 5601309424, "m2l8_pairs": 40214,
+            "m2l8_sources": 2633, "m2l8_targets": 2581}
+    Nf = 15 * 15 * 8
+    had_flop = 8.0 * 64 * Nf * info["m2l8_pairs"]
+    had_bytes = Nf * 64 * (2633 + 2 * 2581) + 26 * 64 * Nf * 8
+    r = bench.pass_roofline(info, 1 << 20, Nf, had_flop, had_bytes, 74.45, 1965.0, 6542.1, "measured", 6.7)
+    st = r["stages_bound_ms"]
+    assert set(st) == {"P2P", "P2M", "M2M", "M2L_up", "M2L_hadamard", "M2L_down", "L2L", "L2P"}
+    # P2P is FP32-bound: 20 flop per pair at 74.45 TFLOP/s
+    assert abs(st["P2P"] - 20.0 * 5601309424 / 74.45e12 * 1e3) < 1e-9
+    # the spectra passes are bandwidth-bound
+    assert abs(st["M2L_up"] - (8.0 * 296 * 8 + 8.0 * Nf * 8) * 2633 / 6542.1e9 * 1e3) < 1e-9
+    assert abs(r["bound_ms"] - sum(st.values())) < 1e-9
+    assert abs(r["frac"] - r["bound_ms"] / 6.7) < 1e-12 and 0.2 < r["frac"] < 1.0
+
