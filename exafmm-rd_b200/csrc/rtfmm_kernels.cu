@@ -48,9 +48,9 @@
 #ifndef P2P_TILE
 #define P2P_TILE 32
 #endif
-// register-blocked FFT-M2L up: resident blocks per SM
+// register-blocked FFT-M2L up: resident blocks per SM (FP32; FP64 keeps 2)
 #ifndef UP_RB_MINB
-#define UP_RB_MINB 2
+#define UP_RB_MINB 3
 #endif
 // FP32 Hadamard: targets per thread, directions per FP32 partial sum,
 // resident blocks per SM
@@ -1124,16 +1124,19 @@ __global__ void __launch_bounds__(256)
 // for bit; the shared-memory traffic per multiply-add falls from two loads
 // to about one broadcast.
 template <typename T, int PP>
-__global__ void __launch_bounds__(256, UP_RB_MINB)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? UP_RB_MINB : 2)
     k_m2l_up_rb(const double* __restrict__ q_equiv, const int* __restrict__ items, const int* __restrict__ surf_ijk,
                 const double* __restrict__ twiddle, int ns, int nsrc, int sp, T* __restrict__ Q) {
   constexpr int P = PP, N = 2 * P - 1, P3 = P * P * P, PNP = P * N * P;
-  constexpr int SPM = 32 / (2 * (int)sizeof(T));  // largest slot group (m2l_up_slots)
-  constexpr int KC = (256 / (N * P)) < 1 ? 1 : ((256 / (N * P)) > N ? N : 256 / (N * P));
+  // the last pass: a thread per (pair of slots, ky, kx, range of kz)
+  constexpr int KC = (128 / (N * P)) < 1 ? 1 : ((128 / (N * P)) > N ? N : 128 / (N * P));
   constexpr int KH = (N + KC - 1) / KC;
-  extern __shared__ unsigned char smem_raw[];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  // the twiddle table padded to 8 values, so that A and the cube (read as
+  // 16-byte vectors) start on 16-byte boundaries
+  constexpr int WSZ = (2 * N * N + 7) / 8 * 8;
   T* W = reinterpret_cast<T*>(smem_raw);  // N*N complex: W[k][n] = w^(k n mod N)
-  T* A = W + 2 * N * N;                   // sp * P^3 complex: [slot][z][y][kx]
+  T* A = W + WSZ;                         // sp * P^3 complex: [slot][z][y][kx]
   T* cube = A + 2 * (size_t)sp * P3;      // sp * P^3, read by the first pass only
   T* Bm = cube;                           // sp * P*N*P complex: [slot][z][ky][kx], after it
   const int* it = items + 10 * blockIdx.x;
@@ -1159,8 +1162,19 @@ __global__ void __launch_bounds__(256, UP_RB_MINB)
     const int j = e / (P * P), zy = e - j * P * P;
     const T* row = cube + (size_t)j * P3 + zy * P;
     T r[P];
+    if constexpr (sizeof(T) == 4 && P % 4 == 0) {
 #pragma unroll
-    for (int x = 0; x < P; ++x) r[x] = row[x];
+      for (int x = 0; x < P; x += 4) {
+        const float4 v = *reinterpret_cast<const float4*>(row + x);
+        r[x] = v.x;
+        r[x + 1] = v.y;
+        r[x + 2] = v.z;
+        r[x + 3] = v.w;
+      }
+    } else {
+#pragma unroll
+      for (int x = 0; x < P; ++x) r[x] = row[x];
+    }
     T* a = A + 2 * ((size_t)j * P3 + zy * P);
 #pragma unroll
     for (int kx = 0; kx < P; ++kx) {
@@ -1198,22 +1212,25 @@ __global__ void __launch_bounds__(256, UP_RB_MINB)
     }
   }
   __syncthreads();
-  // z -> kz: a thread per (ky, kx, range of kz), every slot; two slots of a
-  // frequency written together as in k_m2l_up
+  // z -> kz: a thread per (pair of slots, ky, kx, range of kz); the two
+  // slots of a pair written together as in k_m2l_up
   using V2 = typename Cplx2<T>::type;
-  for (int e = tid; e < N * P * KC; e += nt) {
-    const int c = e / (N * P), ky = (e / P) % N, kx = e % P;
-    T br[SPM][P], bi[SPM][P];
+  const int npair = (sp + 1) / 2;
+  for (int e = tid; e < npair * N * P * KC; e += nt) {
+    const int jp = e / (N * P * KC), c = (e / (N * P)) % KC, ky = (e / P) % N, kx = e % P;
+    const int j = 2 * jp;
+    const bool two = j + 1 < sp;
+    T br[2][P], bi[2][P];
 #pragma unroll
-    for (int j = 0; j < SPM; ++j)
+    for (int u = 0; u < 2; ++u)
 #pragma unroll
       for (int z = 0; z < P; ++z) {
-        if (j < sp) {
-          const T* q = Bm + 2 * ((size_t)j * PNP + (z * N + ky) * P + kx);
-          br[j][z] = q[0];
-          bi[j][z] = q[1];
+        if (u == 0 || two) {
+          const T* q = Bm + 2 * ((size_t)(j + u) * PNP + (z * N + ky) * P + kx);
+          br[u][z] = q[0];
+          bi[u][z] = q[1];
         } else {
-          br[j][z] = bi[j][z] = T(0);
+          br[u][z] = bi[u][z] = T(0);
         }
       }
     const int kz1 = (c + 1) * KH < N ? (c + 1) * KH : N;
@@ -1221,26 +1238,22 @@ __global__ void __launch_bounds__(256, UP_RB_MINB)
       const T* wk = W + 2 * kz * N;
       const int f = (kz * N + ky) * P + kx;
       T* out = Q + (((size_t)f * nsrc + src) * 8 + slot0) * 2;
+      T re0 = 0, im0 = 0, re1 = 0, im1 = 0;
 #pragma unroll
-      for (int j = 0; j < SPM; j += 2) {
-        if (j >= sp) break;
-        T re0 = 0, im0 = 0, re1 = 0, im1 = 0;
-#pragma unroll
-        for (int z = 0; z < P; ++z) {
-          cmad(re0, im0, br[j][z], bi[j][z], wk[2 * z], wk[2 * z + 1]);
-          if (j + 1 < sp) cmad(re1, im1, br[j + 1][z], bi[j + 1][z], wk[2 * z], wk[2 * z + 1]);
-        }
-        if (j + 1 < sp) {
-          V2 v;
-          v.x = re0;
-          v.y = im0;
-          v.z = re1;
-          v.w = im1;
-          *reinterpret_cast<V2*>(out + 2 * j) = v;
-        } else {
-          out[2 * j] = re0;
-          out[2 * j + 1] = im0;
-        }
+      for (int z = 0; z < P; ++z) {
+        cmad(re0, im0, br[0][z], bi[0][z], wk[2 * z], wk[2 * z + 1]);
+        if (two) cmad(re1, im1, br[1][z], bi[1][z], wk[2 * z], wk[2 * z + 1]);
+      }
+      if (two) {
+        V2 v;
+        v.x = re0;
+        v.y = im0;
+        v.z = re1;
+        v.w = im1;
+        *reinterpret_cast<V2*>(out + 2 * j) = v;
+      } else {
+        out[2 * j] = re0;
+        out[2 * j + 1] = im0;
       }
     }
   }
@@ -1908,7 +1921,8 @@ static bool fixed_p(int P) { return P == 4 || P == 6 || P == 8 || P == 10; }
 template <typename T>
 static size_t up_smem(int P, int sp) {
   const size_t N = 2 * P - 1, P3 = (size_t)P * P * P;
-  if (fixed_p(P)) return sizeof(T) * (2 * N * N + 2 * (size_t)sp * P3 + std::max((size_t)sp * P3, 2 * (size_t)sp * P * N * P));
+  if (fixed_p(P))
+    return sizeof(T) * ((2 * N * N + 7) / 8 * 8 + 2 * (size_t)sp * P3 + std::max((size_t)sp * P3, 2 * (size_t)sp * P * N * P));
   return sizeof(T) * (2 * N * N + 3 * P3 + 2 * (size_t)sp * P * N * P);
 }
 template <typename T>
