@@ -67,6 +67,10 @@
 #ifndef HAD_ACC_SMEM
 #define HAD_ACC_SMEM 1
 #endif
+// FP32 Hadamard: packed FP32x2 FMAs (1) or scalar FMAs (0)
+#ifndef HAD_F2
+#define HAD_F2 1
+#endif
 // FP64 operator application: output rows per block (64 or 128), FP64
 // tensor-core (mma.sync) inner product
 #ifndef APPLY_TM
@@ -1439,6 +1443,46 @@ __device__ __forceinline__ void had_mac(const typename Cplx<T>::type* __restrict
     }
 }
 
+// The same product in packed FP32x2 FMAs, with the coefficients of an itar
+// pair laid (gr0, gr1, gi0, gi1) in shared memory: per output the FMAs and
+// their order are those of cmad, so the sums are bit for bit the scalar ones.
+template <int TT>
+__device__ __forceinline__ void had_mac_f2(const float4* __restrict__ g, const int (&sd)[TT], const float2 (&q)[TT][8],
+                                           float (&pr)[TT][8], float (&pi)[TT][8]) {
+  bool any = false;
+#pragma unroll
+  for (int u = 0; u < TT; ++u) any |= sd[u] >= 0;
+  if (!any) return;
+#pragma unroll
+  for (int isrc = 0; isrc < 8; ++isrc) {
+    float2 qr[TT], qi[TT], nqi[TT];
+#pragma unroll
+    for (int u = 0; u < TT; ++u) {
+      qr[u] = make_float2(q[u][isrc].x, q[u][isrc].x);
+      qi[u] = make_float2(q[u][isrc].y, q[u][isrc].y);
+      nqi[u] = make_float2(-q[u][isrc].y, -q[u][isrc].y);
+    }
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      const float4 gv = g[isrc * 4 + p];
+      const float2 gr = make_float2(gv.x, gv.y), gi = make_float2(gv.z, gv.w);
+#pragma unroll
+      for (int u = 0; u < TT; ++u) {
+        float2 re = make_float2(pr[u][2 * p], pr[u][2 * p + 1]);
+        float2 im = make_float2(pi[u][2 * p], pi[u][2 * p + 1]);
+        re = __ffma2_rn(gr, qr[u], re);
+        re = __ffma2_rn(gi, nqi[u], re);
+        im = __ffma2_rn(gr, qi[u], im);
+        im = __ffma2_rn(gi, qr[u], im);
+        pr[u][2 * p] = re.x;
+        pr[u][2 * p + 1] = re.y;
+        pi[u][2 * p] = im.x;
+        pi[u][2 * p + 1] = im.y;
+      }
+    }
+  }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(HadCfg<T>::THREADS, HadCfg<T>::MINB)
     k_m2l_hadamard8(const T* __restrict__ Q, const T* __restrict__ G, const int* __restrict__ tsrcT, int ntar,
@@ -1448,7 +1492,19 @@ __global__ void __launch_bounds__(HadCfg<T>::THREADS, HadCfg<T>::MINB)
   __shared__ __align__(32) C2 Gs[26 * 64];
   const int f = blockIdx.y;
   const C2* Gf = reinterpret_cast<const C2*>(G) + (size_t)f * 26 * 64;
-  for (int e = threadIdx.x; e < 26 * 64; e += NT) Gs[e] = Gf[e];
+  constexpr bool kF2 = HAD_F2 && sizeof(T) == 4;
+  if constexpr (kF2) {
+    // (gr, gi) of itar 2p, 2p+1 -> (gr0, gr1, gi0, gi1)
+    T* gs = reinterpret_cast<T*>(Gs);
+    for (int e = threadIdx.x; e < 26 * 64; e += NT) {
+      const int h = e & 1, b = (e & ~1) * 2;
+      const C2 v = Gf[e];
+      gs[b + h] = v.x;
+      gs[b + 2 + h] = v.y;
+    }
+  } else {
+    for (int e = threadIdx.x; e < 26 * 64; e += NT) Gs[e] = Gf[e];
+  }
   // targets of this thread: t0 + u * NT, u < TT (coalesced tsrcT reads)
   const int t0 = blockIdx.x * NT * TT + threadIdx.x;
   const C2* Qf = reinterpret_cast<const C2*>(Q) + (size_t)f * nsrc * 8;
@@ -1499,11 +1555,18 @@ __global__ void __launch_bounds__(HadCfg<T>::THREADS, HadCfg<T>::MINB)
         pr[u][i] = pi[u][i] = T(0);
       }
   };
+  auto MAC = [&](const C2* g, const int (&sd)[TT], const C2 (&q)[TT][8]) {
+    if constexpr (kF2) {
+      had_mac_f2<TT>(reinterpret_cast<const float4*>(g), sd, q, pr, pi);
+    } else {
+      had_mac<T, TT>(g, sd, q, pr, pi);
+    }
+  };
   for (int d = 0; d < 26; d += 2) {
     int ja[TT];
     had_rows<T, TT>(Qf, ib, qb);
     if (d + 2 < 26) had_index<T, TT>(tsrcT, d + 2, t0, NT, ntar, ja);
-    had_mac<T, TT>(Gs + d * 64, ia, qa, pr, pi);
+    MAC(Gs + d * 64, ia, qa);
     if (DF == 1 || (d + 1) % DF == 0) flush();
     if (d + 2 < 26) {
 #pragma unroll
@@ -1512,7 +1575,7 @@ __global__ void __launch_bounds__(HadCfg<T>::THREADS, HadCfg<T>::MINB)
     }
     int jb[TT];
     if (d + 3 < 26) had_index<T, TT>(tsrcT, d + 3, t0, NT, ntar, jb);
-    had_mac<T, TT>(Gs + (d + 1) * 64, ib, qb, pr, pi);
+    MAC(Gs + (d + 1) * 64, ib, qb);
     if ((d + 2) % DF == 0 || d + 2 == 26) flush();
     if (d + 3 < 26) {
 #pragma unroll
