@@ -67,6 +67,10 @@
 #ifndef HAD_ACC_SMEM
 #define HAD_ACC_SMEM 1
 #endif
+// FP32 8x8 source spectra in 32-byte chunks (1) or whole rows (0), q8_index
+#ifndef Q8_CHUNKED
+#define Q8_CHUNKED 1
+#endif
 // FP32 Hadamard: packed FP32x2 FMAs (1) or scalar FMAs (0)
 #ifndef HAD_F2
 #define HAD_F2 1
@@ -96,6 +100,18 @@ template <> struct Cplx<double> { using type = double2; };
 template <typename T> struct Cplx2;
 template <> struct Cplx2<float> { using type = float4; };
 template <> struct Cplx2<double> { using type = double4; };
+
+// Layout of the 8x8 source spectra Q (complex, [frequency][source][slot]).
+// The FP32 form stores a frequency's rows in two 32-byte chunks (slots
+// 4c .. 4c+3): chunk 0 of every source, then chunk 1, so that the Hadamard's
+// lanes, which take consecutive targets and so mostly consecutive sources,
+// read a chunk of their rows from consecutive sectors, and an up-pass block
+// (4 slots of one source) still writes whole sectors.  FP64 rows stay whole.
+template <typename T>
+__host__ __device__ __forceinline__ size_t q8_index(size_t f, int src, int slot, int nsrc) {
+  if (sizeof(T) == 4 && Q8_CHUNKED) return ((f * 2 + (slot >> 2)) * nsrc + src) * 4 + (slot & 3);
+  return (f * nsrc + src) * 8 + slot;
+}
 
 // 32-byte (one sector) vector loads, sm_100: one lane reads a whole sector.
 __device__ __forceinline__ void ld_sector(const float* p, float (&v)[8]) {
@@ -1094,8 +1110,8 @@ __global__ void __launch_bounds__(256)
   for (int f = tid; f < Nf; f += nt) {
     const int kz = f / (N * P), ky = (f / P) % N, kx = f % P;
     const T* wk = W + 2 * kz * N;
-    T* out = Q + (((size_t)f * nsrc + src) * 8 + slot0) * 2;
     for (int j = 0; j < sp; j += 2) {
+      T* out = Q + 2 * q8_index<T>(f, src, slot0 + j, nsrc);
       T re0 = 0, im0 = 0, re1 = 0, im1 = 0;
       const T* B0 = Bm + 2 * (size_t)j * PNP;
       const T* B1 = B0 + 2 * (size_t)PNP;
@@ -1110,10 +1126,10 @@ __global__ void __launch_bounds__(256)
         v.y = im0;
         v.z = re1;
         v.w = im1;
-        *reinterpret_cast<V2*>(out + 2 * j) = v;
+        *reinterpret_cast<V2*>(out) = v;
       } else {
-        out[2 * j] = re0;
-        out[2 * j + 1] = im0;
+        out[0] = re0;
+        out[1] = im0;
       }
     }
   }
@@ -1241,7 +1257,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? UP_RB_MINB : 2)
     for (int kz = c * KH; kz < kz1; ++kz) {
       const T* wk = W + 2 * kz * N;
       const int f = (kz * N + ky) * P + kx;
-      T* out = Q + (((size_t)f * nsrc + src) * 8 + slot0) * 2;
+      T* out = Q + 2 * q8_index<T>(f, src, slot0 + j, nsrc);
       T re0 = 0, im0 = 0, re1 = 0, im1 = 0;
 #pragma unroll
       for (int z = 0; z < P; ++z) {
@@ -1254,10 +1270,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? UP_RB_MINB : 2)
         v.y = im0;
         v.z = re1;
         v.w = im1;
-        *reinterpret_cast<V2*>(out + 2 * j) = v;
+        *reinterpret_cast<V2*>(out) = v;
       } else {
-        out[2 * j] = re0;
-        out[2 * j + 1] = im0;
+        out[0] = re0;
+        out[1] = im0;
       }
     }
   }
@@ -1400,12 +1416,27 @@ __device__ __forceinline__ void load_row8(const T* qrow, typename Cplx<T>::type 
 }
 
 template <typename T, int TT>
-__device__ __forceinline__ void had_rows(const typename Cplx<T>::type* __restrict__ Qf, const int (&sd)[TT],
+__device__ __forceinline__ void had_rows(const typename Cplx<T>::type* __restrict__ Qf, int nsrc, const int (&sd)[TT],
                                          typename Cplx<T>::type (&q)[TT][8]) {
 #pragma unroll
   for (int u = 0; u < TT; ++u) {
     if (sd[u] >= 0) {
-      load_row8<T>(reinterpret_cast<const T*>(Qf + (size_t)sd[u] * 8), q[u]);
+      if constexpr (sizeof(T) == 4 && Q8_CHUNKED) {
+        // chunk c of this source: slots 4c .. 4c+3, one sector
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const float* qc = reinterpret_cast<const float*>(Qf) + ((size_t)c * nsrc + sd[u]) * 8;
+          float v[8];
+          ld_sector(qc, v);
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            q[u][4 * c + k].x = v[2 * k];
+            q[u][4 * c + k].y = v[2 * k + 1];
+          }
+        }
+      } else {
+        load_row8<T>(reinterpret_cast<const T*>(Qf + (size_t)sd[u] * 8), q[u]);
+      }
     } else {
 #pragma unroll
       for (int i = 0; i < 8; ++i) q[u][i].x = q[u][i].y = T(0);
@@ -1515,7 +1546,7 @@ __global__ void __launch_bounds__(HadCfg<T>::THREADS, HadCfg<T>::MINB)
   C2 qa[TT][8], qb[TT][8];
   if (t0 < ntar) {
     had_index<T, TT>(tsrcT, 0, t0, NT, ntar, ia);
-    had_rows<T, TT>(Qf, ia, qa);
+    had_rows<T, TT>(Qf, nsrc, ia, qa);
     had_index<T, TT>(tsrcT, 1, t0, NT, ntar, ib);
   }
   __syncthreads();
@@ -1564,14 +1595,14 @@ __global__ void __launch_bounds__(HadCfg<T>::THREADS, HadCfg<T>::MINB)
   };
   for (int d = 0; d < 26; d += 2) {
     int ja[TT];
-    had_rows<T, TT>(Qf, ib, qb);
+    had_rows<T, TT>(Qf, nsrc, ib, qb);
     if (d + 2 < 26) had_index<T, TT>(tsrcT, d + 2, t0, NT, ntar, ja);
     MAC(Gs + d * 64, ia, qa);
     if (DF == 1 || (d + 1) % DF == 0) flush();
     if (d + 2 < 26) {
 #pragma unroll
       for (int u = 0; u < TT; ++u) ia[u] = ja[u];
-      had_rows<T, TT>(Qf, ia, qa);
+      had_rows<T, TT>(Qf, nsrc, ia, qa);
     }
     int jb[TT];
     if (d + 3 < 26) had_index<T, TT>(tsrcT, d + 3, t0, NT, ntar, jb);
