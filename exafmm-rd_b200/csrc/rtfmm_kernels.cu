@@ -67,9 +67,13 @@
 #ifndef HAD_ACC_SMEM
 #define HAD_ACC_SMEM 1
 #endif
-// FP32 8x8 source spectra in 32-byte chunks (1) or whole rows (0), q8_index
+// 8x8 source spectra in 32-byte chunks (1) or whole rows (0), q8_index; the
+// FP64 spectra too (Q8_CHUNKED64)
 #ifndef Q8_CHUNKED
 #define Q8_CHUNKED 1
+#endif
+#ifndef Q8_CHUNKED64
+#define Q8_CHUNKED64 1
 #endif
 // FP32 Hadamard: packed FP32x2 FMAs (1) or scalar FMAs (0)
 #ifndef HAD_F2
@@ -102,14 +106,16 @@ template <> struct Cplx2<float> { using type = float4; };
 template <> struct Cplx2<double> { using type = double4; };
 
 // Layout of the 8x8 source spectra Q (complex, [frequency][source][slot]).
-// The FP32 form stores a frequency's rows in two 32-byte chunks (slots
-// 4c .. 4c+3): chunk 0 of every source, then chunk 1, so that the Hadamard's
+// A frequency's rows are stored in 32-byte chunks (4 slots in FP32, 2 in
+// FP64): chunk 0 of every source, then chunk 1, ..., so that the Hadamard's
 // lanes, which take consecutive targets and so mostly consecutive sources,
 // read a chunk of their rows from consecutive sectors, and an up-pass block
-// (4 slots of one source) still writes whole sectors.  FP64 rows stay whole.
+// (slot pairs of one source) still writes whole sectors.
 template <typename T>
 __host__ __device__ __forceinline__ size_t q8_index(size_t f, int src, int slot, int nsrc) {
-  if (sizeof(T) == 4 && Q8_CHUNKED) return ((f * 2 + (slot >> 2)) * nsrc + src) * 4 + (slot & 3);
+  constexpr int per = 32 / (2 * sizeof(T)), nch = 8 / per;  // slots per chunk, chunks per row
+  if (Q8_CHUNKED && (sizeof(T) == 4 || Q8_CHUNKED64))
+    return ((f * nch + slot / per) * nsrc + src) * per + slot % per;
   return (f * nsrc + src) * 8 + slot;
 }
 
@@ -1421,17 +1427,18 @@ __device__ __forceinline__ void had_rows(const typename Cplx<T>::type* __restric
 #pragma unroll
   for (int u = 0; u < TT; ++u) {
     if (sd[u] >= 0) {
-      if constexpr (sizeof(T) == 4 && Q8_CHUNKED) {
-        // chunk c of this source: slots 4c .. 4c+3, one sector
+      if constexpr (Q8_CHUNKED && (sizeof(T) == 4 || Q8_CHUNKED64)) {
+        // chunk c of this source: slots per*c .. per*c+per-1, one sector
+        constexpr int per = 32 / (2 * sizeof(T)), nch = 8 / per;
 #pragma unroll
-        for (int c = 0; c < 2; ++c) {
-          const float* qc = reinterpret_cast<const float*>(Qf) + ((size_t)c * nsrc + sd[u]) * 8;
-          float v[8];
+        for (int c = 0; c < nch; ++c) {
+          const T* qc = reinterpret_cast<const T*>(Qf) + ((size_t)c * nsrc + sd[u]) * 2 * per;
+          T v[2 * per];
           ld_sector(qc, v);
 #pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            q[u][4 * c + k].x = v[2 * k];
-            q[u][4 * c + k].y = v[2 * k + 1];
+          for (int k = 0; k < per; ++k) {
+            q[u][per * c + k].x = v[2 * k];
+            q[u][per * c + k].y = v[2 * k + 1];
           }
         }
       } else {
@@ -1661,7 +1668,7 @@ __global__ void k_m2l_hadamard27(const double* __restrict__ Q, const double* __r
     const int s = tsrc[t * 26 + d];
     if (s < 0) continue;
     const double gr = G27[((size_t)d * Nf + f) * 2], gi = G27[((size_t)d * Nf + f) * 2 + 1];
-    const size_t qo = (((size_t)f * nsrc + s) * 8 + 0) * 2;
+    const size_t qo = 2 * q8_index<double>(f, s, 0, nsrc);  // the up pass's layout, slot 0
     cmad(re, im, gr, gi, Q[qo], Q[qo + 1]);
   }
   const size_t po = (((size_t)f * ntar + t) * 8 + 0) * 2;
