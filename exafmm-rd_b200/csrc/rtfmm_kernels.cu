@@ -2018,7 +2018,7 @@ cudaError_t launch_sum_children(const int* list, int nparents, const double* Y, 
 }
 
 // orders with a compile-time instance (the register-blocked kernels)
-static bool fixed_p(int P) { return P == 4 || P == 6 || P == 8 || P == 10; }
+static bool fixed_p(int P) { return (P >= 4 && P <= 8) || P == 10; }
 template <typename T>
 static size_t up_smem(int P, int sp) {
   const size_t N = 2 * P - 1, P3 = (size_t)P * P * P;
@@ -2076,7 +2076,9 @@ cudaError_t launch_m2l_up(const double* q_equiv, const int* items, int nitems, c
   if (nitems <= 0) return cudaGetLastError();
   switch (P) {
     case 4: return up_p<T, 4>(q_equiv, items, nitems, surf_ijk, twiddle, P, ns, nsrc, sp, Q, st);
+    case 5: return up_p<T, 5>(q_equiv, items, nitems, surf_ijk, twiddle, P, ns, nsrc, sp, Q, st);
     case 6: return up_p<T, 6>(q_equiv, items, nitems, surf_ijk, twiddle, P, ns, nsrc, sp, Q, st);
+    case 7: return up_p<T, 7>(q_equiv, items, nitems, surf_ijk, twiddle, P, ns, nsrc, sp, Q, st);
     case 8: return up_p<T, 8>(q_equiv, items, nitems, surf_ijk, twiddle, P, ns, nsrc, sp, Q, st);
     case 10: return up_p<T, 10>(q_equiv, items, nitems, surf_ijk, twiddle, P, ns, nsrc, sp, Q, st);
     default: return up_p<T, 0>(q_equiv, items, nitems, surf_ijk, twiddle, P, ns, nsrc, sp, Q, st);
@@ -2144,7 +2146,9 @@ cudaError_t launch_m2l_down(const T* Pk, const int* items, const double* tscale,
   if (nitems <= 0) return cudaGetLastError();
   switch (P) {
     case 4: return down_p<T, 4>(Pk, items, tscale, nitems, surf_ijk, twiddle, P, ns, ntar, sp, p_check, st);
+    case 5: return down_p<T, 5>(Pk, items, tscale, nitems, surf_ijk, twiddle, P, ns, ntar, sp, p_check, st);
     case 6: return down_p<T, 6>(Pk, items, tscale, nitems, surf_ijk, twiddle, P, ns, ntar, sp, p_check, st);
+    case 7: return down_p<T, 7>(Pk, items, tscale, nitems, surf_ijk, twiddle, P, ns, ntar, sp, p_check, st);
     case 8: return down_p<T, 8>(Pk, items, tscale, nitems, surf_ijk, twiddle, P, ns, ntar, sp, p_check, st);
     case 10: return down_p<T, 10>(Pk, items, tscale, nitems, surf_ijk, twiddle, P, ns, ntar, sp, p_check, st);
     default: return down_p<T, 0>(Pk, items, tscale, nitems, surf_ijk, twiddle, P, ns, ntar, sp, p_check, st);
