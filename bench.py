@@ -513,7 +513,7 @@ def run_ours(args):
     eq_err = None
     if world == 1 and not args.no_equal_error:
         eq_err = equal_error(pkg, mk, x, q, (phi_d, grad_d), w_dev, dq_dev, dx_dev, (dq_d, dx_d),
-                             [("north-star bound", 1e-5),
+                             [("1e-5 accuracy bound", 1e-5),
                               ("mixed form's own error at P=8 ncrit=256", max(err["l2f"], err_mr))],
                              max(3, args.steps // 2))
     t_m, t_d, t_e = max_over_ranks([t_m, t_d, t_e], world, "cuda")

@@ -2,8 +2,7 @@
 returns dL/dq = K^T w and dL/dx, where K is the discretised FMM operator.
 
 Checks: the transpose identity <w, K q> = <q, K^T w>; central finite
-differences of dL/dx (h = 1e-4, FP64, 64 bodies away from cell faces, as the
-north-star check asks); dL/dx for L = 1/2 sum q phi against q times the
+differences of dL/dx (h = 1e-4, FP64, 64 bodies away from cell faces); dL/dx for L = 1/2 sum q phi against q times the
 reference's own gradient output; and the autograd harness.
 """
 import os

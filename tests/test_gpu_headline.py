@@ -77,7 +77,7 @@ def test_c2_fp64_matches_reference(pkg, c2):
     assert abs(np.linalg.norm(phi - phi.mean()) / float(g["phi_norm_mr"]) - 1) < 1e-8
 
 
-def test_c2_mixed_within_north_star_bound(pkg, c2):
+def test_c2_mixed_within_1e5_bound(pkg, c2):
     """The FP32-mixed form well within the 1e-5 bound of the reference
     (sampled) and of the FP64 form (all bodies), potential and gradient
     (measured: gradient 1.6e-7, potential 6.6e-7 against the FP64 form; the

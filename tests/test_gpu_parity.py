@@ -10,7 +10,7 @@ Tolerances (relative L2, the reference's ``compare`` metric):
                    which differs between any two FP64 implementations and
                    which neither the gradient nor the energy of a neutral
                    system sees.
-  FP32-mixed form  1e-5 on potential and gradient.
+  FP32-mixed form  1e-5 on potential and gradient (the mixed form's accuracy bound).
 """
 import math
 import os
